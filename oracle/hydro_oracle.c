@@ -1,0 +1,871 @@
+/*
+ * hydro_oracle.c -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C restatement of the reference hydro-bench hot path, used by the
+ * tests, smoke() and the CPU-baseline leg of bench.py as the checker. It is
+ * never linked into, loaded by or called from the product library.
+ *
+ * What it restates (paths relative to the reference project):
+ *   deck reader     cuda_native_impl/hydro-cal-src/src/mesh.cpp:5-278
+ *   geometry        mesh.cpp:280-372           (preCalculate)
+ *   boundary tables mesh.cpp:374-533           (take_boundary_for_two_d, BOUNDRYinterp)
+ *   device relayout cuda_native_impl/hydro-cal-src/src/cell.cpp:72-128
+ *   flux            cuda_native_impl/hydro-cal-src/src/functors.cu:47-202 and 204-712
+ *   update          functors.cu:717-784
+ *   variant F       cuda_native_impl/baselines/native_cuda_v0/fp64/hydro-cal-src/src/functors.cu
+ *                   (:376-377 KLAS=1 uses kt, :518-519 no H<HM2 guard,
+ *                    :752-768 per-cell CFL step DT2, :791-793 5 m/s cap)
+ *   step loop       cuda_native_impl/benchmark.cu:87-96
+ *
+ * Compiled with -ffp-contract=off: every product is rounded on its own, so
+ * results differ from the GPU build (which contracts a*b+c into FMAs) by a
+ * few ulps per operation; CUDA's pow may also differ from glibc's by an ulp.
+ *
+ * Where the reference reads memory it never wrote, this restatement defines
+ * the value and says so:
+ *   - KLAS=7 uses a depth HB that the reference leaves uninitialised
+ *     (functors.cu:525 declares it, :246-247 reads it); here HB = the cell's
+ *     own depth.
+ *   - The mirrored Osher branch reads H[NC] with NC = -1 when a slot without a
+ *     neighbour reaches it (functors.cu:165-190); here such a slot raises the
+ *     error flag and uses a zero neighbour state.
+ *   - BOUNDRYinterp reads one element past the time table when the query time
+ *     is at or beyond its last entry (mesh.cpp:525-531); here the missing
+ *     element ends the search (the decks bracket every query time).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_VARIANT_H 0
+#define ORC_VARIANT_F 1
+
+/* functors.cu / common.hpp:44-52 */
+static const double C0 = 1.33, C1 = 1.7, VMIN = 0.001, QLUA = 0.0, BRDTH = 100.0;
+
+typedef struct orc_deck {
+    int cells, nod, ndays, mdt, nz, nq, nzq, nhq, nwe, ndi, ntoutput;
+    double dt, hm1, hm2, jl;
+    /* per slot [4*cells], slot = 4*cell + j */
+    double *nac, *klas, *side, *cosf, *sinf, *slcos, *slsin;
+    double *f0, *f1, *f2, *f3;
+    /* per cell */
+    double *h, *u, *v, *z, *w, *zbc, *zb1, *area, *fnc, *bfeat;
+    int *nhq1;
+    double *zw, *qw;                   /* [cells*nhq]   */
+    double *qt, *dqt, *zt, *dzt;       /* [ndays*cells] */
+    int error;                         /* set when a slot reaches undefined reference behaviour */
+} orc_deck;
+
+/* ------------------------------------------------------------------------ */
+/* deck reader: line-oriented like mesh.cpp's std::getline + istringstream   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct { char *buf; size_t n, pos; } reader;
+
+static int rd_open(reader *r, const char *root, const char *rel) {
+    char path[4096];
+    snprintf(path, sizeof path, "%s/%s", root, rel);
+    FILE *f = fopen(path, "rb");
+    if (!f) return -1;
+    fseek(f, 0, SEEK_END);
+    long n = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    r->buf = (char *)malloc((size_t)n + 1);
+    if (!r->buf) { fclose(f); return -1; }
+    r->n = fread(r->buf, 1, (size_t)n, f);
+    r->buf[r->n] = 0;
+    r->pos = 0;
+    fclose(f);
+    return 0;
+}
+
+static void rd_close(reader *r) { free(r->buf); r->buf = NULL; }
+
+/* next line as a NUL-terminated string (NULL at end of file) */
+static char *rd_line(reader *r) {
+    if (r->pos >= r->n) return NULL;
+    char *s = r->buf + r->pos;
+    char *e = memchr(s, '\n', r->n - r->pos);
+    if (e) { *e = 0; r->pos = (size_t)(e - r->buf) + 1; }
+    else r->pos = r->n;
+    size_t L = strlen(s);
+    if (L && s[L - 1] == '\r') s[L - 1] = 0;
+    return s;
+}
+
+/* parse the next whitespace-separated number; returns 0 and leaves *out untouched when none */
+static int next_d(char **p, double *out) {
+    char *e;
+    double v = strtod(*p, &e);
+    if (e == *p) return 0;
+    *out = v; *p = e; return 1;
+}
+static int next_i(char **p, int *out) {
+    char *e;
+    long v = strtol(*p, &e, 10);
+    if (e == *p) return 0;
+    *out = (int)v; *p = e; return 1;
+}
+
+static int read_scalars_i(const char *root, const char *rel, int n, int **dst) {
+    reader r;
+    if (rd_open(&r, root, rel)) return -1;
+    for (int k = 0; k < n; k++) {
+        char *ln = rd_line(&r);
+        if (!ln || !next_i(&ln, dst[k])) { rd_close(&r); return -1; }
+    }
+    rd_close(&r);
+    return 0;
+}
+
+static void *zalloc(size_t n) { void *p = calloc(n ? n : 1, 1); return p; }
+
+/* per-cell four-column files: header, then "NO a b c d" (mesh.cpp:40-98) */
+static int read_cell4(const char *root, const char *rel, int cells, double *out_d, int *out_i) {
+    reader r;
+    if (rd_open(&r, root, rel)) return -1;
+    rd_line(&r);
+    for (int i = 0; i < cells; i++) {
+        char *ln = rd_line(&r);
+        if (!ln) break;
+        int no;
+        if (!next_i(&ln, &no)) continue;
+        for (int j = 0; j < 4; j++) {
+            if (out_d) { if (!next_d(&ln, &out_d[4 * i + j])) break; }
+            else { if (!next_i(&ln, &out_i[4 * i + j])) break; }
+        }
+    }
+    rd_close(&r);
+    return 0;
+}
+
+/* header, then one value per line (mesh.cpp:100-114, 220-278) */
+static int read_col(const char *root, const char *rel, int n, double *out) {
+    reader r;
+    if (rd_open(&r, root, rel)) return -1;
+    rd_line(&r);
+    for (int i = 0; i < n; i++) {
+        char *ln = rd_line(&r);
+        if (!ln) break;
+        next_d(&ln, &out[i]);
+    }
+    rd_close(&r);
+    return 0;
+}
+
+/* header with the group count, then "NO cell value" rows (mesh.cpp:135-218) */
+static int read_groups(const char *root, const char *rel, int rows, int *count0, double *col1, double *col2) {
+    reader r;
+    if (rd_open(&r, root, rel)) return -1;
+    char *ln = rd_line(&r);
+    if (ln) next_i(&ln, count0);
+    for (int i = 0; i < rows; i++) {
+        ln = rd_line(&r);
+        if (!ln) break;
+        int no;
+        if (!next_i(&ln, &no)) continue;
+        next_d(&ln, &col1[i]);
+        next_d(&ln, &col2[i]);
+    }
+    rd_close(&r);
+    return 0;
+}
+
+typedef struct { int n; double *t, *v; } series;
+
+static int read_series(const char *root, const char *rel, series *s, int cap) {
+    reader r;
+    if (rd_open(&r, root, rel)) return -1;
+    char *ln = rd_line(&r);
+    s->n = 0;
+    if (ln) next_i(&ln, &s->n);
+    int alloc = s->n > cap ? s->n : cap;
+    s->t = (double *)zalloc(sizeof(double) * (size_t)(alloc + 1));
+    s->v = (double *)zalloc(sizeof(double) * (size_t)(alloc + 1));
+    for (int i = 0; i < s->n; i++) {
+        ln = rd_line(&r);
+        if (!ln) break;
+        next_d(&ln, &s->t[i]);
+        next_d(&ln, &s->v[i]);
+    }
+    rd_close(&r);
+    return 0;
+}
+
+/* mesh.cpp:523-533; the search stops where the table ends */
+static double boundary_interp(double t, const series *s) {
+    double result = 0;
+    for (int i = 1; i < s->n; i++) {
+        if (t >= s->t[i - 1] && t <= s->t[i])
+            result = s->v[i - 1] + (s->v[i] - s->v[i - 1]) / (s->t[i] - s->t[i - 1]) * (t - s->t[i - 1]);
+    }
+    return result;
+}
+
+void orc_deck_free(orc_deck *d) {
+    double **dd[] = {&d->nac, &d->klas, &d->side, &d->cosf, &d->sinf, &d->slcos, &d->slsin,
+                     &d->f0, &d->f1, &d->f2, &d->f3, &d->h, &d->u, &d->v, &d->z, &d->w,
+                     &d->zbc, &d->zb1, &d->area, &d->fnc, &d->bfeat, &d->zw, &d->qw,
+                     &d->qt, &d->dqt, &d->zt, &d->dzt};
+    for (size_t k = 0; k < sizeof dd / sizeof dd[0]; k++) { free(*dd[k]); *dd[k] = NULL; }
+    free(d->nhq1); d->nhq1 = NULL;
+}
+
+size_t orc_deck_sizeof(void) { return sizeof(orc_deck); }
+
+/* Load a deck (native layout) into reference device order.  0 on success. */
+int orc_deck_load(const char *root, orc_deck *d) {
+    memset(d, 0, sizeof *d);
+    int dummy = 0;
+    int *t3[] = {&d->mdt, &d->ndays, &d->ntoutput};
+    if (read_scalars_i(root, "BINFOR/TIME.DAT", 3, t3)) return -1;
+    int *g2[] = {&d->nod, &d->cells};
+    if (read_scalars_i(root, "BINFOR/GIRD.DAT", 2, g2)) return -1;
+    {
+        reader r;
+        if (rd_open(&r, root, "BINFOR/DEPTH.DAT")) return -1;
+        char *ln = rd_line(&r); if (!ln || !next_d(&ln, &d->hm1)) { rd_close(&r); return -1; }
+        ln = rd_line(&r); if (!ln || !next_d(&ln, &d->hm2)) { rd_close(&r); return -1; }
+        rd_close(&r);
+    }
+    int *b6[] = {&d->nz, &d->nq, &d->nzq, &d->nhq, &d->nwe, &d->ndi};
+    if (read_scalars_i(root, "BINFOR/BOUNDARY.DAT", 6, b6)) return -1;
+    {
+        reader r;
+        if (rd_open(&r, root, "BINFOR/CALTIME.DAT")) return -1;
+        char *ln = rd_line(&r); if (!ln || !next_i(&ln, &dummy)) { rd_close(&r); return -1; }
+        ln = rd_line(&r); if (!ln || !next_d(&ln, &d->dt)) { rd_close(&r); return -1; }
+        rd_close(&r);
+        if (rd_open(&r, root, "BINFOR/JL.DAT")) return -1;
+        ln = rd_line(&r); if (!ln || !next_d(&ln, &d->jl)) { rd_close(&r); return -1; }
+        rd_close(&r);
+    }
+    const int C = d->cells, S = 4 * C;
+    if (C <= 0 || d->nod <= 0) return -1;
+    d->nac = zalloc(sizeof(double) * S); d->klas = zalloc(sizeof(double) * S);
+    d->side = zalloc(sizeof(double) * S); d->cosf = zalloc(sizeof(double) * S);
+    d->sinf = zalloc(sizeof(double) * S); d->slcos = zalloc(sizeof(double) * S);
+    d->slsin = zalloc(sizeof(double) * S);
+    d->f0 = zalloc(sizeof(double) * S); d->f1 = zalloc(sizeof(double) * S);
+    d->f2 = zalloc(sizeof(double) * S); d->f3 = zalloc(sizeof(double) * S);
+    d->h = zalloc(sizeof(double) * C); d->u = zalloc(sizeof(double) * C);
+    d->v = zalloc(sizeof(double) * C); d->z = zalloc(sizeof(double) * C);
+    d->w = zalloc(sizeof(double) * C); d->zbc = zalloc(sizeof(double) * C);
+    d->zb1 = zalloc(sizeof(double) * C); d->area = zalloc(sizeof(double) * C);
+    d->fnc = zalloc(sizeof(double) * C); d->bfeat = zalloc(sizeof(double) * C);
+    d->nhq1 = zalloc(sizeof(int) * C);
+    d->zw = zalloc(sizeof(double) * (size_t)C * d->nhq); d->qw = zalloc(sizeof(double) * (size_t)C * d->nhq);
+    size_t CD = (size_t)C * (size_t)d->ndays;
+    d->qt = zalloc(sizeof(double) * CD); d->dqt = zalloc(sizeof(double) * CD);
+    d->zt = zalloc(sizeof(double) * CD); d->dzt = zalloc(sizeof(double) * CD);
+
+    int *nap = zalloc(sizeof(int) * S);
+    double *xp = zalloc(sizeof(double) * d->nod), *yp = zalloc(sizeof(double) * d->nod);
+    double *fnc0 = zalloc(sizeof(double) * C);
+    double *mbz = zalloc(sizeof(double) * (d->nz + 1)), *nnz = zalloc(sizeof(double) * (d->nz + 1));
+    double *mbq = zalloc(sizeof(double) * (d->nq + 1)), *nnq = zalloc(sizeof(double) * (d->nq + 1));
+    double *mbzq = zalloc(sizeof(double) * (d->nzq + 1)), *nnzq = zalloc(sizeof(double) * (d->nzq + 1));
+    int nnz0 = 0, nnq0 = 0, nnzq0 = 0, nwe = 0;
+    int rc = 0;
+    rc |= read_cell4(root, "SOURCES/PNAC.DAT", C, d->nac, NULL);
+    rc |= read_cell4(root, "SOURCES/PNAP.DAT", C, NULL, nap);
+    rc |= read_cell4(root, "SOURCES/PKLAS.DAT", C, d->klas, NULL);
+    rc |= read_col(root, "SOURCES/PZBC.DAT", C, d->zbc);
+    {
+        reader r;
+        if (rd_open(&r, root, "SOURCES/PXY.DAT")) rc = -1;
+        else {
+            rd_line(&r);
+            for (int i = 0; i < d->nod; i++) {
+                char *ln = rd_line(&r);
+                if (!ln) break;
+                int no;
+                if (!next_i(&ln, &no)) continue;
+                next_d(&ln, &xp[i]);
+                next_d(&ln, &yp[i]);
+            }
+            rd_close(&r);
+        }
+    }
+    rc |= read_groups(root, "SOURCES/MBZ.DAT", d->nz, &nnz0, mbz, nnz);
+    rc |= read_groups(root, "SOURCES/MBQ.DAT", d->nq, &nnq0, mbq, nnq);
+    /* MBW.DAT: its first line overrides NWE (mesh.cpp:178-197) */
+    double *mbw = NULL, *topw = NULL;
+    {
+        reader r;
+        if (rd_open(&r, root, "SOURCES/MBW.DAT")) rc = -1;
+        else {
+            char *ln = rd_line(&r);
+            if (ln) next_i(&ln, &nwe);
+            d->nwe = nwe;
+            mbw = zalloc(sizeof(double) * (nwe + 1)); topw = zalloc(sizeof(double) * (nwe + 1));
+            for (int i = 0; i < nwe; i++) {
+                ln = rd_line(&r);
+                if (!ln) break;
+                int no;
+                if (!next_i(&ln, &no)) continue;
+                next_d(&ln, &mbw[i]);
+                next_d(&ln, &topw[i]);
+            }
+            rd_close(&r);
+        }
+    }
+    rc |= read_groups(root, "SOURCES/MBZQ.DAT", d->nzq, &nnzq0, mbzq, nnzq);
+    rc |= read_col(root, "BINFOR/INITIALLEVEL.DAT", C, d->z);
+    rc |= read_col(root, "BINFOR/INITIALU1.DAT", C, d->u);
+    rc |= read_col(root, "BINFOR/INITIALV1.DAT", C, d->v);
+    rc |= read_col(root, "BINFOR/CV.DAT", C, fnc0);
+    if (rc) goto fail;
+
+    /* ---- geometry, mesh.cpp:280-372 ---- */
+    {
+        double ximin = xp[0], yimin = yp[0];
+        for (int i = 1; i < d->nod; i++) { if (xp[i] < ximin) ximin = xp[i]; if (yp[i] < yimin) yimin = yp[i]; }
+        for (int i = 0; i < d->nod; i++) { xp[i] -= ximin; yp[i] -= yimin; }
+        int *nv = zalloc(sizeof(int) * C);
+        for (int i = 0; i < C; i++) {
+            const int *np = nap + 4 * i;
+            if (np[0] == 0) continue;
+            d->zb1[i] = d->zbc[i] + d->hm1;
+            nv[i] = (np[3] == 0 || np[3] == np[0]) ? 3 : 4;
+            for (int j = 0; j < nv[i]; j++)
+                if (np[j] < 1 || np[j] > d->nod) { free(nv); goto fail; }
+            double x1 = xp[np[0] - 1], x2 = xp[np[1] - 1], x3 = xp[np[2] - 1];
+            double y1 = yp[np[0] - 1], y2 = yp[np[1] - 1], y3 = yp[np[2] - 1];
+            d->area[i] = fabs(((y3 - y1) * (x2 - x1) - (x3 - x1) * (y2 - y1)) / 2.0);
+            if (nv[i] == 4) {
+                double x4 = xp[np[3] - 1], y4 = yp[np[3] - 1];
+                d->area[i] += fabs(((y4 - y1) * (x3 - x1) - (x4 - x1) * (y3 - y1)) / 2.0);
+            }
+            for (int j = 0; j < nv[i]; j++) {
+                int n1 = np[j] - 1, n2 = np[(j + 1) % nv[i]] - 1;
+                double dx = xp[n1] - xp[n2];
+                double dy = yp[n2] - yp[n1];
+                int s = 4 * i + j;
+                d->side[s] = sqrt(dx * dx + dy * dy);
+                if (d->side[s] > 0.0) {
+                    d->sinf[s] = dx / d->side[s];
+                    d->cosf[s] = dy / d->side[s];
+                }
+            }
+        }
+        for (int i = 0; i < C; i++) d->zb1[i] = d->zbc[i] + d->hm1;
+        for (int i = 0; i < C; i++) {
+            if (nap[4 * i] == 0) continue;
+            if (d->z[i] <= d->zbc[i]) { d->h[i] = d->hm1; d->z[i] = d->zb1[i]; }
+            else d->h[i] = d->z[i] - d->zbc[i];
+        }
+        for (int i = 0; i < C; i++) {
+            d->fnc[i] = 9.81 * fnc0[i] * fnc0[i];
+            for (int j = 0; j < nv[i]; j++) {
+                int s = 4 * i + j;
+                d->slcos[s] = d->side[s] * d->cosf[s];
+                d->slsin[s] = d->side[s] * d->sinf[s];
+            }
+        }
+        free(nv);
+    }
+
+    /* ---- boundary tables, mesh.cpp:374-521, relaid as in cell.cpp:93-128 ---- */
+    {
+        const int ND = d->ndays, NZ = d->nz, NQ = d->nq;
+        double *ZT = zalloc(sizeof(double) * (size_t)(NZ + 1) * ND), *QT = zalloc(sizeof(double) * (size_t)(NQ + 1) * ND);
+        char rel[256];
+        for (int k = 1; k <= nnz0; k++) {
+            series s;
+            snprintf(rel, sizeof rel, "BOUNDE/NZ/NZ%04d.DAT", k);
+            if (read_series(root, rel, &s, 0)) { free(ZT); free(QT); goto fail; }
+            for (int i = 0; i < ND; i++) {
+                double st = 0 + i / (24.0 * 3600.0 / d->mdt);
+                float zt = (float)boundary_interp(st, &s);
+                for (int j = 0; j < NZ; j++)
+                    if (nnz[j] == k) ZT[(size_t)j * ND + i] = zt;
+            }
+            free(s.t); free(s.v);
+        }
+        for (int k = 1; k <= nnq0; k++) {
+            series s;
+            snprintf(rel, sizeof rel, "BOUNDE/NQ/NQ%04d.DAT", k);
+            if (read_series(root, rel, &s, 0)) { free(ZT); free(QT); goto fail; }
+            int kl = 0;
+            for (int j = 1; j <= NQ; j++) if (k == nnq[j - 1]) kl++;
+            for (int i = 0; i < ND; i++) {
+                double st = 0 + i / (24.0 * 3600.0 / d->mdt);
+                float qt = (float)boundary_interp(st, &s);
+                for (int j = 0; j < NQ; j++)
+                    if (nnq[j] == k) QT[(size_t)j * ND + i] = (double)(qt / (float)kl);
+            }
+            free(s.t); free(s.v);
+        }
+        int K0 = (int)(d->mdt / d->dt);
+        for (int i = 0; i < NQ; i++) {
+            int pos = (int)mbq[i] - 1;
+            if (pos < 0 || pos >= C) continue;
+            for (int jt = 0; jt < ND; jt++) {
+                d->qt[(size_t)jt * C + pos] = QT[(size_t)i * ND + jt];
+                d->dqt[(size_t)jt * C + pos] = (jt != ND - 1) ? (QT[(size_t)i * ND + jt + 1] - QT[(size_t)i * ND + jt]) / K0 : 0.0;
+            }
+        }
+        for (int i = 0; i < NZ; i++) {
+            int pos = (int)mbz[i] - 1;
+            if (pos < 0 || pos >= C) continue;
+            for (int jt = 0; jt < ND; jt++) {
+                d->zt[(size_t)jt * C + pos] = ZT[(size_t)i * ND + jt];
+                d->dzt[(size_t)jt * C + pos] = (jt != ND - 1) ? (ZT[(size_t)i * ND + jt + 1] - ZT[(size_t)i * ND + jt]) / K0 : 0.0;
+            }
+        }
+        free(ZT); free(QT);
+        /* rating curves, mesh.cpp:468-520 */
+        const int NHQ = d->nhq, NZQ = d->nzq;
+        double *ZW = zalloc(sizeof(double) * (size_t)NHQ * (NZQ + 1)), *QW = zalloc(sizeof(double) * (size_t)NHQ * (NZQ + 1));
+        int *NHQ1 = zalloc(sizeof(int) * (NZQ + 1));
+        for (int k = 1; k <= nnzq0; k++) {
+            series s;
+            snprintf(rel, sizeof rel, "BOUNDE/NZQ/NZQ%04d.DAT", k);
+            if (read_series(root, rel, &s, NHQ)) { free(ZW); free(QW); free(NHQ1); goto fail; }
+            double *aqzh0 = zalloc(sizeof(double) * (NZQ + 1)), *aqzh1 = zalloc(sizeof(double) * (NHQ + 1));
+            for (int i = 0; i < s.n && i < NHQ; i++) {
+                for (int j = 0; j < NZQ; j++) {
+                    if (nnzq[j] == k) {
+                        int c = (int)mbzq[j] - 1;
+                        NHQ1[j] = s.n;
+                        for (int jj = 0; jj < 4; jj++) {
+                            int si = c * 4 + jj;
+                            if (d->klas[si] == 3)
+                                aqzh0[j] = fmax(s.t[i] - d->zbc[c], d->hm2) * d->side[si];
+                        }
+                        aqzh1[i] += aqzh0[j];
+                    }
+                }
+                for (int j = 0; j < NZQ; j++) {
+                    if (nnzq[j] == k) {
+                        ZW[(size_t)i * (NZQ + 1) + j] = s.t[i];
+                        QW[(size_t)i * (NZQ + 1) + j] = s.v[i] * aqzh0[j] / aqzh1[i];
+                    }
+                }
+            }
+            free(aqzh0); free(aqzh1); free(s.t); free(s.v);
+        }
+        for (int i = 0; i < NZQ; i++) {
+            int pos = (int)mbzq[i] - 1;
+            if (pos < 0 || pos >= C) continue;
+            for (int j = 0; j < NHQ; j++) {
+                d->zw[(size_t)pos * NHQ + j] = ZW[(size_t)j * (NZQ + 1) + i];
+                d->qw[(size_t)pos * NHQ + j] = QW[(size_t)j * (NZQ + 1) + i];
+            }
+            d->nhq1[pos] = NHQ1[i];
+        }
+        free(ZW); free(QW); free(NHQ1);
+        for (int i = 0; i < nwe; i++) {
+            int pos = (int)mbw[i] - 1;
+            if (pos >= 0 && pos < C) d->bfeat[pos] = topw[i];
+        }
+    }
+    free(nap); free(xp); free(yp); free(fnc0); free(mbz); free(nnz); free(mbq); free(nnq);
+    free(mbzq); free(nnzq); free(mbw); free(topw);
+    return 0;
+fail:
+    free(nap); free(xp); free(yp); free(fnc0); free(mbz); free(nnz); free(mbq); free(nnq);
+    free(mbzq); free(nnzq); free(mbw); free(topw);
+    orc_deck_free(d);
+    return -1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* flux                                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* QF, functors.cu:505-511 */
+static void flux_of(double h, double u, double v, double f[4]) {
+    f[0] = h * u;
+    f[1] = f[0] * u;
+    f[2] = f[0] * v;
+    f[3] = 4.905 * h * h;
+}
+
+static void acc(double out[4], const double f[4], int sign) {
+    for (int i = 0; i < 4; i++) out[i] += f[i] * sign;
+}
+
+/* OSHER with its QS<k> sub-integrals, functors.cu:445-503, 570-712.
+ * Piece 1: left state; 2: left sonic point; 3: intermediate state seen from the
+ * left; 5: intermediate state seen from the right; 6: right sonic point; 7: right
+ * state. Pieces 3 and 5 overwrite FIL / FIR with the state they derive. */
+static void osher(double h_left, const double ql[3], const double qr[3], double fil, double out[4]) {
+    double cr = sqrt(9.81 * qr[0]);
+    double fir = qr[1] - 2 * cr;
+    double ua = (fil + fir) / 2;
+    double ca = fabs((fil - fir) / 4);
+    double cl = sqrt(9.81 * h_left);
+    out[0] = out[1] = out[2] = out[3] = 0;
+    int k2 = 0, k1 = 0;
+    if (ca < ua) k2 = 1;
+    else if (ua >= 0.0 && ua < ca) k2 = 2;
+    else if (ua >= -ca && ua < 0.0) k2 = 3;
+    else if (ua < -ca) k2 = 4;
+    if (ql[1] < cl && qr[1] >= -cr) k1 = 1;
+    else if (ql[1] >= cl && qr[1] >= -cr) k1 = 2;
+    else if (ql[1] < cl && qr[1] < -cr) k1 = 3;
+    else if (ql[1] >= cl && qr[1] < -cr) k1 = 4;
+    /* the pieces each (k1, k2) case sums, with signs (functors.cu:612-711) */
+    static const int plan[4][4][5] = {
+        {{2, 0}, {3, 0}, {5, 0}, {6, 0}},
+        {{1, 0}, {1, -2, 3, 0}, {1, -2, 5, 0}, {1, -2, 6, 0}},
+        {{2, -6, 7, 0}, {3, -6, 7, 0}, {5, -6, 7, 0}, {7, 0}},
+        {{1, -6, 7, 0}, {1, -2, 3, -6, 7}, {1, -2, 5, -6, 7}, {1, -2, 7, 0}},
+    };
+    if (k1 == 0 || k2 == 0) return;
+    const int *p = plan[k1 - 1][k2 - 1];
+    for (int q = 0; q < 5 && p[q] != 0; q++) {
+        int piece = p[q] < 0 ? -p[q] : p[q];
+        int sign = p[q] < 0 ? -1 : 1;
+        double f[4];
+        switch (piece) {
+        case 1: flux_of(ql[0], ql[1], ql[2], f); break;
+        case 2: { double us = fil / 3; double hs = us * us / 9.81; flux_of(hs, us, ql[2], f); } break;
+        case 3: { double ua3 = (fil + fir) / 2; fil = fil - ua3; double ha = fil * fil / 39.24; flux_of(ha, ua3, ql[2], f); } break;
+        case 5: { double ua5 = (fil + fir) / 2; fir = fir - ua5; double ha = fir * fir / 39.24; flux_of(ha, ua5, qr[2], f); } break;
+        case 6: { double us = fir / 3; double hs = us * us / 9.81; flux_of(hs, us, qr[2], f); } break;
+        case 7: flux_of(qr[0], qr[1], qr[2], f); break;
+        default: continue;
+        }
+        acc(out, f, sign);
+    }
+}
+
+/* QD, functors.cu:394-421 */
+static double weir_discharge(double zl, double zr, double zb) {
+    const double CM = 0.384, SIGMA = 0.667, FI = 4.43;
+    double zu = fmax(zl, zr), zd = fmin(zl, zr);
+    double h0 = zu - zb, hs = zd - zb;
+    double delta = hs / h0;
+    if (delta <= SIGMA) return copysign(CM * pow(h0, 1.5), zl - zr);
+    double dh = zu - zd;
+    if (dh > 0.09) return copysign(FI * hs * sqrt(dh), zl - zr);
+    return copysign(FI * hs * 0.3 * dh / 0.1, zl - zr);
+}
+
+/* LAQP, functors.cu:423-443 */
+static void table_lookup(double x, double *y, const double *a, const double *b, int ms) {
+    if (ms <= 0) return;
+    if (x < a[0]) { *y = b[0]; return; }
+    if (x > a[ms - 1]) { *y = b[ms - 1]; return; }
+    for (int i = 0; i < ms - 1; i++)
+        if (x >= a[i] && x <= a[i + 1]) { *y = b[i] + (b[i + 1] - b[i]) / (a[i + 1] - a[i]) * (x - a[i]); return; }
+}
+
+#define F0 d->f0[s]
+#define F1 d->f1[s]
+#define F2 d->f2[s]
+#define F3 d->f3[s]
+
+/* BOUNDA and its KLAS branches, functors.cu:204-392, 513-568 */
+static void boundary_slot(orc_deck *d, int variant, int kt, int jt, int pos, int s,
+                          double h, double u, double v, double zp, double zc, double uc, double vc,
+                          double fil, double ql[3]) {
+    (void)u; (void)v;
+    const int C = d->cells;
+    double cl = sqrt(9.81 * h);
+    int supercritical = variant == ORC_VARIANT_F ? (ql[1] > cl) : (ql[1] > cl && h < d->hm2);
+    if (supercritical) {
+        F0 = h * ql[1];
+        F1 = F0 * ql[1];
+        F2 = F0 * ql[2];
+        F3 = 4.905 * h * h;
+        return;
+    }
+    double hb = 0.0;
+    F2 = 0;
+    if (ql[1] > 0) F2 = h * ql[1] * ql[2];
+    double kp = d->klas[s];
+    if (kp == 10) {
+        size_t t = (size_t)jt * C + pos;
+        F0 = -(d->qt[t] + d->dqt[t] * kt);
+        F0 = F0 / d->side[s];
+        double qb2 = F0 * F0;
+        double hb0 = h;
+        for (int k = 1; k <= 20; k++) {
+            double w = fil - F0 / hb0;
+            hb = w * w / 39.24;
+            if (fabs(hb0 - hb) <= 0.005) break;
+            hb0 = hb0 * 0.5 + hb * 0.5;
+        }
+        F1 = hb <= 1 ? 0 : qb2 / hb;
+        F2 = 0;
+        F3 = 4.905 * hb * hb;
+    } else if (kp == 3) {
+        double q3 = (d->u[pos] * d->cosf[s] + d->v[pos] * d->sinf[s]) * h * d->side[s];
+        q3 = fmax(q3, 0.0);
+        const double *qw = d->qw + (size_t)pos * d->nhq, *zw = d->zw + (size_t)pos * d->nhq;
+        double zq = 0.0;
+        table_lookup(q3, &zq, qw, zw, d->nhq1[pos]);
+        double dzq = zq - zp;
+        double hb1 = fmax(zq - d->zbc[pos], d->hm2);
+        if (q3 <= qw[1] || hb1 <= d->hm2 || dzq >= 0.1) {
+            ql[1] = fmax(ql[1], 0.0);
+            F0 = h * ql[1];
+            F1 = F0 * ql[1];
+            F3 = 4.905 * h * h;
+        } else {
+            ql[1] = fmax(ql[1], 0.0);
+            double fial = ql[1] + 6.264 * sqrt(h);
+            double ur0 = ql[1], urb = ur0;
+            for (int k = 1; k <= 30; k++) {
+                double fiar = urb - 6.264 * sqrt(hb1);
+                urb = (fial + fiar) * (fial - fiar) * (fial - fiar) / hb1 / 313.92;
+                if (fabs(urb - ur0) <= 0.001) break;
+                ur0 = urb;
+            }
+            F0 = hb1 * urb;
+            F1 = F0 * urb;
+            F3 = 4.905 * hb1 * hb1;
+        }
+    } else if (kp == 1) {
+        size_t t = (size_t)jt * C + pos;
+        int mult = variant == ORC_VARIANT_F ? kt : jt;
+        double hb1 = d->zt[t] + d->dzt[t] * mult - d->zbc[pos];
+        hb1 = fmax(hb1, d->hm2);
+        double fial = ql[1] + 6.264 * sqrt(h);
+        double ur0 = ql[1], urb = ur0;
+        for (int k = 1; k <= 30; k++) {
+            double fiar = urb - 6.264 * sqrt(hb1);
+            urb = (fial + fiar) * (fial - fiar) * (fial - fiar) / hb1 / 313.92;
+            if (fabs(urb - ur0) <= 0.0001) break;
+            ur0 = urb;
+        }
+        F0 = hb1 * urb;
+        F1 = F0 * urb;
+        F3 = 4.905 * hb1 * hb1;
+    } else if (kp == 4) {
+        F0 = 0; F1 = 0; F2 = 0;
+        F3 = 4.905 * h * h;
+    } else if (kp == 5) {
+        ql[1] = fmax(ql[1], 0.0);
+        F0 = h * ql[1];
+        F1 = F0 * ql[1];
+        F3 = 4.905 * h * h * (1.0 - d->jl) * (1.0 - d->jl);
+    } else if (kp == 6) {
+        double top = d->bfeat[pos], zb = d->zbc[pos];
+        double cs = d->cosf[s], sn = d->sinf[s];
+        if (zp <= top && zc <= top) {
+            F0 = 0; F1 = 0; F2 = 0; F3 = 4.905 * h * h;
+        } else if (zp > top && zc <= top) {
+            F0 = C0 * pow(zp - top, 1.5);
+            F1 = F0 * ql[1];
+            F2 = F0 * ql[2];
+            F3 = 4.905 * pow(top - zb, 2);
+        } else if (zp <= top && zc > top) {
+            F0 = -C0 * pow(zc - top, 1.5);
+            F1 = F0 * fmin(uc * cs + vc * sn, 0.0);
+            F2 = F0 * (vc * cs - uc * sn);
+            F3 = 4.905 * pow(zp - zb, 2);
+        } else if (zp > top && zc > top) {
+            double dz = fabs(zp - zc);
+            if (zp <= zc) {
+                double hd = zp - top;
+                double un = fmin(uc * cs + vc * sn, 0.0);
+                double vt = vc * cs - uc * sn;
+                double sh = hd + dz;
+                double ce = fmin(1.0, 1.05 * pow(dz / sh, 0.33333));
+                if (zp < zc && un > 0.0) un = 0.0;
+                F0 = copysign(ce * C1 * pow(sh, 1.5), zp - zc);
+                F1 = F0 * fabs(un);
+                F2 = F0 * vt;
+                F3 = 4.905 * pow(top - zb, 2);
+            } else {
+                double hd = zc - top;
+                double un = fmax(ql[1], 0.0);
+                double vt = ql[2];
+                double sh = hd + dz;
+                double ce = fmin(1.0, 1.05 * pow(dz / sh, 0.33333));
+                F0 = copysign(ce * C1 * pow(sh, 1.5), zp - zc);
+                F1 = (zp - zc) * fabs(un) * un;
+                F2 = (zp - zc) * fabs(un) * vt;
+                F3 = 4.905 * pow(top - zb, 2);
+            }
+        }
+    } else if (kp == 7) {
+        double top = d->bfeat[pos];
+        if (zp > top || zc > top) {
+            d->klas[s] = 0;
+            hb = h;   /* uninitialised in the reference; see the header comment */
+            double cq = weir_discharge(zp, zc, top);
+            double cb = BRDTH / d->side[s];
+            F0 = cq * cb;
+            F1 = cb * copysign(cq * cq / hb, cq);
+            F3 = 4.905 * hb * hb;
+        } else {
+            F0 = 0; F1 = 0; F2 = 0;
+            F3 = 4.905 * h * h;
+        }
+    }
+}
+
+/* CalculateFluxKernel body for slot s, functors.cu:47-202 */
+static void flux_slot(orc_deck *d, int variant, int kt, int jt, int s) {
+    const double HM1 = d->hm1, HM2 = d->hm2;
+    int pos = s / 4;
+    double u1 = d->u[pos], v1 = d->v[pos], h1 = d->h[pos], z1 = d->z[pos], zb1 = d->zb1[pos];
+    int nc = (int)(d->nac[s] - 1);
+    double kp = d->klas[s], cs = d->cosf[s], sn = d->sinf[s];
+    double ql[3];
+    ql[0] = h1;
+    ql[1] = u1 * cs + v1 * sn;
+    ql[2] = v1 * cs - u1 * sn;
+    double cl = sqrt(9.81 * h1);
+    double fil = ql[1] + 2 * cl;
+    double zi = fmax(z1, zb1);
+    double hc, bc, zc, uc, vc;
+    if (nc == -1) { hc = 0; bc = 0; zc = 0; uc = 0; vc = 0; }
+    else {
+        hc = fmax(d->h[nc], HM1);
+        bc = d->zbc[nc];
+        zc = fmax(bc, d->z[nc]);
+        uc = d->u[nc];
+        vc = d->v[nc];
+    }
+    if ((kp >= 1 && kp <= 8) || kp >= 10) {
+        boundary_slot(d, variant, kt, jt, pos, s, h1, u1, v1, z1, zc, uc, vc, fil, ql);
+    } else if (h1 <= HM1 && hc <= HM1) {
+        F0 = 0; F1 = 0; F2 = 0; F3 = 0;
+    } else if (zi <= bc) {
+        F0 = -C1 * pow(hc, 1.5); F1 = h1 * ql[1] * fabs(ql[1]); F2 = 0; F3 = 4.905 * h1 * h1;
+    } else if (zc <= d->zbc[pos]) {
+        F0 = C1 * pow(h1, 1.5); F1 = h1 * fabs(ql[1]) * ql[1]; F2 = h1 * fabs(ql[1]) * ql[2]; F3 = 0;
+    } else if (h1 <= HM2) {
+        if (zc > zi) {
+            double dh = fmax(zc - d->zbc[pos], HM1);
+            double un = -C1 * sqrt(dh);
+            F0 = dh * un; F1 = F0 * un; F2 = F0 * (vc * cs - uc * sn); F3 = 4.905 * h1 * h1;
+        } else {
+            F0 = C1 * pow(h1, 1.5); F1 = 0; F2 = 0; F3 = 4.905 * h1 * h1;
+        }
+    } else if (hc <= HM2) {
+        if (zi > zc) {
+            double dh = fmax(zi - bc, HM1);
+            double un = C1 * sqrt(dh);
+            double hc1 = zc - d->zbc[pos];
+            F0 = dh * un; F1 = F0 * un; F2 = F0 * ql[2]; F3 = 4.905 * hc1 * hc1;
+        } else {
+            F0 = -C1 * pow(hc, 1.5); F1 = h1 * ql[1] * ql[1]; F2 = 0; F3 = 4.905 * h1 * h1;
+        }
+    } else if (kp == 0 && pos < nc) {
+        double qr[3], fo[4];
+        qr[0] = fmax(zc - d->zbc[pos], HM1);
+        double ur = uc * cs + vc * sn;
+        qr[1] = ur * fmin(hc / qr[0], 1.5);
+        if (hc <= HM2 || qr[0] <= HM2) qr[1] = copysign(VMIN, ur);
+        qr[2] = vc * cs - uc * sn;
+        osher(h1, ql, qr, fil, fo);
+        F0 = fo[0];
+        F1 = fo[1] + (1 - fmin(hc / qr[0], 1.5)) * hc * ur * ur / 2;
+        F2 = fo[2];
+        F3 = fo[3];
+    } else {
+        /* the neighbour's side of the same edge, seen with the normal reversed */
+        if (nc < 0) { d->error |= 1; F0 = F1 = F2 = F3 = 0; return; }
+        double hc2 = fmax(h1, HM1);
+        double zc1 = fmax(d->zbc[pos], z1);
+        double cs1 = -cs, sn1 = -sn;
+        double cl1 = sqrt(9.81 * d->h[nc]);
+        double ql1[3], qr1[3], fo[4];
+        ql1[0] = d->h[nc];
+        ql1[1] = d->u[nc] * cs1 + d->v[nc] * sn1;
+        ql1[2] = d->v[nc] * cs1 - d->u[nc] * sn1;
+        double fil1 = ql1[1] + 2 * cl1;
+        qr1[0] = fmax(zc1 - d->zbc[nc], HM1);
+        double ur1 = u1 * cs1 + v1 * sn1;
+        qr1[1] = ur1 * fmin(hc2 / qr1[0], 1.5);
+        if (hc2 <= HM2 || qr1[0] <= HM2) qr1[1] = copysign(VMIN, ur1);
+        qr1[2] = v1 * cs1 - u1 * sn1;
+        osher(d->h[nc], ql1, qr1, fil1, fo);
+        F1 = fo[1] + (1 - fmin(hc2 / qr1[0], 1.5)) * hc2 * ur1 * ur1 / 2;
+        F0 = -fo[0];
+        F2 = fo[2];
+        double za = sqrt(fo[3] / 4.905) + bc;
+        double hc3 = 0;
+        if (za > d->zbc[pos]) hc3 = za - d->zbc[pos];
+        F3 = 4.905 * hc3 * hc3;
+    }
+}
+
+void orc_flux(orc_deck *d, int variant, int kt, int jt) {
+    const int S = 4 * d->cells;
+#pragma omp parallel for schedule(static)
+    for (int s = 0; s < S; s++) flux_slot(d, variant, kt, jt, s);
+}
+
+/* UpdateCellKernel, functors.cu:717-784 (variant F: v0 functors.cu:719-803) */
+static void update_cell(orc_deck *d, int variant, int pos) {
+    const double HM1 = d->hm1, HM2 = d->hm2, DT = d->dt;
+    double wh = 0.0, wu = 0.0, wv = 0.0;
+    for (int s = 4 * pos; s < 4 * (pos + 1); s++) {
+        double fr1 = d->f1[s] + d->f3[s];
+        double fr2 = d->f2[s];
+        wh += d->side[s] * d->f0[s];
+        wu += d->slcos[s] * fr1 - d->slsin[s] * fr2;
+        wv += d->slsin[s] * fr1 + d->slcos[s] * fr2;
+    }
+    double h1 = d->h[pos], u1 = d->u[pos], v1 = d->v[pos];
+    double dta;
+    if (variant == ORC_VARIANT_F) {
+        const double *sd = d->side + 4 * pos;
+        double sidex;
+        if (sd[3] > 0.0) sidex = fmin(0.5 * (sd[0] + sd[2]), 0.5 * (sd[1] + sd[3]));
+        else {
+            double ss = 0.5 * (sd[0] + sd[1] + sd[2]);
+            sidex = sqrt((ss - sd[0]) * (ss - sd[1]) * (ss - sd[2]) / ss);
+        }
+        double hside = fmax(h1, HM1);
+        double dt2 = sidex / (u1 + sqrt(9.81 * hside));
+        dt2 = fmin(DT, dt2);
+        dt2 = fmax(dt2, DT / 10.0);
+        dta = dt2 / d->area[pos];
+    } else {
+        dta = 1.0 * DT / (1.0 * d->area[pos]);
+    }
+    double wdta = 1.00 * dta;
+    double cap = variant == ORC_VARIANT_F ? 5.0 : 15.0;
+    double h2 = fmax(h1 - wdta * wh + QLUA, HM1);
+    double z2 = h2 + d->zbc[pos];
+    double u2, v2;
+    if (h2 <= HM1) { u2 = 0.0; v2 = 0.0; }
+    else if (h2 <= HM2) {
+        u2 = copysign(fmin(VMIN, fabs(u1)), u1);
+        v2 = copysign(fmin(VMIN, fabs(v1)), v1);
+    } else {
+        double qx1 = h1 * u1, qy1 = h1 * v1;
+        double dtau = wdta * wu, dtav = wdta * wv;
+        double wsf = d->fnc[pos] * sqrt(u1 * u1 + v1 * v1) / pow(h1, 0.33333);
+        u2 = (qx1 - dtau - DT * wsf * u1) / h2;
+        v2 = (qy1 - dtav - DT * wsf * v1) / h2;
+        u2 = copysign(fmin(fabs(u2), cap), u2);
+        v2 = copysign(fmin(fabs(v2), cap), v2);
+    }
+    d->h[pos] = h2; d->u[pos] = u2; d->v[pos] = v2; d->z[pos] = z2;
+    d->w[pos] = sqrt(u2 * u2 + v2 * v2);
+}
+
+void orc_update(orc_deck *d, int variant) {
+#pragma omp parallel for schedule(static)
+    for (int p = 0; p < d->cells; p++) update_cell(d, variant, p);
+}
+
+/* The driver's day/step loop (benchmark.cu:87-96) from step index `first`
+ * (0 = day 0, kt 1) for `n` steps; returns the number of steps taken. */
+int orc_run(orc_deck *d, int variant, int first, int n) {
+    int spd = (int)(d->mdt / d->dt);
+    if (spd < 2) return 0;
+    int per_day = spd - 1, done = 0;
+    for (int s = first; s < first + n; s++) {
+        int jt = s / per_day, kt = 1 + s % per_day;
+        if (jt >= d->ndays) break;
+        orc_flux(d, variant, kt, jt);
+        orc_update(d, variant);
+        done++;
+    }
+    return done;
+}

@@ -1,0 +1,41 @@
+# Builds the reference's own programs from their sources where they lie, into
+# oracle/_ref/ (git-ignored; travels with the tree to the GPU host).
+#
+#   make -f oracle/ref.mk REF=/root/reference
+#
+# hot-path binaries (the reference's dump/timing driver, cuda_native_impl/benchmark.cu):
+#   ref_h64  cuda_native_impl/{benchmark.cu,hydro-cal-src}                  variant H, fp64
+#   ref_f64  cuda_native_impl/baselines/native_cuda_v0/fp64/...             variant F, fp64
+#   ref_h32  cuda_native_impl/fp32_src/...                                  variant H, fp32
+#   ref_f32  cuda_native_impl/baselines/native_cuda_v0/fp32/...             variant F, fp32
+# with the flags of each tree's build.sh (-O3 -rdc=true, default fmad; only
+# fp32_src/build.sh adds --fmad=false) and -arch=sm_100a in place of sm_80.
+#
+# CPU solver: hydro-cal-fortan/calculate.cpp, g++ -O3, no source change; it
+# reads ./origin/changjiangkou/ relative to its working directory.
+REF ?= /root/reference
+OUT := $(dir $(lastword $(MAKEFILE_LIST)))_ref
+NVCC ?= nvcc
+ARCH ?= sm_100a
+CNI := $(REF)/cuda_native_impl
+
+define ref_bin
+$(OUT)/$(1): $$(wildcard $(2)/benchmark.cu $(2)/hydro-cal-src/src/* $(2)/hydro-cal-src/include/*.hpp $(2)/hydro-cal-src/include/*/*.hpp)
+	@mkdir -p $(OUT)
+	$(NVCC) -O3 -arch=$(ARCH) -rdc=true --std=c++17 $(3) -I$(2)/hydro-cal-src/include \
+	    $(2)/benchmark.cu $(2)/hydro-cal-src/src/functors.cu $(2)/hydro-cal-src/src/mesh.cpp \
+	    $(2)/hydro-cal-src/src/cell.cpp $(2)/hydro-cal-src/src/side.cpp -o $$@ -lcudadevrt
+endef
+
+all: $(OUT)/ref_h64 $(OUT)/ref_f64 $(OUT)/ref_h32 $(OUT)/ref_f32 $(OUT)/calculate
+
+$(eval $(call ref_bin,ref_h64,$(CNI),))
+$(eval $(call ref_bin,ref_f64,$(CNI)/baselines/native_cuda_v0/fp64,))
+$(eval $(call ref_bin,ref_h32,$(CNI)/fp32_src,--fmad=false))
+$(eval $(call ref_bin,ref_f32,$(CNI)/baselines/native_cuda_v0/fp32,))
+
+$(OUT)/calculate: $(REF)/hydro-cal-fortan/calculate.cpp
+	@mkdir -p $(OUT)
+	g++ -O3 -std=c++17 -w -I$(REF)/hydro-cal-fortan $< -o $@
+
+.PHONY: all
