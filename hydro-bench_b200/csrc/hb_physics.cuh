@@ -1,0 +1,636 @@
+// hb_physics.cuh -- the per-slot flux and per-cell update of hydro-cal.
+//
+// Follows cuda_native_impl/hydro-cal-src/src/functors.cu (variant H) and
+// cuda_native_impl/baselines/native_cuda_v0/fp64/hydro-cal-src/src/functors.cu
+// (variant F); each function cites the lines it follows.
+//
+// Rounding.  The fp64 policy (F64Exact) evaluates every operation with an
+// explicit IEEE intrinsic (__dmul_rn, __dadd_rn, __fma_rn, __ddiv_rn,
+// __dsqrt_rn), so the compiler cannot fuse anything on its own.  Where the
+// reference build fuses a multiply into an add (nvcc's default -fmad=true),
+// the same fusion is written out here: the `mode` arguments of dot() and
+// madd() name which product is fused.  The modes were established by
+// matching the reference binary's own dumps bit for bit; with them the
+// kernels below reproduce the reference's fp64 results exactly no matter
+// how they are scheduled or fused into larger kernels.  pow() is CUDA's own.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace hb {
+
+// ---------------------------------------------------------------------------
+// constants (common.hpp:44-52, functors.cu)
+// ---------------------------------------------------------------------------
+struct K {
+    static constexpr double C0 = 1.33, C1 = 1.7, VMIN = 0.001, QLUA = 0.0, BRDTH = 100.0;
+};
+
+// boundary-code categories; every double KLAS value maps to one of them
+// without changing behaviour (functors.cu:109, :151, :532-565)
+enum SlotCode : int8_t {
+    CODE_ZERO = 0,        // KLAS == 0: interior chain, direct Osher from the lower-numbered side
+    CODE_K1 = 1, CODE_K3 = 3, CODE_K4 = 4, CODE_K5 = 5, CODE_K6 = 6, CODE_K7 = 7, CODE_K10 = 10,
+    CODE_BOUNDA_OTHER = 2,    // in [1,8] or >= 10 but none of the above: only FLUX2 is written
+    CODE_NONZERO_INTERIOR = 9 // not a boundary code and not 0 (e.g. 9, NaN): mirrored Osher
+};
+
+__host__ __device__ inline int8_t klas_code(double kp) {
+    if ((kp >= 1 && kp <= 8) || kp >= 10) {
+        if (kp == 10) return CODE_K10;
+        if (kp == 3) return CODE_K3;
+        if (kp == 1) return CODE_K1;
+        if (kp == 4) return CODE_K4;
+        if (kp == 5) return CODE_K5;
+        if (kp == 6) return CODE_K6;
+        if (kp == 7) return CODE_K7;
+        return CODE_BOUNDA_OTHER;
+    }
+    return kp == 0 ? CODE_ZERO : CODE_NONZERO_INTERIOR;
+}
+__host__ __device__ inline bool code_is_bounda(int8_t c) { return c != CODE_ZERO && c != CODE_NONZERO_INTERIOR; }
+
+// ---------------------------------------------------------------------------
+// arithmetic policies
+// ---------------------------------------------------------------------------
+struct F64Exact {
+    using real = double;
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+    static __device__ __forceinline__ double sqrt(double a) { return __dsqrt_rn(a); }
+    static __device__ __forceinline__ double pow(double a, double b) { return ::pow(a, b); }
+    static __device__ __forceinline__ double fmax(double a, double b) { return ::fmax(a, b); }
+    static __device__ __forceinline__ double fmin(double a, double b) { return ::fmin(a, b); }
+    static __device__ __forceinline__ double fabs(double a) { return ::fabs(a); }
+    static __device__ __forceinline__ double copysign(double a, double b) { return ::copysign(a, b); }
+    static __device__ __forceinline__ double c(double v) { return v; }
+    // a*b + c*d; mode 0 rounds both products, 1 fuses a*b, 2 fuses c*d
+    static __device__ __forceinline__ double dot(double a, double b, double c, double d, int mode) {
+        return mode == 1 ? __fma_rn(a, b, __dmul_rn(c, d))
+             : mode == 2 ? __fma_rn(c, d, __dmul_rn(a, b))
+                         : __dadd_rn(__dmul_rn(a, b), __dmul_rn(c, d));
+    }
+    // c + a*b; mode 0 rounds the product, otherwise fused
+    static __device__ __forceinline__ double madd(double a, double b, double c, int mode) {
+        return mode ? __fma_rn(a, b, c) : __dadd_rn(c, __dmul_rn(a, b));
+    }
+};
+
+struct F32Fast {
+    using real = float;
+    static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
+    static __device__ __forceinline__ float add(float a, float b) { return a + b; }
+    static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+    static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return fmaf(a, b, c); }
+    static __device__ __forceinline__ float sqrt(float a) { return sqrtf(a); }
+    static __device__ __forceinline__ float pow(float a, float b) { return powf(a, b); }
+    static __device__ __forceinline__ float fmax(float a, float b) { return fmaxf(a, b); }
+    static __device__ __forceinline__ float fmin(float a, float b) { return fminf(a, b); }
+    static __device__ __forceinline__ float fabs(float a) { return fabsf(a); }
+    static __device__ __forceinline__ float copysign(float a, float b) { return copysignf(a, b); }
+    static __device__ __forceinline__ float c(double v) { return (float)v; }
+    static __device__ __forceinline__ float dot(float a, float b, float c, float d, int) { return fmaf(a, b, c * d); }
+    static __device__ __forceinline__ float madd(float a, float b, float c, int) { return fmaf(a, b, c); }
+};
+
+// Fusion modes of the reference sm_100a build (see file comment).
+enum : int {
+    M_QL1 = 2, M_QL2 = 1, M_UR = 1, M_QR2 = 1,          // functors.cu:90-91, :153, :158
+    M_QL1M = 2, M_QL2M = 2, M_UR1 = 2, M_QR2M = 1,      // :176-177, :181, :186
+    M_ACC0 = 0, M_ACC123 = 1,                           // Osher sums, :453-497
+    M_SHALLOW_VT = 1,                                   // :130
+    M_K10 = 1, M_K1 = 1, M_FIAL1 = 1, M_FIAR1 = 1,      // :209, :376, :379, :383
+    M_K3Q = 1, M_FIAL3 = 1, M_FIAR3 = 1, M_LAQP = 1,    // :327, :355, :359, :439
+    M_K6UN = 1, M_K6VT = 1,                             // :280-281, :293-294
+    M_WH = 1, M_WU = 1, M_WV = 2,                       // :739-741
+    M_H2 = 1, M_U2A = 1, M_U2B = 1, M_SQ1 = 1, M_SQ2 = 1 // :754, :771-772, :770, :777
+};
+
+// ---------------------------------------------------------------------------
+// inputs / outputs of one slot
+// ---------------------------------------------------------------------------
+template <class R>
+struct CellState { R h, u, v, z, zbc; };
+
+template <class R>
+struct SlotIn {
+    CellState<R> own;       // H1, U1, V1, Z1 and ZBC of the slot's cell
+    CellState<R> nb;        // raw H, U, V, Z, ZBC of the neighbour (unused when has_nb == false)
+    bool has_nb;            // NAC != 0
+    bool own_first;         // pos < NC in the reference numbering
+    int8_t code;            // klas_code(KLAS)
+    R cosj, sinj, side;     // COSF, SINF, SIDE of the slot
+};
+
+// boundary tables at (jt, pos), fetched only for boundary slots
+template <class R>
+struct BoundaryIn {
+    R qt, dqt, zt, dzt, top;        // QT, DQT, ZT, DZT at [jt][pos]; BoundaryFeature[pos]
+    const R *zw, *qw;               // rating-curve row of the cell
+    int nhq1;                       // points used (NHQ1[pos])
+    int nhq;                        // row width (NHQ)
+};
+
+template <class R>
+struct SlotOut {
+    R f[4];
+    uint8_t mask;        // bit i set: FLUX<i> written this step (otherwise keeps its old value)
+    bool klas_to_zero;   // a breach slot opened (functors.cu:242)
+    bool undefined;      // reached the reference's read of H[-1] (functors.cu:170)
+};
+
+struct StepParams {
+    double hm1, hm2, jl, dt;
+    int kt, jt;
+};
+
+// ---------------------------------------------------------------------------
+// Osher approximate Riemann solver, functors.cu:445-511, :570-712
+// ---------------------------------------------------------------------------
+// out += sign * QF(h, u, v) with the reference build's sums (functors.cu:453-497, :505-511)
+template <class A>
+__device__ __forceinline__ void qf_acc(typename A::real out[4], typename A::real h, typename A::real u,
+                                       typename A::real v, int sign) {
+    using R = typename A::real;
+    R f0 = A::mul(h, u);
+    R sh = sign > 0 ? h : -h;
+    R sf0 = sign > 0 ? f0 : -f0;
+    out[0] = A::madd(sh, u, out[0], M_ACC0);
+    out[1] = A::madd(sf0, u, out[1], M_ACC123);
+    out[2] = A::madd(sf0, v, out[2], M_ACC123);
+    R h4 = A::mul(A::c(4.905), h);
+    out[3] = A::madd(sign > 0 ? h4 : -h4, h, out[3], M_ACC123);
+}
+
+// the sub-integrals QS<1..7> (QS<4> adds nothing)
+template <class A, int PIECE>
+__device__ __forceinline__ void qs(typename A::real out[4], const typename A::real ql[3], const typename A::real qr[3],
+                                   typename A::real &fil, typename A::real &fir, int sign) {
+    using R = typename A::real;
+    if constexpr (PIECE == 1) {
+        qf_acc<A>(out, ql[0], ql[1], ql[2], sign);
+    } else if constexpr (PIECE == 2) {
+        R us = A::div(fil, A::c(3.0));
+        R hs = A::div(A::mul(us, us), A::c(9.81));
+        qf_acc<A>(out, hs, us, ql[2], sign);
+    } else if constexpr (PIECE == 3) {
+        R ua = A::mul(A::add(fil, fir), A::c(0.5));
+        fil = A::sub(fil, ua);
+        R ha = A::div(A::mul(fil, fil), A::c(39.24));
+        qf_acc<A>(out, ha, ua, ql[2], sign);
+    } else if constexpr (PIECE == 5) {
+        R ua = A::mul(A::add(fil, fir), A::c(0.5));
+        fir = A::sub(fir, ua);
+        R ha = A::div(A::mul(fir, fir), A::c(39.24));
+        qf_acc<A>(out, ha, ua, qr[2], sign);
+    } else if constexpr (PIECE == 6) {
+        R us = A::div(fir, A::c(3.0));
+        R hs = A::div(A::mul(us, us), A::c(9.81));
+        qf_acc<A>(out, hs, us, qr[2], sign);
+    } else if constexpr (PIECE == 7) {
+        qf_acc<A>(out, qr[0], qr[1], qr[2], sign);
+    }
+}
+
+// OSHER(pos, H_pre, QL, QR, FIL, FLR_OSHER); `cl` is sqrt(9.81*h_left), the
+// same value the reference recomputes at :577.
+template <class A>
+__device__ __forceinline__ void osher(typename A::real cl, const typename A::real ql[3],
+                                      const typename A::real qr[3], typename A::real fil,
+                                      typename A::real out[4]) {
+    using R = typename A::real;
+    R cr = A::sqrt(A::mul(A::c(9.81), qr[0]));
+    R fir = A::sub(qr[1], A::mul(A::c(2.0), cr));
+    R ua = A::mul(A::add(fil, fir), A::c(0.5));
+    R ca = A::fabs(A::mul(A::sub(fil, fir), A::c(0.25)));
+    out[0] = out[1] = out[2] = out[3] = R(0);
+    int k2 = 0, k1 = 0;
+    if (ca < ua) k2 = 1;
+    else if (ua >= R(0) && ua < ca) k2 = 2;
+    else if (ua >= -ca && ua < R(0)) k2 = 3;
+    else if (ua < -ca) k2 = 4;
+    if (ql[1] < cl && qr[1] >= -cr) k1 = 1;
+    else if (ql[1] >= cl && qr[1] >= -cr) k1 = 2;
+    else if (ql[1] < cl && qr[1] < -cr) k1 = 3;
+    else if (ql[1] >= cl && qr[1] < -cr) k1 = 4;
+    switch (k1 * 4 + k2) {
+    case 5: qs<A, 2>(out, ql, qr, fil, fir, 1); break;
+    case 6: qs<A, 3>(out, ql, qr, fil, fir, 1); break;
+    case 7: qs<A, 5>(out, ql, qr, fil, fir, 1); break;
+    case 8: qs<A, 6>(out, ql, qr, fil, fir, 1); break;
+    case 9: qs<A, 1>(out, ql, qr, fil, fir, 1); break;
+    case 10: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 3>(out, ql, qr, fil, fir, 1); break;
+    case 11: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 5>(out, ql, qr, fil, fir, 1); break;
+    case 12: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 6>(out, ql, qr, fil, fir, 1); break;
+    case 13: qs<A, 2>(out, ql, qr, fil, fir, 1); qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
+    case 14: qs<A, 3>(out, ql, qr, fil, fir, 1); qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
+    case 15: qs<A, 5>(out, ql, qr, fil, fir, 1); qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
+    case 16: qs<A, 7>(out, ql, qr, fil, fir, 1); break;
+    case 17: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
+    case 18: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 3>(out, ql, qr, fil, fir, 1);
+             qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
+    case 19: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 5>(out, ql, qr, fil, fir, 1);
+             qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
+    case 20: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
+    default: break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// boundary slots: BOUNDA and the KLAS branches, functors.cu:204-443, :513-568
+// ---------------------------------------------------------------------------
+// QD, functors.cu:394-421
+template <class A>
+__device__ __forceinline__ typename A::real weir_discharge(typename A::real zl, typename A::real zr, typename A::real zb) {
+    using R = typename A::real;
+    R zu = A::fmax(zl, zr), zd = A::fmin(zl, zr);
+    R h0 = A::sub(zu, zb), hs = A::sub(zd, zb);
+    R delta = A::div(hs, h0);
+    if (delta <= A::c(0.667)) return A::copysign(A::mul(A::c(0.384), A::pow(h0, A::c(1.5))), A::sub(zl, zr));
+    R dh = A::sub(zu, zd);
+    if (dh > A::c(0.09)) return A::copysign(A::mul(A::mul(A::c(4.43), hs), A::sqrt(dh)), A::sub(zl, zr));
+    return A::copysign(A::div(A::mul(A::mul(A::mul(A::c(4.43), hs), A::c(0.3)), dh), A::c(0.1)), A::sub(zl, zr));
+}
+
+// LAQP, functors.cu:423-443: y(x) by linear interpolation in the table (a -> b)
+template <class A>
+__device__ __forceinline__ void table_lookup(typename A::real x, typename A::real &y, const typename A::real *a,
+                                             const typename A::real *b, int ms) {
+    if (ms <= 0) return;
+    if (x < a[0]) { y = b[0]; return; }
+    if (x > a[ms - 1]) { y = b[ms - 1]; return; }
+    for (int i = 0; i < ms - 1; i++) {
+        if (x >= a[i] && x <= a[i + 1]) {
+            y = A::madd(A::div(A::sub(b[i + 1], b[i]), A::sub(a[i + 1], a[i])), A::sub(x, a[i]), b[i], M_LAQP);
+            return;
+        }
+    }
+}
+
+// Riemann-invariant iteration of KLAS 1 / 3 (functors.cu:355-367, :379-391)
+template <class A>
+__device__ __forceinline__ typename A::real invariant_iter(typename A::real ql1, typename A::real h,
+                                                           typename A::real hb1, double tol, int mfial, int mfiar) {
+    using R = typename A::real;
+    R fial = A::madd(A::c(6.264), A::sqrt(h), ql1, mfial);
+    R ur0 = ql1, urb = ur0;
+    R shb = A::sqrt(hb1);
+    for (int k = 1; k <= 30; k++) {
+        R fiar = A::madd(A::c(-6.264), shb, urb, mfiar);
+        R dsum = A::add(fial, fiar), ddif = A::sub(fial, fiar);
+        urb = A::div(A::div(A::mul(A::mul(dsum, ddif), ddif), hb1), A::c(313.92));
+        if (A::fabs(A::sub(urb, ur0)) <= A::c(tol)) break;
+        ur0 = urb;
+    }
+    return urb;
+}
+
+template <class A, int VARIANT, class TableFetch>
+__device__ __forceinline__ void bounda(const SlotIn<typename A::real> &in, const StepParams &p, typename A::real fil,
+                                       typename A::real ql[3], typename A::real zc, typename A::real uc,
+                                       typename A::real vc, const TableFetch &fetch, SlotOut<typename A::real> &o) {
+    using R = typename A::real;
+    const R h = in.own.h;
+    const R hm2 = A::c(p.hm2);
+    R cl = A::sqrt(A::mul(A::c(9.81), h));
+    bool super = (VARIANT == 1) ? (ql[1] > cl) : (ql[1] > cl && h < hm2);
+    if (super) {
+        o.f[0] = A::mul(h, ql[1]);
+        o.f[1] = A::mul(o.f[0], ql[1]);
+        o.f[2] = A::mul(o.f[0], ql[2]);
+        o.f[3] = A::mul(A::mul(A::c(4.905), h), h);
+        o.mask = 0xF;
+        return;
+    }
+    o.f[2] = R(0);
+    if (ql[1] > R(0)) o.f[2] = A::mul(A::mul(h, ql[1]), ql[2]);
+    o.mask = 0x4;
+    switch (in.code) {
+    case CODE_K10: {
+        BoundaryIn<R> b = fetch();
+        R f0 = -A::madd(b.dqt, A::c((double)p.kt), b.qt, M_K10);
+        f0 = A::div(f0, in.side);
+        R qb2 = A::mul(f0, f0);
+        R hb0 = h, hb = R(0);
+        for (int k = 1; k <= 20; k++) {
+            R w = A::sub(fil, A::div(f0, hb0));
+            hb = A::div(A::mul(w, w), A::c(39.24));
+            if (A::fabs(A::sub(hb0, hb)) <= A::c(0.005)) break;
+            hb0 = A::add(A::mul(hb0, A::c(0.5)), A::mul(hb, A::c(0.5)));
+        }
+        o.f[0] = f0;
+        o.f[1] = hb <= R(1) ? R(0) : A::div(qb2, hb);
+        o.f[2] = R(0);
+        o.f[3] = A::mul(A::mul(A::c(4.905), hb), hb);
+        o.mask = 0xF;
+        break;
+    }
+    case CODE_K3: {
+        BoundaryIn<R> b = fetch();
+        R q3 = A::mul(A::mul(A::dot(in.own.u, in.cosj, in.own.v, in.sinj, M_K3Q), h), in.side);
+        q3 = A::fmax(q3, R(0));
+        R zq = R(0);   // the reference leaves ZQH1 unset when the cell has no table (NHQ1 = 0)
+        table_lookup<A>(q3, zq, b.qw, b.zw, b.nhq1);
+        R dzq = A::sub(zq, in.own.z);
+        R hb1 = A::fmax(A::sub(zq, in.own.zbc), hm2);
+        R qw1 = b.nhq > 1 ? b.qw[1] : R(0);   // QW_row[1] (functors.cu:347)
+        ql[1] = A::fmax(ql[1], R(0));
+        if (q3 <= qw1 || hb1 <= hm2 || dzq >= A::c(0.1)) {
+            o.f[0] = A::mul(h, ql[1]);
+            o.f[1] = A::mul(o.f[0], ql[1]);
+            o.f[3] = A::mul(A::mul(A::c(4.905), h), h);
+        } else {
+            R urb = invariant_iter<A>(ql[1], h, hb1, 0.001, M_FIAL3, M_FIAR3);
+            o.f[0] = A::mul(hb1, urb);
+            o.f[1] = A::mul(o.f[0], urb);
+            o.f[3] = A::mul(A::mul(A::c(4.905), hb1), hb1);
+        }
+        o.mask = 0xF;
+        break;
+    }
+    case CODE_K1: {
+        BoundaryIn<R> b = fetch();
+        int mult = VARIANT == 1 ? p.kt : p.jt;
+        R hb1 = A::sub(A::madd(b.dzt, A::c((double)mult), b.zt, M_K1), in.own.zbc);
+        hb1 = A::fmax(hb1, hm2);
+        R urb = invariant_iter<A>(ql[1], h, hb1, 0.0001, M_FIAL1, M_FIAR1);
+        o.f[0] = A::mul(hb1, urb);
+        o.f[1] = A::mul(o.f[0], urb);
+        o.f[3] = A::mul(A::mul(A::c(4.905), hb1), hb1);
+        o.mask = 0xF;
+        break;
+    }
+    case CODE_K4:
+        o.f[0] = R(0); o.f[1] = R(0); o.f[2] = R(0);
+        o.f[3] = A::mul(A::mul(A::c(4.905), h), h);
+        o.mask = 0xF;
+        break;
+    case CODE_K5: {
+        ql[1] = A::fmax(ql[1], R(0));
+        o.f[0] = A::mul(h, ql[1]);
+        o.f[1] = A::mul(o.f[0], ql[1]);
+        R omj = A::sub(A::c(1.0), A::c(p.jl));
+        o.f[3] = A::mul(A::mul(A::mul(A::mul(A::c(4.905), h), h), omj), omj);
+        o.mask = 0xF;
+        break;
+    }
+    case CODE_K6: {   // CalculataKlas6, functors.cu:258-318
+        BoundaryIn<R> b = fetch();
+        const R top = b.top, zb = in.own.zbc, zp = in.own.z;
+        const R cs = in.cosj, sn = in.sinj;
+        if (zp <= top && zc <= top) {
+            o.f[0] = R(0); o.f[1] = R(0); o.f[2] = R(0);
+            o.f[3] = A::mul(A::mul(A::c(4.905), h), h);
+        } else if (zp > top && zc <= top) {
+            o.f[0] = A::mul(A::c(K::C0), A::pow(A::sub(zp, top), A::c(1.5)));
+            o.f[1] = A::mul(o.f[0], ql[1]);
+            o.f[2] = A::mul(o.f[0], ql[2]);
+            o.f[3] = A::mul(A::c(4.905), A::pow(A::sub(top, zb), A::c(2.0)));
+        } else if (zp <= top && zc > top) {
+            o.f[0] = A::mul(A::c(-K::C0), A::pow(A::sub(zc, top), A::c(1.5)));
+            o.f[1] = A::mul(o.f[0], A::fmin(A::dot(uc, cs, vc, sn, M_K6UN), R(0)));
+            o.f[2] = A::mul(o.f[0], A::dot(vc, cs, -uc, sn, M_K6VT));
+            o.f[3] = A::mul(A::c(4.905), A::pow(A::sub(zp, zb), A::c(2.0)));
+        } else if (zp > top && zc > top) {
+            R dz = A::fabs(A::sub(zp, zc));
+            if (zp <= zc) {
+                R hd = A::sub(zp, top);
+                R un = A::fmin(A::dot(uc, cs, vc, sn, M_K6UN), R(0));
+                R vt = A::dot(vc, cs, -uc, sn, M_K6VT);
+                R sh = A::add(hd, dz);
+                R ce = A::fmin(A::c(1.0), A::mul(A::c(1.05), A::pow(A::div(dz, sh), A::c(0.33333))));
+                if (zp < zc && un > R(0)) un = R(0);
+                o.f[0] = A::copysign(A::mul(A::mul(ce, A::c(K::C1)), A::pow(sh, A::c(1.5))), A::sub(zp, zc));
+                o.f[1] = A::mul(o.f[0], A::fabs(un));
+                o.f[2] = A::mul(o.f[0], vt);
+                o.f[3] = A::mul(A::c(4.905), A::pow(A::sub(top, zb), A::c(2.0)));
+            } else {
+                R hd = A::sub(zc, top);
+                R un = A::fmax(ql[1], R(0));
+                R vt = ql[2];
+                R sh = A::add(hd, dz);
+                R ce = A::fmin(A::c(1.0), A::mul(A::c(1.05), A::pow(A::div(dz, sh), A::c(0.33333))));
+                o.f[0] = A::copysign(A::mul(A::mul(ce, A::c(K::C1)), A::pow(sh, A::c(1.5))), A::sub(zp, zc));
+                R dzs = A::sub(zp, zc);
+                o.f[1] = A::mul(A::mul(dzs, A::fabs(un)), un);
+                o.f[2] = A::mul(A::mul(dzs, A::fabs(un)), vt);
+                o.f[3] = A::mul(A::c(4.905), A::pow(A::sub(top, zb), A::c(2.0)));
+            }
+        }
+        o.mask = 0xF;
+        break;
+    }
+    case CODE_K7: {   // CalculateKlas7, functors.cu:234-256
+        BoundaryIn<R> b = fetch();
+        const R top = b.top, zp = in.own.z;
+        if (zp > top || zc > top) {
+            o.klas_to_zero = true;
+            // The reference reads an uninitialised HB here (functors.cu:246-247); the
+            // cell's own depth is used instead.
+            R hb = h;
+            R cq = weir_discharge<A>(zp, zc, top);
+            R cb = A::div(A::c(K::BRDTH), in.side);
+            o.f[0] = A::mul(cq, cb);
+            o.f[1] = A::mul(cb, A::copysign(A::div(A::mul(cq, cq), hb), cq));
+            o.f[3] = A::mul(A::mul(A::c(4.905), hb), hb);
+        } else {
+            o.f[0] = R(0); o.f[1] = R(0); o.f[2] = R(0);
+            o.f[3] = A::mul(A::mul(A::c(4.905), h), h);
+        }
+        o.mask = 0xF;
+        break;
+    }
+    default:   // codes the reference does not handle: only FLUX2 (functors.cu:525-565)
+        break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CalculateFluxKernel body for one slot, functors.cu:47-202
+// `cl_own` is sqrt(9.81*H) of the slot's cell (the caller may compute it once
+// per cell; it is bit-identical to the reference's per-slot value).
+// ---------------------------------------------------------------------------
+template <class A, int VARIANT, class TableFetch>
+__device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, typename A::real cl_own,
+                                          const StepParams &p, const TableFetch &fetch,
+                                          SlotOut<typename A::real> &o) {
+    using R = typename A::real;
+    o.mask = 0xF; o.klas_to_zero = false; o.undefined = false;
+    const R HM1 = A::c(p.hm1), HM2 = A::c(p.hm2);
+    const R h1 = in.own.h, u1 = in.own.u, v1 = in.own.v, z1 = in.own.z, zbc1 = in.own.zbc;
+    const R cs = in.cosj, sn = in.sinj;
+    R ql[3];
+    ql[0] = h1;
+    ql[1] = A::dot(u1, cs, v1, sn, M_QL1);
+    ql[2] = A::dot(v1, cs, -u1, sn, M_QL2);
+    R fil = A::add(ql[1], A::mul(A::c(2.0), cl_own));
+    R zi = A::fmax(z1, A::add(zbc1, HM1));
+    R hc, bc, zc, uc, vc;
+    if (!in.has_nb) { hc = R(0); bc = R(0); zc = R(0); uc = R(0); vc = R(0); }
+    else {
+        hc = A::fmax(in.nb.h, HM1);
+        bc = in.nb.zbc;
+        zc = A::fmax(bc, in.nb.z);
+        uc = in.nb.u;
+        vc = in.nb.v;
+    }
+    if (code_is_bounda(in.code)) {
+        bounda<A, VARIANT>(in, p, fil, ql, zc, uc, vc, fetch, o);
+    } else if (h1 <= HM1 && hc <= HM1) {
+        o.f[0] = R(0); o.f[1] = R(0); o.f[2] = R(0); o.f[3] = R(0);
+    } else if (zi <= bc) {
+        o.f[0] = A::mul(A::c(-K::C1), A::pow(hc, A::c(1.5)));
+        o.f[1] = A::mul(A::mul(h1, ql[1]), A::fabs(ql[1]));
+        o.f[2] = R(0);
+        o.f[3] = A::mul(A::mul(A::c(4.905), h1), h1);
+    } else if (zc <= zbc1) {
+        o.f[0] = A::mul(A::c(K::C1), A::pow(h1, A::c(1.5)));
+        R ha = A::mul(h1, A::fabs(ql[1]));
+        o.f[1] = A::mul(ha, ql[1]);
+        o.f[2] = A::mul(ha, ql[2]);
+        o.f[3] = R(0);
+    } else if (h1 <= HM2) {
+        if (zc > zi) {
+            R dh = A::fmax(A::sub(zc, zbc1), HM1);
+            R un = A::mul(A::c(-K::C1), A::sqrt(dh));
+            o.f[0] = A::mul(dh, un);
+            o.f[1] = A::mul(o.f[0], un);
+            o.f[2] = A::mul(o.f[0], A::dot(vc, cs, -uc, sn, M_SHALLOW_VT));
+            o.f[3] = A::mul(A::mul(A::c(4.905), h1), h1);
+        } else {
+            o.f[0] = A::mul(A::c(K::C1), A::pow(h1, A::c(1.5)));
+            o.f[1] = R(0); o.f[2] = R(0);
+            o.f[3] = A::mul(A::mul(A::c(4.905), h1), h1);
+        }
+    } else if (hc <= HM2) {
+        if (zi > zc) {
+            R dh = A::fmax(A::sub(zi, bc), HM1);
+            R un = A::mul(A::c(K::C1), A::sqrt(dh));
+            R hc1 = A::sub(zc, zbc1);
+            o.f[0] = A::mul(dh, un);
+            o.f[1] = A::mul(o.f[0], un);
+            o.f[2] = A::mul(o.f[0], ql[2]);
+            o.f[3] = A::mul(A::mul(A::c(4.905), hc1), hc1);
+        } else {
+            o.f[0] = A::mul(A::c(-K::C1), A::pow(hc, A::c(1.5)));
+            o.f[1] = A::mul(A::mul(h1, ql[1]), ql[1]);
+            o.f[2] = R(0);
+            o.f[3] = A::mul(A::mul(A::c(4.905), h1), h1);
+        }
+    } else if (in.code == CODE_ZERO && in.own_first) {
+        // direct Osher across the edge (functors.cu:151-164)
+        R qr[3], fo[4];
+        qr[0] = A::fmax(A::sub(zc, zbc1), HM1);
+        R ur = A::dot(uc, cs, vc, sn, M_UR);
+        R ratio = A::fmin(A::div(hc, qr[0]), A::c(1.5));
+        qr[1] = A::mul(ur, ratio);
+        if (hc <= HM2 || qr[0] <= HM2) qr[1] = A::copysign(A::c(K::VMIN), ur);
+        qr[2] = A::dot(vc, cs, -uc, sn, M_QR2);
+        osher<A>(cl_own, ql, qr, fil, fo);
+        o.f[0] = fo[0];
+        o.f[1] = A::add(fo[1], A::mul(A::mul(A::mul(A::mul(A::sub(A::c(1.0), ratio), hc), ur), ur), A::c(0.5)));
+        o.f[2] = fo[2];
+        o.f[3] = fo[3];
+    } else {
+        // the same edge seen from the neighbour, normal reversed (functors.cu:165-200)
+        if (!in.has_nb) {
+            o.undefined = true;
+            o.f[0] = R(0); o.f[1] = R(0); o.f[2] = R(0); o.f[3] = R(0);
+            return;
+        }
+        const R hn = in.nb.h, un_ = in.nb.u, vn = in.nb.v;
+        R hc2 = A::fmax(h1, HM1);
+        R zc1 = A::fmax(zbc1, z1);
+        R cs1 = -cs, sn1 = -sn;
+        R ql1[3], qr1[3], fo[4];
+        ql1[0] = hn;
+        ql1[1] = A::dot(un_, cs1, vn, sn1, M_QL1M);
+        ql1[2] = A::dot(vn, cs1, -un_, sn1, M_QL2M);
+        const R cl_nb = A::sqrt(A::mul(A::c(9.81), hn));
+        R fil1 = A::add(ql1[1], A::mul(A::c(2.0), cl_nb));
+        qr1[0] = A::fmax(A::sub(zc1, bc), HM1);
+        R ur1 = A::dot(u1, cs1, v1, sn1, M_UR1);
+        R ratio = A::fmin(A::div(hc2, qr1[0]), A::c(1.5));
+        qr1[1] = A::mul(ur1, ratio);
+        if (hc2 <= HM2 || qr1[0] <= HM2) qr1[1] = A::copysign(A::c(K::VMIN), ur1);
+        qr1[2] = A::dot(v1, cs1, -u1, sn1, M_QR2M);
+        osher<A>(cl_nb, ql1, qr1, fil1, fo);
+        o.f[1] = A::add(fo[1], A::mul(A::mul(A::mul(A::mul(A::sub(A::c(1.0), ratio), hc2), ur1), ur1), A::c(0.5)));
+        o.f[0] = -fo[0];
+        o.f[2] = fo[2];
+        R za = A::add(A::sqrt(A::div(fo[3], A::c(4.905))), bc);
+        R hc3 = R(0);
+        if (za > zbc1) hc3 = A::sub(za, zbc1);
+        o.f[3] = A::mul(A::mul(A::c(4.905), hc3), hc3);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// UpdateCellKernel body, functors.cu:717-784 (variant F: v0 functors.cu:719-803)
+// ---------------------------------------------------------------------------
+template <class R>
+struct CellUpdateIn {
+    R h, u, v, zbc, fnc;
+    R dta_or_area;     // variant H: DT/AREA; variant F: AREA
+    R sidex;           // variant F: the CFL length of the cell (v0 functors.cu:752-763)
+};
+template <class R>
+struct CellUpdateOut { R h, u, v, z, w; };
+
+// accumulate slot j's contribution (functors.cu:732-742), in slot order
+template <class A>
+__device__ __forceinline__ void wsum_add(typename A::real &wh, typename A::real &wu, typename A::real &wv,
+                                         typename A::real f0, typename A::real f1, typename A::real f2,
+                                         typename A::real f3, typename A::real side, typename A::real slcos,
+                                         typename A::real slsin) {
+    using R = typename A::real;
+    R fr1 = A::add(f1, f3);
+    R fr2 = f2;
+    wh = A::madd(side, f0, wh, M_WH);
+    wu = A::add(wu, A::dot(slcos, fr1, -slsin, fr2, M_WU));
+    wv = A::add(wv, A::dot(slsin, fr1, slcos, fr2, M_WV));
+}
+
+template <class A, int VARIANT>
+__device__ __forceinline__ CellUpdateOut<typename A::real> update_cell(const CellUpdateIn<typename A::real> &c,
+                                                                      typename A::real wh, typename A::real wu,
+                                                                      typename A::real wv, const StepParams &p) {
+    using R = typename A::real;
+    const R HM1 = A::c(p.hm1), HM2 = A::c(p.hm2), DT = A::c(p.dt);
+    R dta;
+    if (VARIANT == 1) {
+        R hside = A::fmax(c.h, HM1);
+        R dt2 = A::div(c.sidex, A::add(c.u, A::sqrt(A::mul(A::c(9.81), hside))));
+        dt2 = A::fmin(DT, dt2);
+        dt2 = A::fmax(dt2, A::div(DT, A::c(10.0)));
+        dta = A::div(dt2, c.dta_or_area);
+    } else {
+        dta = c.dta_or_area;
+    }
+    const R cap = A::c(VARIANT == 1 ? 5.0 : 15.0);
+    CellUpdateOut<R> o;
+    o.h = A::fmax(A::add(A::madd(-dta, wh, c.h, M_H2), A::c(K::QLUA)), HM1);
+    o.z = A::add(o.h, c.zbc);
+    if (o.h <= HM1) {
+        o.u = R(0); o.v = R(0);
+    } else if (o.h <= HM2) {
+        o.u = A::copysign(A::fmin(A::c(K::VMIN), A::fabs(c.u)), c.u);
+        o.v = A::copysign(A::fmin(A::c(K::VMIN), A::fabs(c.v)), c.v);
+    } else {
+        R wsf = A::div(A::mul(c.fnc, A::sqrt(A::dot(c.u, c.u, c.v, c.v, M_SQ1))), A::pow(c.h, A::c(0.33333)));
+        R dtw = A::mul(DT, wsf);
+        R u2 = A::div(A::madd(-dtw, c.u, A::dot(c.h, c.u, -dta, wu, M_U2A), M_U2B), o.h);
+        R v2 = A::div(A::madd(-dtw, c.v, A::dot(c.h, c.v, -dta, wv, M_U2A), M_U2B), o.h);
+        o.u = A::copysign(A::fmin(A::fabs(u2), cap), u2);
+        o.v = A::copysign(A::fmin(A::fabs(v2), cap), v2);
+    }
+    o.w = A::sqrt(A::dot(o.u, o.u, o.v, o.v, M_SQ2));
+    return o;
+}
+
+}  // namespace hb

@@ -1,0 +1,128 @@
+/*
+ * hydrob200.h -- C ABI of the B200 shallow-water timestep library.
+ *
+ * Replaces the hot path of hydro-bench's hydro-cal solver: the per-edge flux
+ * (CalculateFlux, cuda_native_impl/hydro-cal-src/src/functors.cu:787-792 and
+ * :802-809) and the per-cell update (UpdateCell, functors.cu:794-799 and
+ * :811-818) driven by the day/step loop of cuda_native_impl/benchmark.cu:87-96.
+ * Every call returns an hb_status; nothing calls exit() (the reference's
+ * CUDA_CHECK does, common.hpp:57-59).
+ *
+ * Arrays crossing this boundary are in the reference's own order and types:
+ * per cell [CELL], per slot [4*CELL] with slot = 4*cell + j, per cell and day
+ * [NDAYS*CELL] with index day*CELL + cell, rating tables [CELL*NHQ]
+ * (cell.cpp:93-128).  The handle keeps its own renumbered copy on the device.
+ */
+#ifndef HYDROB200_H
+#define HYDROB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    HB_OK = 0,
+    HB_E_INVALID = 1,          /* bad argument */
+    HB_E_BADMESH = 2,          /* mesh arrays inconsistent (neighbour index out of range, ...) */
+    HB_E_CUDA = 3,             /* a CUDA call failed; hb_last_error_string() says which */
+    HB_E_NONFINITE = 4,        /* a step produced NaN/Inf depth or velocity */
+    HB_E_BARRIER_TIMEOUT = 5,  /* the persistent kernel's grid barrier gave up waiting */
+    HB_E_IO = 6,               /* a deck file could not be read */
+    HB_E_UNDEFINED_REF = 7,    /* a slot reached reference behaviour that reads undefined memory */
+    HB_E_NOMEM = 8,
+    HB_E_TOO_LARGE = 9         /* size beyond a fixed capacity */
+} hb_status;
+
+typedef enum { HB_VARIANT_H = 0, HB_VARIANT_F = 1 } hb_variant;
+typedef enum { HB_FP64 = 0, HB_FP32 = 1, HB_SPLIT = 2 } hb_precision;
+
+/* Host description of a mesh and its boundary tables, reference layout.
+ * Mirrors what MeshView/CellView/SideView hold after FromHost
+ * (mesh.hpp:114-141, cell.hpp:28-61, side.hpp:29-52). */
+typedef struct hb_mesh_desc {
+    int32_t cells;            /* CELL */
+    int32_t ndays;            /* NDAYS: rows of the qt/dqt/zt/dzt tables */
+    int32_t nhq;              /* NHQ: columns of zw/qw */
+    int32_t steps_per_day;    /* MDT / DT (benchmark.cu:55); the loop runs kt = 1..steps_per_day-1 */
+    double dt, hm1, hm2, jl;  /* DT, HM1, HM2, JL */
+    const double *nac;        /* [4C] 1-based neighbour, 0 = none (stored as double, side.hpp:34) */
+    const double *klas;       /* [4C] boundary code (double, side.hpp:32) */
+    const double *side, *cosf, *sinf, *slcos, *slsin;   /* [4C] */
+    const double *zbc, *zb1, *area, *fnc, *bfeat;       /* [C]; bfeat = BoundaryFeature (weir crest) */
+    const int32_t *nhq1;      /* [C] rating-curve points used per cell */
+    const double *zw, *qw;    /* [C*NHQ] */
+    const double *qt, *dqt, *zt, *dzt;                   /* [NDAYS*C] */
+} hb_mesh_desc;
+
+typedef struct hb_handle hb_handle;
+
+typedef struct hb_options {
+    int32_t variant;          /* hb_variant */
+    int32_t precision;        /* hb_precision */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t renumber;         /* 1: reverse Cuthill-McKee cell order on the device (default), 0: input order */
+    int32_t block_cells;      /* cells per CTA of the step kernel (0 = autotuned default) */
+    int32_t reserved[3];
+} hb_options;
+
+/* Default options: variant H, fp64, device 0, renumbered. */
+void hb_options_default(hb_options *opt);
+
+/* Copy the mesh to the device (renumbered) and set the state to zero.
+ * Replaces MeshView construction (benchmark.cu:52 -> cell.cpp:11-146, side.cpp:11-52). */
+int hb_create(const hb_mesh_desc *mesh, const hb_options *opt, hb_handle **out);
+int hb_destroy(hb_handle *h);
+
+/* State in reference order, fp64 host arrays of [CELL]. W may be NULL. */
+int hb_set_state(hb_handle *h, const double *H, const double *U, const double *V, const double *Z, const double *W);
+int hb_get_state(hb_handle *h, double *H, double *U, double *V, double *Z, double *W);
+/* The per-slot fluxes left by the last step, [4*CELL] each, and the current
+ * boundary codes (KLAS=7 slots turn into 0 once breached, functors.cu:242). */
+int hb_get_flux(hb_handle *h, double *F0, double *F1, double *F2, double *F3);
+int hb_get_klas(hb_handle *h, double *klas);
+
+/* Advance nsteps steps of the reference driver loop from its current
+ * position (day jt, step kt); the first call starts at jt = 0, kt = 1.
+ * `stream` is a cudaStream_t (NULL = the legacy default stream).  Returns
+ * once the work is queued; hb_sync waits and reports device-side faults. */
+int hb_step(hb_handle *h, int32_t nsteps, void *stream);
+int hb_sync(hb_handle *h, void *stream);
+/* Current position: steps taken so far, and the (kt, jt) of the next step. */
+int hb_position(hb_handle *h, int64_t *steps_done, int32_t *kt, int32_t *jt);
+int hb_set_position(hb_handle *h, int64_t steps_done);
+
+/* Capture nsteps steps as one CUDA graph owned by the handle; each replay
+ * (hb_graph_launch) advances the boundary-table time like hb_step would. */
+int hb_capture_graph(hb_handle *h, int32_t nsteps, void *stream);
+int hb_graph_launch(hb_handle *h, void *stream);
+
+/* Device-resident state pointers (renumbered order) for zero-copy use from
+ * PyTorch: H, U, V, Z, W as fp64 [CELL] (fp32 for HB_FP32). */
+int hb_device_state(hb_handle *h, void **H, void **U, void **V, void **Z, void **W);
+/* Renumbering: perm[new] = old (cell ids, 0-based). */
+int hb_get_permutation(hb_handle *h, int32_t *perm);
+/* Sticky device error word (bit set of hb_status codes seen by kernels). */
+int hb_device_errors(hb_handle *h, uint32_t *bits);
+
+int hb_last_error(void);
+const char *hb_last_error_string(void);
+const char *hb_status_string(int status);
+
+/* ---- deck reader (cuda_native_impl/hydro-cal-src/src/mesh.cpp:5-533, cell.cpp:72-128) ---- */
+typedef struct hb_deck hb_deck;
+/* Read a hydro-cal text deck (BINFOR/, SOURCES/, BOUNDE/ under `root`). */
+int hb_deck_load(const char *root, hb_deck **out);
+/* Borrow the deck's mesh description (valid until hb_deck_free) and its
+ * initial state (H, U, V, Z, W after preCalculate). */
+int hb_deck_mesh(const hb_deck *d, hb_mesh_desc *mesh);
+int hb_deck_state(const hb_deck *d, const double **H, const double **U, const double **V,
+                  const double **Z, const double **W);
+int hb_deck_free(hb_deck *d);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

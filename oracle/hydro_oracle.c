@@ -45,6 +45,55 @@
 /* functors.cu / common.hpp:44-52 */
 static const double C0 = 1.33, C1 = 1.7, VMIN = 0.001, QLUA = 0.0, BRDTH = 100.0;
 
+/*
+ * Rounding pattern.  nvcc contracts a*b+c into one fused multiply-add where
+ * its heuristics allow, which changes the last bit.  Each expression whose
+ * result depends on that choice has an id below; its mode says how the
+ * reference's sm_100a build evaluates it:
+ *   0  every product rounded, then added
+ *   1  the first product of a*b + c*d (or a*b + c) fused into the add
+ *   2  the second product fused
+ * The defaults were found by matching the reference's own step-1 dumps
+ * (tests/golden) bit for bit; orc_set_pattern(-1, 0) restores plain
+ * round-every-operation arithmetic.
+ */
+enum {
+    P_QL1, P_QL2,                         /* U*cos + V*sin, V*cos - U*sin of the cell (functors.cu:90-91) */
+    P_UR, P_QR2,                          /* neighbour rotation, direct Osher (:153, :158) */
+    P_QL1M, P_QL2M, P_UR1, P_QR2M,        /* mirrored Osher (:176-177, :181, :186) */
+    P_ACC0, P_ACC123,                     /* Osher sums: F0 and F1..F3 (:453-497) */
+    P_SHALLOW_VT,                         /* VC*cos - UC*sin, shallow branch (:130) */
+    P_K10, P_K1, P_FIAL1, P_FIAR1,        /* KLAS 10 / 1 (:209, :376, :379, :383) */
+    P_K3Q, P_FIAL3, P_FIAR3, P_LAQP,      /* KLAS 3 (:327, :355, :359, :439) */
+    P_K6UN, P_K6VT,                       /* KLAS 6 normal / tangential (:280-281, :293-294) */
+    P_WH, P_WU, P_WV,                     /* UpdateCell sums (:739-741) */
+    P_H2, P_U2A, P_U2B, P_SQ1, P_SQ2,     /* UpdateCell (:754, :771-772, :770, :777) */
+    P_COUNT
+};
+static int pat[P_COUNT] = {
+    [P_QL1] = 2, [P_QL2] = 1, [P_UR] = 1, [P_QR2] = 1,
+    [P_QL1M] = 2, [P_QL2M] = 2, [P_UR1] = 2, [P_QR2M] = 1,
+    [P_ACC0] = 0, [P_ACC123] = 1,
+};
+
+void orc_set_pattern(int id, int mode) {
+    if (id < 0) { for (int k = 0; k < P_COUNT; k++) pat[k] = mode; return; }
+    if (id < P_COUNT) pat[id] = mode;
+}
+int orc_get_pattern(int id) { return (id >= 0 && id < P_COUNT) ? pat[id] : -1; }
+int orc_pattern_count(void) { return P_COUNT; }
+
+/* a*b + c*d under pattern mode m */
+static inline double dot2(double a, double b, double c, double d, int m) {
+    if (m == 1) return fma(a, b, c * d);
+    if (m == 2) return fma(c, d, a * b);
+    return a * b + c * d;
+}
+/* c + a*b under pattern mode m (m != 0 fuses) */
+static inline double madd(double a, double b, double c, int m) {
+    return m ? fma(a, b, c) : c + a * b;
+}
+
 typedef struct orc_deck {
     int cells, nod, ndays, mdt, nz, nq, nzq, nhq, nwe, ndi, ntoutput;
     double dt, hm1, hm2, jl;
@@ -478,16 +527,13 @@ fail:
 /* flux                                                                      */
 /* ------------------------------------------------------------------------ */
 
-/* QF, functors.cu:505-511 */
-static void flux_of(double h, double u, double v, double f[4]) {
-    f[0] = h * u;
-    f[1] = f[0] * u;
-    f[2] = f[0] * v;
-    f[3] = 4.905 * h * h;
-}
-
-static void acc(double out[4], const double f[4], int sign) {
-    for (int i = 0; i < 4; i++) out[i] += f[i] * sign;
+/* out += sign * QF(h, u, v) with the reference build's fused sums */
+static void acc_qf(double out[4], double h, double u, double v, int sign) {
+    double f0 = h * u;
+    out[0] = madd(sign * h, u, out[0], pat[P_ACC0]);
+    out[1] = madd(sign * f0, u, out[1], pat[P_ACC123]);
+    out[2] = madd(sign * f0, v, out[2], pat[P_ACC123]);
+    out[3] = madd(sign * (4.905 * h), h, out[3], pat[P_ACC123]);
 }
 
 /* OSHER with its QS<k> sub-integrals, functors.cu:445-503, 570-712.
@@ -522,17 +568,15 @@ static void osher(double h_left, const double ql[3], const double qr[3], double 
     for (int q = 0; q < 5 && p[q] != 0; q++) {
         int piece = p[q] < 0 ? -p[q] : p[q];
         int sign = p[q] < 0 ? -1 : 1;
-        double f[4];
         switch (piece) {
-        case 1: flux_of(ql[0], ql[1], ql[2], f); break;
-        case 2: { double us = fil / 3; double hs = us * us / 9.81; flux_of(hs, us, ql[2], f); } break;
-        case 3: { double ua3 = (fil + fir) / 2; fil = fil - ua3; double ha = fil * fil / 39.24; flux_of(ha, ua3, ql[2], f); } break;
-        case 5: { double ua5 = (fil + fir) / 2; fir = fir - ua5; double ha = fir * fir / 39.24; flux_of(ha, ua5, qr[2], f); } break;
-        case 6: { double us = fir / 3; double hs = us * us / 9.81; flux_of(hs, us, qr[2], f); } break;
-        case 7: flux_of(qr[0], qr[1], qr[2], f); break;
+        case 1: acc_qf(out, ql[0], ql[1], ql[2], sign); break;
+        case 2: { double us = fil / 3; double hs = us * us / 9.81; acc_qf(out, hs, us, ql[2], sign); } break;
+        case 3: { double ua3 = (fil + fir) / 2; fil = fil - ua3; double ha = fil * fil / 39.24; acc_qf(out, ha, ua3, ql[2], sign); } break;
+        case 5: { double ua5 = (fil + fir) / 2; fir = fir - ua5; double ha = fir * fir / 39.24; acc_qf(out, ha, ua5, qr[2], sign); } break;
+        case 6: { double us = fir / 3; double hs = us * us / 9.81; acc_qf(out, hs, us, qr[2], sign); } break;
+        case 7: acc_qf(out, qr[0], qr[1], qr[2], sign); break;
         default: continue;
         }
-        acc(out, f, sign);
     }
 }
 
@@ -554,7 +598,7 @@ static void table_lookup(double x, double *y, const double *a, const double *b, 
     if (x < a[0]) { *y = b[0]; return; }
     if (x > a[ms - 1]) { *y = b[ms - 1]; return; }
     for (int i = 0; i < ms - 1; i++)
-        if (x >= a[i] && x <= a[i + 1]) { *y = b[i] + (b[i + 1] - b[i]) / (a[i + 1] - a[i]) * (x - a[i]); return; }
+        if (x >= a[i] && x <= a[i + 1]) { *y = madd((b[i + 1] - b[i]) / (a[i + 1] - a[i]), x - a[i], b[i], pat[P_LAQP]); return; }
 }
 
 #define F0 d->f0[s]
@@ -583,7 +627,7 @@ static void boundary_slot(orc_deck *d, int variant, int kt, int jt, int pos, int
     double kp = d->klas[s];
     if (kp == 10) {
         size_t t = (size_t)jt * C + pos;
-        F0 = -(d->qt[t] + d->dqt[t] * kt);
+        F0 = -madd(d->dqt[t], (double)kt, d->qt[t], pat[P_K10]);
         F0 = F0 / d->side[s];
         double qb2 = F0 * F0;
         double hb0 = h;
@@ -597,7 +641,7 @@ static void boundary_slot(orc_deck *d, int variant, int kt, int jt, int pos, int
         F2 = 0;
         F3 = 4.905 * hb * hb;
     } else if (kp == 3) {
-        double q3 = (d->u[pos] * d->cosf[s] + d->v[pos] * d->sinf[s]) * h * d->side[s];
+        double q3 = dot2(d->u[pos], d->cosf[s], d->v[pos], d->sinf[s], pat[P_K3Q]) * h * d->side[s];
         q3 = fmax(q3, 0.0);
         const double *qw = d->qw + (size_t)pos * d->nhq, *zw = d->zw + (size_t)pos * d->nhq;
         double zq = 0.0;
@@ -611,10 +655,10 @@ static void boundary_slot(orc_deck *d, int variant, int kt, int jt, int pos, int
             F3 = 4.905 * h * h;
         } else {
             ql[1] = fmax(ql[1], 0.0);
-            double fial = ql[1] + 6.264 * sqrt(h);
+            double fial = madd(6.264, sqrt(h), ql[1], pat[P_FIAL3]);
             double ur0 = ql[1], urb = ur0;
             for (int k = 1; k <= 30; k++) {
-                double fiar = urb - 6.264 * sqrt(hb1);
+                double fiar = madd(-6.264, sqrt(hb1), urb, pat[P_FIAR3]);
                 urb = (fial + fiar) * (fial - fiar) * (fial - fiar) / hb1 / 313.92;
                 if (fabs(urb - ur0) <= 0.001) break;
                 ur0 = urb;
@@ -626,12 +670,12 @@ static void boundary_slot(orc_deck *d, int variant, int kt, int jt, int pos, int
     } else if (kp == 1) {
         size_t t = (size_t)jt * C + pos;
         int mult = variant == ORC_VARIANT_F ? kt : jt;
-        double hb1 = d->zt[t] + d->dzt[t] * mult - d->zbc[pos];
+        double hb1 = madd(d->dzt[t], (double)mult, d->zt[t], pat[P_K1]) - d->zbc[pos];
         hb1 = fmax(hb1, d->hm2);
-        double fial = ql[1] + 6.264 * sqrt(h);
+        double fial = madd(6.264, sqrt(h), ql[1], pat[P_FIAL1]);
         double ur0 = ql[1], urb = ur0;
         for (int k = 1; k <= 30; k++) {
-            double fiar = urb - 6.264 * sqrt(hb1);
+            double fiar = madd(-6.264, sqrt(hb1), urb, pat[P_FIAR1]);
             urb = (fial + fiar) * (fial - fiar) * (fial - fiar) / hb1 / 313.92;
             if (fabs(urb - ur0) <= 0.0001) break;
             ur0 = urb;
@@ -659,15 +703,15 @@ static void boundary_slot(orc_deck *d, int variant, int kt, int jt, int pos, int
             F3 = 4.905 * pow(top - zb, 2);
         } else if (zp <= top && zc > top) {
             F0 = -C0 * pow(zc - top, 1.5);
-            F1 = F0 * fmin(uc * cs + vc * sn, 0.0);
-            F2 = F0 * (vc * cs - uc * sn);
+            F1 = F0 * fmin(dot2(uc, cs, vc, sn, pat[P_K6UN]), 0.0);
+            F2 = F0 * dot2(vc, cs, -uc, sn, pat[P_K6VT]);
             F3 = 4.905 * pow(zp - zb, 2);
         } else if (zp > top && zc > top) {
             double dz = fabs(zp - zc);
             if (zp <= zc) {
                 double hd = zp - top;
-                double un = fmin(uc * cs + vc * sn, 0.0);
-                double vt = vc * cs - uc * sn;
+                double un = fmin(dot2(uc, cs, vc, sn, pat[P_K6UN]), 0.0);
+                double vt = dot2(vc, cs, -uc, sn, pat[P_K6VT]);
                 double sh = hd + dz;
                 double ce = fmin(1.0, 1.05 * pow(dz / sh, 0.33333));
                 if (zp < zc && un > 0.0) un = 0.0;
@@ -713,8 +757,8 @@ static void flux_slot(orc_deck *d, int variant, int kt, int jt, int s) {
     double kp = d->klas[s], cs = d->cosf[s], sn = d->sinf[s];
     double ql[3];
     ql[0] = h1;
-    ql[1] = u1 * cs + v1 * sn;
-    ql[2] = v1 * cs - u1 * sn;
+    ql[1] = dot2(u1, cs, v1, sn, pat[P_QL1]);
+    ql[2] = dot2(v1, cs, -u1, sn, pat[P_QL2]);
     double cl = sqrt(9.81 * h1);
     double fil = ql[1] + 2 * cl;
     double zi = fmax(z1, zb1);
@@ -739,7 +783,7 @@ static void flux_slot(orc_deck *d, int variant, int kt, int jt, int s) {
         if (zc > zi) {
             double dh = fmax(zc - d->zbc[pos], HM1);
             double un = -C1 * sqrt(dh);
-            F0 = dh * un; F1 = F0 * un; F2 = F0 * (vc * cs - uc * sn); F3 = 4.905 * h1 * h1;
+            F0 = dh * un; F1 = F0 * un; F2 = F0 * dot2(vc, cs, -uc, sn, pat[P_SHALLOW_VT]); F3 = 4.905 * h1 * h1;
         } else {
             F0 = C1 * pow(h1, 1.5); F1 = 0; F2 = 0; F3 = 4.905 * h1 * h1;
         }
@@ -755,10 +799,10 @@ static void flux_slot(orc_deck *d, int variant, int kt, int jt, int s) {
     } else if (kp == 0 && pos < nc) {
         double qr[3], fo[4];
         qr[0] = fmax(zc - d->zbc[pos], HM1);
-        double ur = uc * cs + vc * sn;
+        double ur = dot2(uc, cs, vc, sn, pat[P_UR]);
         qr[1] = ur * fmin(hc / qr[0], 1.5);
         if (hc <= HM2 || qr[0] <= HM2) qr[1] = copysign(VMIN, ur);
-        qr[2] = vc * cs - uc * sn;
+        qr[2] = dot2(vc, cs, -uc, sn, pat[P_QR2]);
         osher(h1, ql, qr, fil, fo);
         F0 = fo[0];
         F1 = fo[1] + (1 - fmin(hc / qr[0], 1.5)) * hc * ur * ur / 2;
@@ -773,14 +817,14 @@ static void flux_slot(orc_deck *d, int variant, int kt, int jt, int s) {
         double cl1 = sqrt(9.81 * d->h[nc]);
         double ql1[3], qr1[3], fo[4];
         ql1[0] = d->h[nc];
-        ql1[1] = d->u[nc] * cs1 + d->v[nc] * sn1;
-        ql1[2] = d->v[nc] * cs1 - d->u[nc] * sn1;
+        ql1[1] = dot2(d->u[nc], cs1, d->v[nc], sn1, pat[P_QL1M]);
+        ql1[2] = dot2(d->v[nc], cs1, -d->u[nc], sn1, pat[P_QL2M]);
         double fil1 = ql1[1] + 2 * cl1;
         qr1[0] = fmax(zc1 - d->zbc[nc], HM1);
-        double ur1 = u1 * cs1 + v1 * sn1;
+        double ur1 = dot2(u1, cs1, v1, sn1, pat[P_UR1]);
         qr1[1] = ur1 * fmin(hc2 / qr1[0], 1.5);
         if (hc2 <= HM2 || qr1[0] <= HM2) qr1[1] = copysign(VMIN, ur1);
-        qr1[2] = v1 * cs1 - u1 * sn1;
+        qr1[2] = dot2(v1, cs1, -u1, sn1, pat[P_QR2M]);
         osher(d->h[nc], ql1, qr1, fil1, fo);
         F1 = fo[1] + (1 - fmin(hc2 / qr1[0], 1.5)) * hc2 * ur1 * ur1 / 2;
         F0 = -fo[0];
@@ -805,9 +849,9 @@ static void update_cell(orc_deck *d, int variant, int pos) {
     for (int s = 4 * pos; s < 4 * (pos + 1); s++) {
         double fr1 = d->f1[s] + d->f3[s];
         double fr2 = d->f2[s];
-        wh += d->side[s] * d->f0[s];
-        wu += d->slcos[s] * fr1 - d->slsin[s] * fr2;
-        wv += d->slsin[s] * fr1 + d->slcos[s] * fr2;
+        wh = madd(d->side[s], d->f0[s], wh, pat[P_WH]);
+        wu += dot2(d->slcos[s], fr1, -d->slsin[s], fr2, pat[P_WU]);
+        wv += dot2(d->slsin[s], fr1, d->slcos[s], fr2, pat[P_WV]);
     }
     double h1 = d->h[pos], u1 = d->u[pos], v1 = d->v[pos];
     double dta;
@@ -829,7 +873,7 @@ static void update_cell(orc_deck *d, int variant, int pos) {
     }
     double wdta = 1.00 * dta;
     double cap = variant == ORC_VARIANT_F ? 5.0 : 15.0;
-    double h2 = fmax(h1 - wdta * wh + QLUA, HM1);
+    double h2 = fmax(madd(-wdta, wh, h1, pat[P_H2]) + QLUA, HM1);
     double z2 = h2 + d->zbc[pos];
     double u2, v2;
     if (h2 <= HM1) { u2 = 0.0; v2 = 0.0; }
@@ -839,14 +883,15 @@ static void update_cell(orc_deck *d, int variant, int pos) {
     } else {
         double qx1 = h1 * u1, qy1 = h1 * v1;
         double dtau = wdta * wu, dtav = wdta * wv;
-        double wsf = d->fnc[pos] * sqrt(u1 * u1 + v1 * v1) / pow(h1, 0.33333);
-        u2 = (qx1 - dtau - DT * wsf * u1) / h2;
-        v2 = (qy1 - dtav - DT * wsf * v1) / h2;
+        double wsf = d->fnc[pos] * sqrt(dot2(u1, u1, v1, v1, pat[P_SQ1])) / pow(h1, 0.33333);
+        (void)qx1; (void)qy1; (void)dtau; (void)dtav;
+        u2 = madd(-(DT * wsf), u1, dot2(h1, u1, -wdta, wu, pat[P_U2A]), pat[P_U2B]) / h2;
+        v2 = madd(-(DT * wsf), v1, dot2(h1, v1, -wdta, wv, pat[P_U2A]), pat[P_U2B]) / h2;
         u2 = copysign(fmin(fabs(u2), cap), u2);
         v2 = copysign(fmin(fabs(v2), cap), v2);
     }
     d->h[pos] = h2; d->u[pos] = u2; d->v[pos] = v2; d->z[pos] = z2;
-    d->w[pos] = sqrt(u2 * u2 + v2 * v2);
+    d->w[pos] = sqrt(dot2(u2, u2, v2, v2, pat[P_SQ2]));
 }
 
 void orc_update(orc_deck *d, int variant) {
