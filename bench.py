@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark: the plain fp64 hydro-cal timestep on the 207,234-cell channel.
+
+One step = CalculateFlux + UpdateCell over the whole mesh (one fused kernel
+launch here), replayed from a captured CUDA graph.  Prints ONE JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one process per GPU (torchrun); each rank runs its own replica of
+the scenario (the path has no exchange step between independent meshes), the
+time is the max over ranks and the value is the total cell-steps/s.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hydro-bench_b200"))
+
+METRIC = "cell-steps/s"
+WORKLOAD = "plain fp64 step, 207,234-cell Delaunay channel 40 km x 8 km (1 m bumps, 400 m^3/s Gaussian hydrograph), CUDA-graph replay"
+FALLBACK_HBM_GBS = 6650.0
+L2_FLUSH_BYTES = 256 << 20
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the step kernel from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "step_kernel_c207k_fp64.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+def make_deck(total_steps: int, tag: str):
+    from hydrob200 import deck as D
+    d = D.config_207k(steps=total_steps)
+    root = os.path.join(tempfile.gettempdir(), f"hb_bench_{tag}_{d.ndays}")
+    if not os.path.exists(os.path.join(root, "BINFOR", "TIME.DAT")):
+        tmp = root + f".tmp{os.getpid()}"
+        D.write_deck(d, tmp)
+        shutil.rmtree(root, ignore_errors=True)
+        os.replace(tmp, root)
+    return d, root
+
+
+def unique_edges(deck) -> int:
+    """Edges of the mesh counted once: paired interior slots / 2 + boundary slots."""
+    import numpy as np
+    nac = deck.array("nac").reshape(-1, 4)
+    side = deck.array("side").reshape(-1, 4)
+    real = side > 0
+    interior = int(np.sum(real & (nac > 0)))
+    boundary = int(np.sum(real & (nac == 0)))
+    return interior // 2 + boundary
+
+
+def alg_bytes_per_cell_step(cells: int, edges: int, w: int) -> float:
+    """Values one step must touch once: state in (H,U,V,Z) and out (H,U,V,Z,W),
+    per-cell constants (AREA, ZBC, FNC); per unique edge two int32 cell ids,
+    a 1-byte code and SIDE, COSF, SINF."""
+    return 12 * w + (edges / cells) * (8 + 1 + 3 * w)
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for ln in f:
+                p = [x.strip() for x in ln.split(",")]
+                if len(p) >= 9 and p[1].replace(".", "").isdigit():
+                    rows.append(p)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        smax = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference CPU solver (hydro-cal-fortan/calculate.cpp)
+# ---------------------------------------------------------------------------
+def _calc_deck(deck, steps: int, workdir: str) -> None:
+    from hydrob200 import deck as D
+    root = os.path.join(workdir, f"s{steps}", "origin", "changjiangkou")
+    if not os.path.exists(os.path.join(root, "TIME.DAT")):
+        D.write_cpu_solver_deck(deck, root, steps=steps)
+
+
+def _calc_run(binary: str, deck, steps: int, workdir: str) -> float:
+    _calc_deck(deck, steps, workdir)
+    t0 = time.perf_counter()
+    subprocess.run([binary], cwd=os.path.join(workdir, f"s{steps}"), check=True, stdout=subprocess.DEVNULL,
+                   stderr=subprocess.DEVNULL, timeout=900)
+    return time.perf_counter() - t0
+
+
+def cpu_reference_rate(deck, sample_steps: int, replicas: int):
+    """Cell-steps/s of the reference CPU solver, `replicas` concurrent
+    single-threaded processes (one per core); returns (value, cores, kind, sample)."""
+    binary = os.path.join(ROOT, "oracle", "_ref", "calculate")
+    work = tempfile.mkdtemp(prefix="hb_cpu_")
+    try:
+        if os.path.exists(binary):
+            t1 = _calc_run(binary, deck, 1, work)           # start-up and deck reading
+            _calc_deck(deck, sample_steps, work)
+            times = []
+            lock = threading.Lock()
+
+            def one():
+                t = _calc_run(binary, deck, sample_steps, work)
+                with lock:
+                    times.append(t)
+            th = [threading.Thread(target=one) for _ in range(replicas)]
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+            per = [max(t - t1, 1e-9) / (sample_steps - 1) for t in times]
+            value = sum(deck.cells / p for p in per)
+            return value, replicas, "reference", (f"hydro-cal-fortan/calculate.cpp (g++ -O3), {replicas} concurrent "
+                                                  f"single-threaded processes x {sample_steps} steps of the {deck.cells}-cell "
+                                                  f"mesh (open boundaries as walls), start-up time subtracted")
+        # no reference build: the oracle port, all host threads
+        sys.path.insert(0, ROOT)
+        from oracle.oracle import OracleDeck
+        from hydrob200 import deck as D
+        root = os.path.join(work, "native")
+        D.write_deck(deck, root)
+        o = OracleDeck(root)
+        t0 = time.perf_counter()
+        n = o.run(sample_steps)
+        t = time.perf_counter() - t0
+        return deck.cells * n / t, os.cpu_count(), "port", f"oracle port (OpenMP, {os.cpu_count()} threads) x {n} steps"
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def run_reference(args):
+    rank = _env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    from hydrob200 import deck as D
+    d = D.config_207k(steps=max(args.steps, 2) + 2)
+    replicas = os.cpu_count() or 1
+    # bounded sample: about 60 s of CPU time per process at most
+    sample = max(3, min(args.steps, 600))
+    value, cores, kind, desc = cpu_reference_rate(d, sample, replicas)
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "cells": d.cells},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind, "sample": desc},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=900)
+    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--graph-steps", type=int, default=100)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--e2e-steps", type=int, default=30)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import hydrob200 as hb
+
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local = _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    K, W, G = args.steps, args.warmup, max(1, min(args.graph_steps, args.steps))
+    total_steps = W + K + args.e2e_steps + 20
+    d, root = make_deck(total_steps, f"r{rank}")
+    deck = hb.Deck(root)
+    C = deck.cells
+    edges = unique_edges(deck)
+    w = 8 if args.precision == "fp64" else 4
+    b_alg = alg_bytes_per_cell_step(C, edges, w)
+
+    solver = hb.Solver(deck, precision=args.precision, device=local)
+    stream = torch.cuda.current_stream()
+    solver.capture_graph(G, stream)
+    # warm-up
+    done = 0
+    while done + G <= W:
+        solver.graph_launch(stream); done += G
+    if W - done:
+        solver.step(W - done, stream)
+    torch.cuda.synchronize()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    n_full, rem = divmod(K, G)
+    events = []
+    launches = 0
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        for _ in range(n_full):
+            flush.zero_()   # L2 flushed between timed iterations (one iteration = G steps)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solver.graph_launch(stream)
+            e1.record(stream)
+            events.append((e0, e1))
+            launches += G + 1          # G step kernels + the step-counter tick
+        if rem:
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solver.step(rem, stream)
+            e1.record(stream)
+            events.append((e0, e1))
+            launches += rem + 1
+        torch.cuda.synchronize()
+        barrier()
+    clocks = clk.summary()
+    solver.sync(stream)
+    ms = sum(a.elapsed_time(b) for a, b in events)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * C * K / (ms_max / 1e3)
+    step_ms = ms_max / K
+    peak, peak_kind = load_peaks()
+    achieved = b_alg * C / (step_ms / 1e3) / 1e9
+    traffic = ncu_traffic()
+
+    # end to end through the public API: host state in and out every step (page-locked buffers)
+    st = solver.get_state()
+    host = {k: torch.from_numpy(st[k]).pin_memory() for k in "HUVZW"}
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        solver.step_host(host["H"], host["U"], host["V"], host["Z"], host["W"], 1, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * C * args.e2e_steps / (float(t.item()) / 1e3)
+    launches_e2e = args.e2e_steps * 4
+
+    # stated error: a fresh 10-step run against the CPU oracle
+    err = None
+    if rank == 0:
+        try:
+            sys.path.insert(0, ROOT)
+            from oracle.oracle import OracleDeck
+            chk = hb.Solver(deck, precision=args.precision, device=local)
+            chk.step(10)
+            g = chk.get_state()
+            o = OracleDeck(root)
+            o.run(10)
+            od = o.dump()
+            err = {"vs": "CPU oracle (oracle/hydro_oracle.c)", "steps": 10}
+            for k in ("H", "U", "V"):
+                err[k] = float(np.max(np.abs(g[k] - od[k])) / max(float(np.max(np.abs(od[k]))), 1e-300))
+            if args.precision == "fp64":
+                err["vs_reference_build"] = "bit-identical at every golden step (tests/test_parity_gpu.py)"
+        except Exception as ex:   # the bench line still prints
+            err = {"error": str(ex)[:200]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            v, cores, kind, desc = cpu_reference_rate(d, 120, 1)
+            cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": kind, "sample": desc}
+        except Exception as ex:
+            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "reference", "sample": f"failed: {ex}"[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": C, "unique_edges": edges, "graph_steps": G,
+                       "l2": f"flushed ({L2_FLUSH_BYTES >> 20} MiB write) between timed iterations of {G} steps",
+                       "parallelism": f"{world} independent replicas, one per GPU" if world > 1 else "1 GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} hbm_gbs", "alg_bytes_per_cell_step": b_alg,
+                         "kernel_time": "timed-region time / steps (includes launch gaps)"},
+            "hbm_gbs_alg": achieved,
+            "error": err,
+            "clocks": clocks,
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 4 * 8 * C,
+                    "d2h_bytes_per_step": 5 * 8 * C, "api": "hb_step_host, one step per call, page-locked buffers"},
+            "gpu_launches": launches,
+            "gpu_launches_e2e": launches_e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -111,6 +111,8 @@ enum : int {
     M_H2 = 1, M_U2A = 1, M_U2B = 1, M_SQ1 = 1, M_SQ2 = 1 // :754, :771-772, :770, :777
 };
 
+static_assert(M_QL1 == M_QL1M && M_QR2 == M_QR2M, "flux_slot shares these modes between the two Osher routes");
+
 // ---------------------------------------------------------------------------
 // inputs / outputs of one slot
 // ---------------------------------------------------------------------------
@@ -167,38 +169,36 @@ __device__ __forceinline__ void qf_acc(typename A::real out[4], typename A::real
     out[3] = A::madd(sign > 0 ? h4 : -h4, h, out[3], M_ACC123);
 }
 
-// the sub-integrals QS<1..7> (QS<4> adds nothing)
-template <class A, int PIECE>
-__device__ __forceinline__ void qs(typename A::real out[4], const typename A::real ql[3], const typename A::real qr[3],
-                                   typename A::real &fil, typename A::real &fir, int sign) {
+// out += QF(h, u, v) (sign +1) or -= (sign -1) when `on`, with the reference
+// build's sums (functors.cu:453-497, :505-511); `out` is untouched otherwise.
+template <class A>
+__device__ __forceinline__ void qf_acc_if(typename A::real out[4], bool on, bool neg, typename A::real h,
+                                          typename A::real u, typename A::real v) {
     using R = typename A::real;
-    if constexpr (PIECE == 1) {
-        qf_acc<A>(out, ql[0], ql[1], ql[2], sign);
-    } else if constexpr (PIECE == 2) {
-        R us = A::div(fil, A::c(3.0));
-        R hs = A::div(A::mul(us, us), A::c(9.81));
-        qf_acc<A>(out, hs, us, ql[2], sign);
-    } else if constexpr (PIECE == 3) {
-        R ua = A::mul(A::add(fil, fir), A::c(0.5));
-        fil = A::sub(fil, ua);
-        R ha = A::div(A::mul(fil, fil), A::c(39.24));
-        qf_acc<A>(out, ha, ua, ql[2], sign);
-    } else if constexpr (PIECE == 5) {
-        R ua = A::mul(A::add(fil, fir), A::c(0.5));
-        fir = A::sub(fir, ua);
-        R ha = A::div(A::mul(fir, fir), A::c(39.24));
-        qf_acc<A>(out, ha, ua, qr[2], sign);
-    } else if constexpr (PIECE == 6) {
-        R us = A::div(fir, A::c(3.0));
-        R hs = A::div(A::mul(us, us), A::c(9.81));
-        qf_acc<A>(out, hs, us, qr[2], sign);
-    } else if constexpr (PIECE == 7) {
-        qf_acc<A>(out, qr[0], qr[1], qr[2], sign);
-    }
+    R f0 = A::mul(h, u);
+    R sh = neg ? -h : h;
+    R sf0 = neg ? -f0 : f0;
+    R h4 = A::mul(A::c(4.905), h);
+    R o0 = A::madd(sh, u, out[0], M_ACC0);
+    R o1 = A::madd(sf0, u, out[1], M_ACC123);
+    R o2 = A::madd(sf0, v, out[2], M_ACC123);
+    R o3 = A::madd(neg ? -h4 : h4, h, out[3], M_ACC123);
+    if (on) { out[0] = o0; out[1] = o1; out[2] = o2; out[3] = o3; }
 }
 
-// OSHER(pos, H_pre, QL, QR, FIL, FLR_OSHER); `cl` is sqrt(9.81*h_left), the
-// same value the reference recomputes at :577.
+// OSHER(pos, H_pre, QL, QR, FIL, FLR_OSHER), functors.cu:570-712, with the
+// sub-integrals QS<1..7> of :445-503.  `cl` is sqrt(9.81*h_left), the value
+// the reference recomputes at :577.
+//
+// The reference's 16 (K1, K2) cases each add a signed subset of the pieces
+// 1 (left state), 2 (left sonic point), 3 (intermediate state, left),
+// 5 (intermediate state, right), 6 (right sonic point), 7 (right state), and
+// every case lists its pieces in increasing order.  Here all six pieces are
+// evaluated in that order and each is added when its case coefficient is
+// non-zero: the same sums in the same order, without the per-case branches
+// that would serialise a warp whose lanes fall into different cases.
+// Piece 3 updates FIL and piece 5 updates FIR (QS<3>, QS<5>); no case has
+// both, and piece 6 sees the FIR that piece 5 left.
 template <class A>
 __device__ __forceinline__ void osher(typename A::real cl, const typename A::real ql[3],
                                       const typename A::real qr[3], typename A::real fil,
@@ -218,27 +218,45 @@ __device__ __forceinline__ void osher(typename A::real cl, const typename A::rea
     else if (ql[1] >= cl && qr[1] >= -cr) k1 = 2;
     else if (ql[1] < cl && qr[1] < -cr) k1 = 3;
     else if (ql[1] >= cl && qr[1] < -cr) k1 = 4;
-    switch (k1 * 4 + k2) {
-    case 5: qs<A, 2>(out, ql, qr, fil, fir, 1); break;
-    case 6: qs<A, 3>(out, ql, qr, fil, fir, 1); break;
-    case 7: qs<A, 5>(out, ql, qr, fil, fir, 1); break;
-    case 8: qs<A, 6>(out, ql, qr, fil, fir, 1); break;
-    case 9: qs<A, 1>(out, ql, qr, fil, fir, 1); break;
-    case 10: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 3>(out, ql, qr, fil, fir, 1); break;
-    case 11: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 5>(out, ql, qr, fil, fir, 1); break;
-    case 12: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 6>(out, ql, qr, fil, fir, 1); break;
-    case 13: qs<A, 2>(out, ql, qr, fil, fir, 1); qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
-    case 14: qs<A, 3>(out, ql, qr, fil, fir, 1); qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
-    case 15: qs<A, 5>(out, ql, qr, fil, fir, 1); qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
-    case 16: qs<A, 7>(out, ql, qr, fil, fir, 1); break;
-    case 17: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
-    case 18: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 3>(out, ql, qr, fil, fir, 1);
-             qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
-    case 19: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 5>(out, ql, qr, fil, fir, 1);
-             qs<A, 6>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
-    case 20: qs<A, 1>(out, ql, qr, fil, fir, 1); qs<A, 2>(out, ql, qr, fil, fir, -1); qs<A, 7>(out, ql, qr, fil, fir, 1); break;
-    default: break;
+    const bool any = k1 != 0 && k2 != 0;
+    // coefficients of the pieces (functors.cu:612-711)
+    const bool p1 = any && (k1 == 2 || k1 == 4);
+    const bool p2 = any && (k2 == 1 ? (k1 == 1 || k1 == 3) : (k1 == 2 || k1 == 4));
+    const bool n2 = k2 != 1;                                   // piece 2 subtracted
+    const bool p3 = any && k2 == 2;
+    const bool p5 = any && k2 == 3;
+    const bool p6 = any && (k2 == 4 ? k1 <= 2 : k1 >= 3);
+    const bool n6 = k2 != 4;                                   // piece 6 subtracted
+    const bool p7 = any && k1 >= 3;
+    // piece 1: QF(QL)
+    qf_acc_if<A>(out, p1, false, ql[0], ql[1], ql[2]);
+    // piece 2: US = FIL/3, HS = US^2/9.81
+    {
+        R us = A::div(fil, A::c(3.0));
+        R hs = A::div(A::mul(us, us), A::c(9.81));
+        qf_acc_if<A>(out, p2, n2, hs, us, ql[2]);
     }
+    // pieces 3 and 5 share UA = (FIL + FIR)/2
+    const R ua35 = A::mul(A::add(fil, fir), A::c(0.5));
+    {
+        R fil3 = A::sub(fil, ua35);
+        R ha = A::div(A::mul(fil3, fil3), A::c(39.24));
+        qf_acc_if<A>(out, p3, false, ha, ua35, ql[2]);
+    }
+    R fir5 = A::sub(fir, ua35);
+    {
+        R ha = A::div(A::mul(fir5, fir5), A::c(39.24));
+        qf_acc_if<A>(out, p5, false, ha, ua35, qr[2]);
+    }
+    // piece 6: US = FIR/3 with FIR as piece 5 left it
+    {
+        R f6 = p5 ? fir5 : fir;
+        R us = A::div(f6, A::c(3.0));
+        R hs = A::div(A::mul(us, us), A::c(9.81));
+        qf_acc_if<A>(out, p6, n6, hs, us, qr[2]);
+    }
+    // piece 7: QF(QR)
+    qf_acc_if<A>(out, p7, false, qr[0], qr[1], qr[2]);
 }
 
 // ---------------------------------------------------------------------------
@@ -454,8 +472,21 @@ __device__ __forceinline__ void bounda(const SlotIn<typename A::real> &in, const
 // CalculateFluxKernel body for one slot, functors.cu:47-202
 // `cl_own` is sqrt(9.81*H) of the slot's cell (the caller may compute it once
 // per cell; it is bit-identical to the reference's per-slot value).
+//
+// ZERO_LEN: the slot is a zero-length edge without neighbour (the unused
+// fourth slot of a triangle, mesh.cpp:303-306), and only its contribution
+// SIDE*F = 0*F to the cell sums is wanted.  pow(x, 1.5) is then replaced by
+// |x| (NaN for x < 0): 0*F keeps the same sign and NaN-ness, so the sums are
+// unchanged, and the slot costs no pow.
 // ---------------------------------------------------------------------------
-template <class A, int VARIANT, class TableFetch>
+template <class A, bool ZERO_LEN>
+__device__ __forceinline__ typename A::real pow15(typename A::real x) {
+    using R = typename A::real;
+    if constexpr (ZERO_LEN) return x < R(0) ? A::div(R(0), R(0)) : A::fabs(x);
+    else return A::pow(x, A::c(1.5));
+}
+
+template <class A, int VARIANT, class TableFetch, bool ZERO_LEN = false>
 __device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, typename A::real cl_own,
                                           const StepParams &p, const TableFetch &fetch,
                                           SlotOut<typename A::real> &o) {
@@ -479,17 +510,18 @@ __device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, ty
         uc = in.nb.u;
         vc = in.nb.v;
     }
+    int route = 0;   // 1: direct Osher (functors.cu:151-164), 2: mirrored Osher (:165-200)
     if (code_is_bounda(in.code)) {
         bounda<A, VARIANT>(in, p, fil, ql, zc, uc, vc, fetch, o);
     } else if (h1 <= HM1 && hc <= HM1) {
         o.f[0] = R(0); o.f[1] = R(0); o.f[2] = R(0); o.f[3] = R(0);
     } else if (zi <= bc) {
-        o.f[0] = A::mul(A::c(-K::C1), A::pow(hc, A::c(1.5)));
+        o.f[0] = A::mul(A::c(-K::C1), pow15<A, ZERO_LEN>(hc));
         o.f[1] = A::mul(A::mul(h1, ql[1]), A::fabs(ql[1]));
         o.f[2] = R(0);
         o.f[3] = A::mul(A::mul(A::c(4.905), h1), h1);
     } else if (zc <= zbc1) {
-        o.f[0] = A::mul(A::c(K::C1), A::pow(h1, A::c(1.5)));
+        o.f[0] = A::mul(A::c(K::C1), pow15<A, ZERO_LEN>(h1));
         R ha = A::mul(h1, A::fabs(ql[1]));
         o.f[1] = A::mul(ha, ql[1]);
         o.f[2] = A::mul(ha, ql[2]);
@@ -503,7 +535,7 @@ __device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, ty
             o.f[2] = A::mul(o.f[0], A::dot(vc, cs, -uc, sn, M_SHALLOW_VT));
             o.f[3] = A::mul(A::mul(A::c(4.905), h1), h1);
         } else {
-            o.f[0] = A::mul(A::c(K::C1), A::pow(h1, A::c(1.5)));
+            o.f[0] = A::mul(A::c(K::C1), pow15<A, ZERO_LEN>(h1));
             o.f[1] = R(0); o.f[2] = R(0);
             o.f[3] = A::mul(A::mul(A::c(4.905), h1), h1);
         }
@@ -517,52 +549,52 @@ __device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, ty
             o.f[2] = A::mul(o.f[0], ql[2]);
             o.f[3] = A::mul(A::mul(A::c(4.905), hc1), hc1);
         } else {
-            o.f[0] = A::mul(A::c(-K::C1), A::pow(hc, A::c(1.5)));
+            o.f[0] = A::mul(A::c(-K::C1), pow15<A, ZERO_LEN>(hc));
             o.f[1] = A::mul(A::mul(h1, ql[1]), ql[1]);
             o.f[2] = R(0);
             o.f[3] = A::mul(A::mul(A::c(4.905), h1), h1);
         }
     } else if (in.code == CODE_ZERO && in.own_first) {
-        // direct Osher across the edge (functors.cu:151-164)
-        R qr[3], fo[4];
-        qr[0] = A::fmax(A::sub(zc, zbc1), HM1);
-        R ur = A::dot(uc, cs, vc, sn, M_UR);
-        R ratio = A::fmin(A::div(hc, qr[0]), A::c(1.5));
-        qr[1] = A::mul(ur, ratio);
-        if (hc <= HM2 || qr[0] <= HM2) qr[1] = A::copysign(A::c(K::VMIN), ur);
-        qr[2] = A::dot(vc, cs, -uc, sn, M_QR2);
-        osher<A>(cl_own, ql, qr, fil, fo);
+        route = 1;
+    } else if (!in.has_nb) {
+        // the reference reads H[-1] here (functors.cu:170)
+        o.undefined = true;
+        o.f[0] = R(0); o.f[1] = R(0); o.f[2] = R(0); o.f[3] = R(0);
+    } else {
+        route = 2;
+    }
+    if (route == 0) return;
+    // One Osher evaluation for both routes.  Direct: left = this cell, right =
+    // the neighbour, normal (COSF, SINF).  Mirrored: left = the neighbour, right
+    // = this cell, normal reversed.  The fused products differ between the two
+    // in the reference build (M_QL2 vs M_QL2M, M_UR vs M_UR1).
+    const bool mir = route == 2;
+    const R hL = mir ? in.nb.h : h1, uL = mir ? in.nb.u : u1, vL = mir ? in.nb.v : v1;
+    const R zbcL = mir ? in.nb.zbc : zbc1;
+    const R hR = mir ? h1 : in.nb.h, uR = mir ? u1 : in.nb.u, vR = mir ? v1 : in.nb.v;
+    const R zR = mir ? A::fmax(zbc1, z1) : zc;
+    const R c_ = mir ? -cs : cs, s_ = mir ? -sn : sn;
+    const R clL = mir ? A::sqrt(A::mul(A::c(9.81), hL)) : cl_own;
+    R qlx[3], qr[3], fo[4];
+    qlx[0] = hL;
+    qlx[1] = A::dot(uL, c_, vL, s_, M_QL1);                    // M_QL1 == M_QL1M
+    qlx[2] = mir ? A::dot(vL, c_, -uL, s_, M_QL2M) : A::dot(vL, c_, -uL, s_, M_QL2);
+    const R filx = A::add(qlx[1], A::mul(A::c(2.0), clL));
+    const R hcR = A::fmax(hR, HM1);
+    qr[0] = A::fmax(A::sub(zR, zbcL), HM1);
+    const R ur = mir ? A::dot(uR, c_, vR, s_, M_UR1) : A::dot(uR, c_, vR, s_, M_UR);
+    const R ratio = A::fmin(A::div(hcR, qr[0]), A::c(1.5));
+    qr[1] = A::mul(ur, ratio);
+    if (hcR <= HM2 || qr[0] <= HM2) qr[1] = A::copysign(A::c(K::VMIN), ur);
+    qr[2] = A::dot(vR, c_, -uR, s_, M_QR2);                    // M_QR2 == M_QR2M
+    osher<A>(clL, qlx, qr, filx, fo);
+    o.f[1] = A::add(fo[1], A::mul(A::mul(A::mul(A::mul(A::sub(A::c(1.0), ratio), hcR), ur), ur), A::c(0.5)));
+    o.f[2] = fo[2];
+    if (!mir) {
         o.f[0] = fo[0];
-        o.f[1] = A::add(fo[1], A::mul(A::mul(A::mul(A::mul(A::sub(A::c(1.0), ratio), hc), ur), ur), A::c(0.5)));
-        o.f[2] = fo[2];
         o.f[3] = fo[3];
     } else {
-        // the same edge seen from the neighbour, normal reversed (functors.cu:165-200)
-        if (!in.has_nb) {
-            o.undefined = true;
-            o.f[0] = R(0); o.f[1] = R(0); o.f[2] = R(0); o.f[3] = R(0);
-            return;
-        }
-        const R hn = in.nb.h, un_ = in.nb.u, vn = in.nb.v;
-        R hc2 = A::fmax(h1, HM1);
-        R zc1 = A::fmax(zbc1, z1);
-        R cs1 = -cs, sn1 = -sn;
-        R ql1[3], qr1[3], fo[4];
-        ql1[0] = hn;
-        ql1[1] = A::dot(un_, cs1, vn, sn1, M_QL1M);
-        ql1[2] = A::dot(vn, cs1, -un_, sn1, M_QL2M);
-        const R cl_nb = A::sqrt(A::mul(A::c(9.81), hn));
-        R fil1 = A::add(ql1[1], A::mul(A::c(2.0), cl_nb));
-        qr1[0] = A::fmax(A::sub(zc1, bc), HM1);
-        R ur1 = A::dot(u1, cs1, v1, sn1, M_UR1);
-        R ratio = A::fmin(A::div(hc2, qr1[0]), A::c(1.5));
-        qr1[1] = A::mul(ur1, ratio);
-        if (hc2 <= HM2 || qr1[0] <= HM2) qr1[1] = A::copysign(A::c(K::VMIN), ur1);
-        qr1[2] = A::dot(v1, cs1, -u1, sn1, M_QR2M);
-        osher<A>(cl_nb, ql1, qr1, fil1, fo);
-        o.f[1] = A::add(fo[1], A::mul(A::mul(A::mul(A::mul(A::sub(A::c(1.0), ratio), hc2), ur1), ur1), A::c(0.5)));
         o.f[0] = -fo[0];
-        o.f[2] = fo[2];
         R za = A::add(A::sqrt(A::div(fo[3], A::c(4.905))), bc);
         R hc3 = R(0);
         if (za > zbc1) hc3 = A::sub(za, zbc1);

@@ -72,7 +72,7 @@ extern "C" void hb_options_default(hb_options *o) {
     o->precision = HB_FP64;
     o->device = 0;
     o->renumber = 1;
-    o->block_cells = 0;
+    o->tile_config = 0;
 }
 
 namespace hb {
@@ -82,21 +82,40 @@ namespace hb {
 // ---------------------------------------------------------------------------
 enum : uint8_t { META_CODE = 0x0F, META_OWN_FIRST = 0x10, META_HAS_NB = 0x20 };
 
+// Tile configurations of the step kernel: threads per CTA (= the most real
+// slots and the most cells a tile holds) and the CTAs per SM the compiler is
+// asked to fit (__launch_bounds__), which caps the registers per thread.
+struct TileConfig { int threads, min_blocks; };
+constexpr TileConfig TILE_CONFIGS[] = {{256, 2}, {256, 3}, {256, 4}, {128, 6}, {128, 8}, {512, 2}};
+constexpr int N_TILE_CONFIGS = sizeof(TILE_CONFIGS) / sizeof(TILE_CONFIGS[0]);
+constexpr int DEFAULT_TILE_CONFIG = 2;   // (256, 4): fastest in the 207,234-cell sweep
+
+// Device mesh.  Cells are in reverse Cuthill-McKee order and cut into tiles of
+// consecutive cells holding at most TILE real slots; a tile is one CTA.  Real
+// slots (every slot except the zero-length fourth slot of a triangle) are
+// stored compactly, tile by tile, in slot order within each cell.
 template <class R>
 struct DevMesh {
     int C;                     // cells
     int per_day;               // steps per table interval (steps_per_day - 1)
-    int ndays, nb, nhq;
+    int ndays, nb, nhq, ntiles;
     double hm1, hm2, jl, dt;
     R *H[2], *U[2], *V[2], *Z[2];
     R *W;
     const R *zbc, *fnc, *dta;  // dta: DT/AREA (variant H) or AREA (variant F)
     const R *sidex;            // variant F CFL length
     const int32_t *bcell;      // [C] row of the boundary tables, -1 = none
-    const int32_t *nbr;        // [4C] neighbour (device order), -1 = none
-    uint8_t *meta;             // [4C] code | own_first | has_nb (code changes on breach)
+    const int32_t *cslot0;     // [C] first compact slot of the cell
+    const uint8_t *cmask;      // [C] bit j: slot j is a real slot
+    const int32_t *tcell0;     // [ntiles+1] first cell of each tile
+    const int32_t *tslot0;     // [ntiles+1] first compact slot of each tile
+    // compact real slots [NS]
+    const int32_t *scell;      // owning cell
+    const uint8_t *sj;         // slot index j within the cell
+    const int32_t *nbr;        // neighbour (device order), -1 = none
+    uint8_t *meta;             // code | own_first | has_nb (code changes on breach)
     const R *cosf, *sinf, *side;
-    R *f0, *f1, *f2, *f3;      // [4C] persistent fluxes
+    R *f0, *f1, *f2, *f3;      // [4C] persistent fluxes, index 4*cell + j
     const R *bqt, *bdqt, *bzt, *bdzt;   // [ndays*nb]
     const R *btop;             // [nb]
     const int32_t *bnhq1;      // [nb]
@@ -105,9 +124,17 @@ struct DevMesh {
     const long long *step_ctr;
 };
 
-template <class A, int VARIANT>
-__global__ void __launch_bounds__(256) step_kernel(DevMesh<typename A::real> m, int k, int write_flux) {
+// One step of one tile.  Phase 1: a thread per real slot computes the slot's
+// flux (CalculateFluxKernel, functors.cu:47-202) into shared memory.
+// Phase 2: a thread per cell sums its four slots in order j = 0..3 and
+// updates the cell (UpdateCellKernel, functors.cu:717-784); the zero-length
+// fourth slot of a triangle is evaluated there, without pow (flux_slot's
+// ZERO_LEN).  The state is double-buffered: read (step & 1), write the other.
+template <class A, int VARIANT, int TILE, int MINB>
+__global__ void __launch_bounds__(TILE, MINB) step_kernel(DevMesh<typename A::real> m, int k, int write_flux) {
     using R = typename A::real;
+    __shared__ R sf[4][TILE];
+    __shared__ R sg[3][TILE];
     const long long step = *m.step_ctr + k;
     const int par = (int)(step & 1);
     int jt = (int)(step / m.per_day);
@@ -120,87 +147,138 @@ __global__ void __launch_bounds__(256) step_kernel(DevMesh<typename A::real> m, 
     const R *__restrict__ U = m.U[par];
     const R *__restrict__ V = m.V[par];
     const R *__restrict__ Z = m.Z[par];
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int cell = gtid >> 2;
-    const int j = gtid & 3;
-    const bool active = cell < m.C;
-    const int c = active ? cell : m.C - 1;
-    const int s = 4 * c + j;
     const StepParams p{m.hm1, m.hm2, m.jl, m.dt, kt, jt};
+    const int tile = blockIdx.x;
+    const int t = threadIdx.x;
+    const int c0 = m.tcell0[tile], c1 = m.tcell0[tile + 1];
+    const int s0 = m.tslot0[tile], s1 = m.tslot0[tile + 1];
 
-    SlotIn<R> in;
-    in.own = {H[c], U[c], V[c], Z[c], m.zbc[c]};
-    const uint8_t meta = m.meta[s];
-    const int nb = m.nbr[s];
-    in.code = (int8_t)(meta & META_CODE);
-    in.own_first = meta & META_OWN_FIRST;
-    in.has_nb = meta & META_HAS_NB;
-    if (in.has_nb) in.nb = {H[nb], U[nb], V[nb], Z[nb], m.zbc[nb]};
-    else in.nb = {R(0), R(0), R(0), R(0), R(0)};
-    in.cosj = m.cosf[s];
-    in.sinj = m.sinf[s];
-    in.side = m.side[s];
-    auto fetch = [&]() {
-        BoundaryIn<R> b;
-        const int r = m.bcell[c];
-        if (r >= 0) {
-            const size_t t = (size_t)jt * m.nb + r;
-            b.qt = m.bqt[t]; b.dqt = m.bdqt[t]; b.zt = m.bzt[t]; b.dzt = m.bdzt[t];
-            b.top = m.btop[r]; b.nhq1 = m.bnhq1[r];
-            b.zw = m.bzw + (size_t)r * m.nhq; b.qw = m.bqw + (size_t)r * m.nhq;
-        } else {
-            b.qt = b.dqt = b.zt = b.dzt = b.top = R(0); b.nhq1 = 0;
-            b.zw = m.bzw + (size_t)m.nb * m.nhq; b.qw = m.bqw + (size_t)m.nb * m.nhq;
-        }
-        b.nhq = m.nhq;
-        return b;
-    };
-    const R cl = A::sqrt(A::mul(A::c(9.81), in.own.h));
-    SlotOut<R> o;
-    flux_slot<A, VARIANT>(in, cl, p, fetch, o);
-    if (active) {
+    if (s0 + t < s1) {
+        const int s = s0 + t;
+        const int c = m.scell[s];
+        const int j = m.sj[s];
+        SlotIn<R> in;
+        in.own = {H[c], U[c], V[c], Z[c], m.zbc[c]};
+        const uint8_t meta = m.meta[s];
+        const int nb = m.nbr[s];
+        in.code = (int8_t)(meta & META_CODE);
+        in.own_first = meta & META_OWN_FIRST;
+        in.has_nb = meta & META_HAS_NB;
+        if (in.has_nb) in.nb = {H[nb], U[nb], V[nb], Z[nb], m.zbc[nb]};
+        else in.nb = {R(0), R(0), R(0), R(0), R(0)};
+        in.cosj = m.cosf[s];
+        in.sinj = m.sinf[s];
+        in.side = m.side[s];
+        auto fetch = [&]() {
+            BoundaryIn<R> b;
+            const int r = m.bcell[c];
+            if (r >= 0) {
+                const size_t q = (size_t)jt * m.nb + r;
+                b.qt = m.bqt[q]; b.dqt = m.bdqt[q]; b.zt = m.bzt[q]; b.dzt = m.bdzt[q];
+                b.top = m.btop[r]; b.nhq1 = m.bnhq1[r];
+                b.zw = m.bzw + (size_t)r * m.nhq; b.qw = m.bqw + (size_t)r * m.nhq;
+            } else {
+                b.qt = b.dqt = b.zt = b.dzt = b.top = R(0); b.nhq1 = 0;
+                b.zw = m.bzw + (size_t)m.nb * m.nhq; b.qw = m.bqw + (size_t)m.nb * m.nhq;
+            }
+            b.nhq = m.nhq;
+            return b;
+        };
+        const R cl = A::sqrt(A::mul(A::c(9.81), in.own.h));
+        SlotOut<R> o;
+        flux_slot<A, VARIANT>(in, cl, p, fetch, o);
+        const size_t fs = 4 * (size_t)c + j;
         if (o.mask != 0xF) {   // codes that leave fluxes unwritten keep the old values
-            if (!(o.mask & 1)) o.f[0] = m.f0[s];
-            if (!(o.mask & 2)) o.f[1] = m.f1[s];
-            if (!(o.mask & 4)) o.f[2] = m.f2[s];
-            if (!(o.mask & 8)) o.f[3] = m.f3[s];
+            if (!(o.mask & 1)) o.f[0] = m.f0[fs];
+            if (!(o.mask & 2)) o.f[1] = m.f1[fs];
+            if (!(o.mask & 4)) o.f[2] = m.f2[fs];
+            if (!(o.mask & 8)) o.f[3] = m.f3[fs];
         }
         if (write_flux || in.code == CODE_BOUNDA_OTHER) {
-            m.f0[s] = o.f[0]; m.f1[s] = o.f[1]; m.f2[s] = o.f[2]; m.f3[s] = o.f[3];
+            m.f0[fs] = o.f[0]; m.f1[fs] = o.f[1]; m.f2[fs] = o.f[2]; m.f3[fs] = o.f[3];
         }
         if (o.klas_to_zero) m.meta[s] = (uint8_t)((meta & ~META_CODE) | CODE_ZERO);
         if (o.undefined) atomicOr(m.err, ERRBIT_UNDEFINED);
+        sf[0][t] = o.f[0]; sf[1][t] = o.f[1]; sf[2][t] = o.f[2]; sf[3][t] = o.f[3];
+        sg[0][t] = in.side; sg[1][t] = in.cosj; sg[2][t] = in.sinj;
     }
-    // gather the cell's four slots on all four lanes and sum in slot order
-    const unsigned full = 0xffffffffu;
-    const int base = (threadIdx.x & 31) & ~3;
+    __syncthreads();
+    if (c0 + t >= c1) return;
+    const int c = c0 + t;
+    const R h = H[c], u = U[c], v = V[c], z = Z[c], zbc = m.zbc[c];
+    const unsigned mask = m.cmask[c];
+    int q = m.cslot0[c] - s0;
     R wh = R(0), wu = R(0), wv = R(0);
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int src = base + q;
-        R f0 = __shfl_sync(full, o.f[0], src);
-        R f1 = __shfl_sync(full, o.f[1], src);
-        R f2 = __shfl_sync(full, o.f[2], src);
-        R f3 = __shfl_sync(full, o.f[3], src);
-        R sd = __shfl_sync(full, in.side, src);
-        R cs = __shfl_sync(full, in.cosj, src);
-        R sn = __shfl_sync(full, in.sinj, src);
+    for (int j = 0; j < 4; j++) {
+        R f0, f1, f2, f3, sd, cs, sn;
+        if (mask & (1u << j)) {
+            f0 = sf[0][q]; f1 = sf[1][q]; f2 = sf[2][q]; f3 = sf[3][q];
+            sd = sg[0][q]; cs = sg[1][q]; sn = sg[2][q];
+            q++;
+        } else {
+            // zero-length slot without neighbour, code 0, COSF = SINF = SIDE = 0
+            SlotIn<R> in;
+            in.own = {h, u, v, z, zbc};
+            in.nb = {R(0), R(0), R(0), R(0), R(0)};
+            in.has_nb = false; in.own_first = false; in.code = CODE_ZERO;
+            in.cosj = R(0); in.sinj = R(0); in.side = R(0);
+            auto nofetch = []() { return BoundaryIn<R>{}; };
+            const R cl = A::sqrt(A::mul(A::c(9.81), h));
+            SlotOut<R> o;
+            if (write_flux) {
+                flux_slot<A, VARIANT, decltype(nofetch), false>(in, cl, p, nofetch, o);
+                const size_t fs = 4 * (size_t)c + j;
+                m.f0[fs] = o.f[0]; m.f1[fs] = o.f[1]; m.f2[fs] = o.f[2]; m.f3[fs] = o.f[3];
+            } else {
+                flux_slot<A, VARIANT, decltype(nofetch), true>(in, cl, p, nofetch, o);
+            }
+            f0 = o.f[0]; f1 = o.f[1]; f2 = o.f[2]; f3 = o.f[3];
+            sd = R(0); cs = R(0); sn = R(0);
+        }
         // SLCOS = SIDE*COSF, SLSIN = SIDE*SINF (mesh.cpp:368-369): one rounded product each
         wsum_add<A>(wh, wu, wv, f0, f1, f2, f3, sd, A::mul(sd, cs), A::mul(sd, sn));
     }
-    if (!active || j != 0) return;
     CellUpdateIn<R> ci;
-    ci.h = in.own.h; ci.u = in.own.u; ci.v = in.own.v; ci.zbc = in.own.zbc;
+    ci.h = h; ci.u = u; ci.v = v; ci.zbc = zbc;
     ci.fnc = m.fnc[c];
     ci.dta_or_area = m.dta[c];
     ci.sidex = VARIANT == 1 ? m.sidex[c] : R(0);
-    CellUpdateOut<R> u = update_cell<A, VARIANT>(ci, wh, wu, wv, p);
+    CellUpdateOut<R> r = update_cell<A, VARIANT>(ci, wh, wu, wv, p);
     const int np = par ^ 1;
-    m.H[np][c] = u.h; m.U[np][c] = u.u; m.V[np][c] = u.v; m.Z[np][c] = u.z; m.W[c] = u.w;
-    if (!(isfinite((double)u.h) && isfinite((double)u.u) && isfinite((double)u.v))) atomicOr(m.err, ERRBIT_NONFINITE);
+    m.H[np][c] = r.h; m.U[np][c] = r.u; m.V[np][c] = r.v; m.Z[np][c] = r.z; m.W[c] = r.w;
+    if (!(isfinite((double)r.h) && isfinite((double)r.u) && isfinite((double)r.v))) atomicOr(m.err, ERRBIT_NONFINITE);
 }
 
 __global__ void tick_kernel(long long *ctr, int n) { *ctr += n; }
+
+// reference-order staging <-> device-order state (perm[new] = old)
+template <class R>
+__global__ void stage_in_kernel(int C, const int32_t *__restrict__ perm, const double *__restrict__ stage,
+                                const long long *ctr, R *H0, R *U0, R *V0, R *Z0, R *H1, R *U1, R *V1, R *Z1) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) return;
+    const int o = perm[i];
+    const bool odd = (*ctr) & 1;
+    (odd ? H1 : H0)[i] = (R)stage[o];
+    (odd ? U1 : U0)[i] = (R)stage[(size_t)C + o];
+    (odd ? V1 : V0)[i] = (R)stage[2 * (size_t)C + o];
+    (odd ? Z1 : Z0)[i] = (R)stage[3 * (size_t)C + o];
+}
+template <class R>
+__global__ void stage_out_kernel(int C, const int32_t *__restrict__ perm, double *__restrict__ stage,
+                                 const long long *ctr, const R *H0, const R *U0, const R *V0, const R *Z0,
+                                 const R *H1, const R *U1, const R *V1, const R *Z1, const R *W) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) return;
+    const int o = perm[i];
+    const bool odd = (*ctr) & 1;
+    stage[o] = (double)(odd ? H1 : H0)[i];
+    stage[(size_t)C + o] = (double)(odd ? U1 : U0)[i];
+    stage[2 * (size_t)C + o] = (double)(odd ? V1 : V0)[i];
+    stage[3 * (size_t)C + o] = (double)(odd ? Z1 : Z0)[i];
+    stage[4 * (size_t)C + o] = (double)W[i];
+}
 
 // per-cell constants that the update needs, computed on the device with the
 // reference's arithmetic (functors.cu:750, v0 functors.cu:752-763)
@@ -294,11 +372,16 @@ struct hb_handle {
     hb::DevMesh<float> m32{};
     uint32_t *d_err = nullptr;
     long long *d_ctr = nullptr;
+    int32_t *d_perm = nullptr;       // perm on the device
+    std::vector<int32_t> slot_index; // [4C] device-order slot -> compact real slot, -1 = zero-length slot
+    int nslots = 0;
+    int ntiles() const { return fp32() ? m32.ntiles : m64.ntiles; }
+    double *d_stage = nullptr;       // [5C] reference-order staging for hb_step_host
     long long steps_done = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int graph_steps = 0;
-    int block = 256;
+    int tile_config = 0;             // index into TILE_CONFIGS
     bool fp32() const { return opt.precision == HB_FP32; }
     ~hb_handle() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -357,29 +440,66 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
     m.ndays = h->ndays;
     m.nhq = h->nhq;
     m.hm1 = h->hm1; m.hm2 = h->hm2; m.jl = h->jl; m.dt = h->dt;
-    std::vector<int32_t> nbr(S, -1);
-    std::vector<uint8_t> meta(S, 0);
+    // real slots: everything except a zero-length slot without neighbour and code 0
+    std::vector<int32_t> nbr4(S, -1);
+    std::vector<uint8_t> meta4(S, 0);
+    std::vector<char> real4(S, 0);
     std::vector<char> needs_table(C, 0);
     for (int i = 0; i < C; i++) {
         const int old = perm[i];
         for (int j = 0; j < 4; j++) {
-            const size_t so = 4 * (size_t)old + j;
+            const size_t so = 4 * (size_t)old + j, sn = 4 * (size_t)i + j;
             const int nc_old = (int)(md->nac[so] - 1.0);
             int8_t code = hb::klas_code(md->klas[so]);
             uint8_t mt = (uint8_t)code;
             if (nc_old != -1) {
                 if (nc_old < 0 || nc_old >= C)
                     return hb::set_error(HB_E_BADMESH, "NAC of cell %d slot %d = %g out of range", old + 1, j, md->nac[so]);
-                nbr[4 * (size_t)i + j] = inv[nc_old];
+                nbr4[sn] = inv[nc_old];
                 mt |= hb::META_HAS_NB;
                 if (old < nc_old) mt |= hb::META_OWN_FIRST;
             }
-            meta[4 * (size_t)i + j] = mt;
+            meta4[sn] = mt;
+            real4[sn] = !(md->side[so] == 0.0 && md->cosf[so] == 0.0 && md->sinf[so] == 0.0 && nc_old == -1 &&
+                          code == hb::CODE_ZERO);
             if (code == hb::CODE_K10 || code == hb::CODE_K1 || code == hb::CODE_K3 || code == hb::CODE_K6 ||
                 code == hb::CODE_K7)
                 needs_table[i] = 1;
         }
     }
+    // tiles of consecutive cells with at most TILE real slots (and TILE cells)
+    std::vector<int32_t> tcell0{0}, tslot0{0}, cslot0(C), scell, nbr;
+    std::vector<uint8_t> cmask(C), sj, meta;
+    std::vector<R> scos, ssin, sside;
+    h->slot_index.assign(S, -1);
+    int tile_slots = 0, tile_cells = 0;
+    for (int i = 0; i < C; i++) {
+        int nreal = 0;
+        for (int j = 0; j < 4; j++) nreal += real4[4 * (size_t)i + j];
+        const int TILE = hb::TILE_CONFIGS[h->tile_config].threads;
+        if (tile_slots + nreal > TILE || tile_cells + 1 > TILE) {
+            tcell0.push_back(i);
+            tslot0.push_back((int32_t)scell.size());
+            tile_slots = 0; tile_cells = 0;
+        }
+        cslot0[i] = (int32_t)scell.size();
+        uint8_t mk = 0;
+        for (int j = 0; j < 4; j++) {
+            const size_t sn = 4 * (size_t)i + j, so = 4 * (size_t)perm[i] + j;
+            if (!real4[sn]) continue;
+            mk |= (uint8_t)(1u << j);
+            h->slot_index[sn] = (int32_t)scell.size();
+            scell.push_back(i); sj.push_back((uint8_t)j); nbr.push_back(nbr4[sn]); meta.push_back(meta4[sn]);
+            scos.push_back((R)md->cosf[so]); ssin.push_back((R)md->sinf[so]); sside.push_back((R)md->side[so]);
+        }
+        cmask[i] = mk;
+        tile_slots += nreal;
+        tile_cells += 1;
+    }
+    tcell0.push_back(C);
+    tslot0.push_back((int32_t)scell.size());
+    m.ntiles = (int)tcell0.size() - 1;
+    h->nslots = (int)scell.size();
     // compact boundary tables
     std::vector<int32_t> bcell(C, -1);
     std::vector<int> rows;
@@ -411,11 +531,18 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
     TRY(dev_upload(h, &rp, cellv(md->fnc))); m.fnc = rp;
     R *area_d = nullptr, *side_d = nullptr;
     TRY(dev_upload(h, &area_d, cellv(md->area)));
-    TRY(dev_upload(h, &side_d, slotv(md->side))); m.side = side_d;
-    TRY(dev_upload(h, &rp, slotv(md->cosf))); m.cosf = rp;
-    TRY(dev_upload(h, &rp, slotv(md->sinf))); m.sinf = rp;
+    TRY(dev_upload(h, &side_d, slotv(md->side)));   // [4C], for the per-cell setup only
+    TRY(dev_upload(h, &rp, sside)); m.side = rp;
+    TRY(dev_upload(h, &rp, scos)); m.cosf = rp;
+    TRY(dev_upload(h, &rp, ssin)); m.sinf = rp;
     TRY(dev_upload(h, &ip, nbr)); m.nbr = ip;
     TRY(dev_upload(h, &up, meta)); m.meta = up;
+    TRY(dev_upload(h, &ip, scell)); m.scell = ip;
+    TRY(dev_upload(h, &up, sj)); m.sj = up;
+    TRY(dev_upload(h, &ip, cslot0)); m.cslot0 = ip;
+    TRY(dev_upload(h, &up, cmask)); m.cmask = up;
+    TRY(dev_upload(h, &ip, tcell0)); m.tcell0 = ip;
+    TRY(dev_upload(h, &ip, tslot0)); m.tslot0 = ip;
     TRY(dev_upload(h, &ip, bcell)); m.bcell = ip;
     TRY(dev_upload(h, &rp, bqt)); m.bqt = rp;
     TRY(dev_upload(h, &rp, bdqt)); m.bdqt = rp;
@@ -451,11 +578,17 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
 
 template <class A, int VARIANT>
 int launch_steps(hb_handle *h, hb::DevMesh<typename A::real> &m, int n, cudaStream_t st) {
-    const long long threads = 4LL * h->C;
-    const int block = h->block;
-    const int grid = (int)((threads + block - 1) / block);
-    for (int k = 0; k < n; k++) {
-        hb::step_kernel<A, VARIANT><<<grid, block, 0, st>>>(m, k, k == n - 1);
+    const int grid = m.ntiles;
+    auto go = [&](auto kern, int threads) {
+        for (int k = 0; k < n; k++) kern<<<grid, threads, 0, st>>>(m, k, k == n - 1);
+    };
+    switch (h->tile_config) {
+    case 0: go(hb::step_kernel<A, VARIANT, 256, 2>, 256); break;
+    case 1: go(hb::step_kernel<A, VARIANT, 256, 3>, 256); break;
+    case 2: go(hb::step_kernel<A, VARIANT, 256, 4>, 256); break;
+    case 3: go(hb::step_kernel<A, VARIANT, 128, 6>, 128); break;
+    case 4: go(hb::step_kernel<A, VARIANT, 128, 8>, 128); break;
+    default: go(hb::step_kernel<A, VARIANT, 512, 2>, 512); break;
     }
     hb::tick_kernel<<<1, 1, 0, st>>>(h->d_ctr, n);
     HB_CUDA_RET(cudaGetLastError());
@@ -479,6 +612,14 @@ int check_range(hb_handle *h, long long n) {
 
 }  // namespace
 
+extern "C" int hb_tile_configs(int32_t *threads, int32_t *min_blocks, int32_t capacity) {
+    for (int i = 0; i < hb::N_TILE_CONFIGS && i < capacity; i++) {
+        if (threads) threads[i] = hb::TILE_CONFIGS[i].threads;
+        if (min_blocks) min_blocks[i] = hb::TILE_CONFIGS[i].min_blocks;
+    }
+    return hb::N_TILE_CONFIGS;
+}
+
 extern "C" int hb_create(const hb_mesh_desc *md, const hb_options *opt_in, hb_handle **out) {
     if (!md || !out) return hb::set_error(HB_E_INVALID, "hb_create: null argument");
     *out = nullptr;
@@ -500,7 +641,11 @@ extern "C" int hb_create(const hb_mesh_desc *md, const hb_options *opt_in, hb_ha
     h->C = md->cells; h->ndays = md->ndays; h->nhq = md->nhq;
     h->steps_per_day = md->steps_per_day; h->per_day = md->steps_per_day - 1;
     h->dt = md->dt; h->hm1 = md->hm1; h->hm2 = md->hm2; h->jl = md->jl;
-    h->block = 256;
+    if (opt.tile_config < 0 || opt.tile_config > hb::N_TILE_CONFIGS) {
+        delete h;
+        return hb::set_error(HB_E_INVALID, "hb_create: tile_config %d outside 0..%d", opt.tile_config, hb::N_TILE_CONFIGS);
+    }
+    h->tile_config = opt.tile_config == 0 ? hb::DEFAULT_TILE_CONFIG : opt.tile_config - 1;
     const int C = h->C;
     // neighbour lists in input order, for the renumbering
     std::vector<int32_t> nbr_old(4 * (size_t)C, -1);
@@ -518,7 +663,11 @@ extern "C" int hb_create(const hb_mesh_desc *md, const hb_options *opt_in, hb_ha
     for (int i = 0; i < C; i++) h->inv[h->perm[i]] = i;
     h->klas_orig.assign(md->klas, md->klas + 4 * (size_t)C);
     int st;
-    if ((st = dev_alloc(h, &h->d_err, 1)) != HB_OK || (st = dev_alloc(h, &h->d_ctr, 1)) != HB_OK) { delete h; return st; }
+    if ((st = dev_alloc(h, &h->d_err, 1)) != HB_OK || (st = dev_alloc(h, &h->d_ctr, 1)) != HB_OK ||
+        (st = dev_upload(h, &h->d_perm, h->perm)) != HB_OK || (st = dev_alloc(h, &h->d_stage, 5 * (size_t)C)) != HB_OK) {
+        delete h;
+        return st;
+    }
     st = h->fp32() ? build_device_mesh<float>(h, md, h->m32) : build_device_mesh<double>(h, md, h->m64);
     if (st != HB_OK) { delete h; return st; }
     *out = h;
@@ -581,13 +730,14 @@ template <class R>
 int get_klas_t(hb_handle *h, hb::DevMesh<R> &m, double *klas) {
     const int C = h->C;
     const size_t S = 4 * (size_t)C;
-    std::vector<uint8_t> meta(S);
+    std::vector<uint8_t> meta(std::max(h->nslots, 1));
     HB_CUDA_RET(cudaDeviceSynchronize());
-    HB_CUDA_RET(cudaMemcpy(meta.data(), m.meta, S, cudaMemcpyDeviceToHost));
+    HB_CUDA_RET(cudaMemcpy(meta.data(), m.meta, h->nslots, cudaMemcpyDeviceToHost));
     for (int i = 0; i < C; i++)
         for (int j = 0; j < 4; j++) {
             const size_t so = 4 * (size_t)h->perm[i] + j;
-            const int code = meta[4 * (size_t)i + j] & hb::META_CODE;
+            const int ci = h->slot_index[4 * (size_t)i + j];
+            const int code = ci < 0 ? hb::CODE_ZERO : (meta[ci] & hb::META_CODE);
             double k = h->klas_orig[so];
             if (hb::klas_code(k) == hb::CODE_K7 && code == hb::CODE_ZERO) k = 0.0;   // breached (functors.cu:242)
             klas[so] = k;
@@ -619,6 +769,38 @@ extern "C" int hb_step(hb_handle *h, int32_t nsteps, void *stream) {
     TRY(enqueue_steps(h, nsteps, (cudaStream_t)stream));
     h->steps_done += nsteps;
     return HB_OK;
+}
+
+namespace {
+template <class R>
+int step_host_t(hb_handle *h, hb::DevMesh<R> &m, double *H, double *U, double *V, double *Z, double *W, int n,
+                cudaStream_t st) {
+    const int C = h->C;
+    const size_t b = (size_t)C * sizeof(double);
+    double *io[5] = {H, U, V, Z, W};
+    for (int k = 0; k < 4; k++) HB_CUDA_RET(cudaMemcpyAsync(h->d_stage + (size_t)k * C, io[k], b, cudaMemcpyHostToDevice, st));
+    const int blocks = (C + 255) / 256;
+    hb::stage_in_kernel<R><<<blocks, 256, 0, st>>>(C, h->d_perm, h->d_stage, h->d_ctr, m.H[0], m.U[0], m.V[0], m.Z[0],
+                                                    m.H[1], m.U[1], m.V[1], m.Z[1]);
+    HB_CUDA_RET(cudaGetLastError());
+    TRY(enqueue_steps(h, n, st));
+    hb::stage_out_kernel<R><<<blocks, 256, 0, st>>>(C, h->d_perm, h->d_stage, h->d_ctr, m.H[0], m.U[0], m.V[0], m.Z[0],
+                                                     m.H[1], m.U[1], m.V[1], m.Z[1], m.W);
+    HB_CUDA_RET(cudaGetLastError());
+    for (int k = 0; k < 5; k++)
+        if (io[k]) HB_CUDA_RET(cudaMemcpyAsync(io[k], h->d_stage + (size_t)k * C, b, cudaMemcpyDeviceToHost, st));
+    return HB_OK;
+}
+}  // namespace
+
+extern "C" int hb_step_host(hb_handle *h, double *H, double *U, double *V, double *Z, double *W, int32_t nsteps,
+                            void *stream) {
+    if (!h || !H || !U || !V || !Z || nsteps < 0) return hb::set_error(HB_E_INVALID, "hb_step_host: bad argument");
+    TRY(check_range(h, nsteps));
+    cudaStream_t st = (cudaStream_t)stream;
+    int r = h->fp32() ? step_host_t(h, h->m32, H, U, V, Z, W, nsteps, st) : step_host_t(h, h->m64, H, U, V, Z, W, nsteps, st);
+    if (r == HB_OK) h->steps_done += nsteps;
+    return r;
 }
 
 extern "C" int hb_sync(hb_handle *h, void *stream) {
@@ -653,8 +835,6 @@ extern "C" int hb_set_position(hb_handle *h, int64_t steps_done) {
     if ((steps_done & 1) != (h->steps_done & 1)) {
         const size_t bytes = (size_t)h->C * (h->fp32() ? sizeof(float) : sizeof(double));
         const int from = (int)(h->steps_done & 1), to = from ^ 1;
-        void *const *src64[4] = {(void *const *)&h->m64.H[from], (void *const *)&h->m64.U[from], (void *const *)&h->m64.V[from], (void *const *)&h->m64.Z[from]};
-        (void)src64;
         if (h->fp32()) {
             float **B[4] = {h->m32.H, h->m32.U, h->m32.V, h->m32.Z};
             for (auto b : B) HB_CUDA_RET(cudaMemcpy(b[to], b[from], bytes, cudaMemcpyDeviceToDevice));

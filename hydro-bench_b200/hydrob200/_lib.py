@@ -35,7 +35,7 @@ class MeshDesc(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("variant", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32), ("renumber", C.c_int32),
-                ("block_cells", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("tile_config", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 def _view_types(real):
@@ -77,6 +77,7 @@ def lib():
     vp = C.c_void_p
     sig = {
         "hb_options_default": (None, [C.POINTER(Options)]),
+        "hb_tile_configs": (C.c_int, [_ip, _ip, C.c_int32]),
         "hb_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(Options), C.POINTER(vp)]),
         "hb_destroy": (C.c_int, [vp]),
         "hb_set_state": (C.c_int, [vp, _dp, _dp, _dp, _dp, _dp]),
@@ -87,6 +88,7 @@ def lib():
         "hb_sync": (C.c_int, [vp, vp]),
         "hb_position": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
         "hb_set_position": (C.c_int, [vp, C.c_int64]),
+        "hb_step_host": (C.c_int, [vp, _dp, _dp, _dp, _dp, _dp, C.c_int32, vp]),
         "hb_capture_graph": (C.c_int, [vp, C.c_int32, vp]),
         "hb_graph_launch": (C.c_int, [vp, vp]),
         "hb_device_state": (C.c_int, [vp] + [C.POINTER(vp)] * 5),
@@ -120,8 +122,8 @@ def check(status: int) -> None:
 
 
 # every symbol the C headers declare (checked by the CPU tests)
-EXPORTED = ["hb_options_default", "hb_create", "hb_destroy", "hb_set_state", "hb_get_state", "hb_get_flux",
-            "hb_get_klas", "hb_step", "hb_sync", "hb_position", "hb_set_position", "hb_capture_graph",
+EXPORTED = ["hb_options_default", "hb_tile_configs", "hb_create", "hb_destroy", "hb_set_state", "hb_get_state", "hb_get_flux",
+            "hb_get_klas", "hb_step", "hb_sync", "hb_position", "hb_set_position", "hb_step_host", "hb_capture_graph",
             "hb_graph_launch", "hb_device_state", "hb_get_permutation", "hb_device_errors", "hb_last_error",
             "hb_last_error_string", "hb_status_string", "hb_deck_load", "hb_deck_mesh", "hb_deck_state",
             "hb_deck_free", "hb_ref_calculate_flux", "hb_ref_update_cell", "hb_ref_calculate_flux_f32",

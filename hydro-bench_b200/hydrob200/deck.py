@@ -442,6 +442,49 @@ def stress_deck(name: str, mx: int, my: int, seed: int, *, dt: float = 1.0, step
                 nzq_tables=[zq], meta=dict(seed=seed, mx=mx, my=my, steps=steps))
 
 
+def probe_deck(name: str, seed: int = 31, mx: int = 20, my: int = 40, steps: int = 60, mdt: int = 20) -> Deck:
+    """A stress deck whose boundary tables jump by orders of magnitude between
+    table intervals, so that ``QT + DQT*kt`` and ``ZT + DZT*jt`` (functors.cu:209,
+    :376) are dominated by the product term and their rounding becomes visible
+    in the fluxes; also more rating-curve (KLAS 3) and weir (KLAS 6) slots."""
+    d = stress_deck(name, mx, my, seed, steps=steps, mdt=mdt, jl=0.2)
+    rng = np.random.default_rng(seed + 7)
+    t_unit = mdt / 86400.0
+    nd = d.ndays + 2
+    ts = np.arange(nd + 2) * t_unit
+    ts[-1] = (d.ndays + 1) * t_unit * 2 + 1.0
+    q_lo, q_hi = rng.uniform(0.01, 0.2, ts.size), rng.uniform(20.0, 80.0, ts.size)
+    qa = np.where(np.arange(ts.size) % 2 == 0, q_lo, q_hi)
+    qb = np.where(np.arange(ts.size) % 2 == 1, q_lo * 3.0, q_hi * 0.7)
+    d.nq_series = [Series(ts, qa), Series(ts, qb)]
+    zlo = 1.6 + rng.uniform(0.0, 0.1, ts.size)
+    zhi = 2.4 + rng.uniform(0.0, 0.6, ts.size)
+    d.nz_series = [Series(ts, np.where(np.arange(ts.size) % 2 == 0, zlo, zhi))]
+    # every right-side slot alternates 1 / 3 (no open slots), so more rating-curve cells
+    nv = np.where(d.nap[:, 3] == 0, 3, 4)
+    bc, bs = _boundary_slots(d.nac, d.nap)
+    mid = _slot_midpoints(d.xy, d.nap, bc, bs)
+    lx = d.xy[:, 0].max()
+    right = np.nonzero(mid[:, 0] > lx * (1 - 1e-9))[0]
+    right = right[np.argsort(mid[right, 1])]
+    lvl, rat = [], []
+    for k, r in enumerate(right):
+        code = KLAS_LEVEL if k % 2 == 0 else KLAS_RATING
+        d.klas[bc[r], bs[r]] = code
+        (lvl if code == KLAS_LEVEL else rat).append(int(bc[r]) + 1)
+    d.mbz = [(c, 1) for c in sorted(set(lvl))]
+    d.mbzq = [(c, 1) for c in sorted(set(rat) - set(lvl))]
+    cx = np.array([d.xy[r[:k] - 1].mean(axis=0)[0] for r, k in zip(d.nap, np.where(d.nap[:, 3] == 0, 3, 4))])
+    deep = cx > 0.85 * lx            # keep the cells at the level/rating boundary well wet
+    d.z0 = np.where(deep, d.zbc + 1.2, d.z0)
+    for (c, _) in d.mbzq:            # rating cells flowing outwards
+        d.u0[c - 1] = rng.uniform(0.5, 2.0)
+        d.v0[c - 1] = rng.uniform(-0.5, 0.5)
+    d.nzq_tables = [Series(np.array([1.0, 1.4, 1.8, 2.4, 3.2]), np.array([0.0, 2.0, 9.0, 30.0, 90.0]))]
+    del nv
+    return d
+
+
 # ---------------------------------------------------------------------------
 # writers
 # ---------------------------------------------------------------------------

@@ -18,6 +18,8 @@ DECKS = {
                      bins=("h64", "f64"), steps=(1, 50), full=True),
     "breach": dict(make=lambda: D.stress_deck("breach", 12, 8, 23, steps=10, with_breach=True),
                    bins=("h64",), steps=(1,), full=True),
+    "probe": dict(make=lambda: D.probe_deck("probe"),
+                  bins=("h64", "f64"), steps=(7, 13, 45, 58), full=True),
     "f1": dict(make=lambda: D.config_f1(),
                bins=("h64", "f64", "h32"), steps=(1, 50, 100), full=False),
 }

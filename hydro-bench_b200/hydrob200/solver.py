@@ -77,7 +77,7 @@ class Solver:
     """
 
     def __init__(self, deck: Deck, variant="H", precision="fp64", device: int = 0, renumber: bool = True,
-                 init_state: bool = True):
+                 init_state: bool = True, tile_config: int = 0):
         self.deck = deck   # keeps the host arrays alive
         opt = _lib.Options()
         lib().hb_options_default(C.byref(opt))
@@ -85,6 +85,7 @@ class Solver:
         opt.precision = _PRECISIONS[precision]
         opt.device = device
         opt.renumber = 1 if renumber else 0
+        opt.tile_config = int(tile_config)
         self.variant = opt.variant
         self.precision = opt.precision
         self._h = C.c_void_p()
@@ -130,6 +131,17 @@ class Solver:
 
     def step(self, n: int, stream=None) -> None:
         check(lib().hb_step(self._h, int(n), _stream_handle(stream)))
+
+    def step_host(self, H, U, V, Z, W, n: int = 1, stream=None) -> None:
+        """hb_step_host: state in/out through host buffers (numpy arrays or
+        page-locked CPU torch tensors, fp64, reference order). Asynchronous."""
+        def ptr(a):
+            if a is None:
+                return None
+            if hasattr(a, "data_ptr"):
+                return C.cast(C.c_void_p(a.data_ptr()), _lib._dp)
+            return _as_dp(a)
+        check(lib().hb_step_host(self._h, ptr(H), ptr(U), ptr(V), ptr(Z), ptr(W), int(n), _stream_handle(stream)))
 
     def sync(self, stream=None) -> None:
         check(lib().hb_sync(self._h, _stream_handle(stream)))

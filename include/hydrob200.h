@@ -64,9 +64,13 @@ typedef struct hb_options {
     int32_t precision;        /* hb_precision */
     int32_t device;           /* CUDA device ordinal */
     int32_t renumber;         /* 1: reverse Cuthill-McKee cell order on the device (default), 0: input order */
-    int32_t block_cells;      /* cells per CTA of the step kernel (0 = autotuned default) */
+    int32_t tile_config;      /* step-kernel tile shape: 0 = default, k > 0 = entry k-1 of hb_tile_configs() */
     int32_t reserved[3];
 } hb_options;
+
+/* The step kernel's compiled tile shapes: threads (= real slots and cells
+ * per tile) and CTAs per SM; returns how many there are. */
+int hb_tile_configs(int32_t *threads, int32_t *min_blocks, int32_t capacity);
 
 /* Default options: variant H, fp64, device 0, renumbered. */
 void hb_options_default(hb_options *opt);
@@ -93,6 +97,14 @@ int hb_sync(hb_handle *h, void *stream);
 /* Current position: steps taken so far, and the (kt, jt) of the next step. */
 int hb_position(hb_handle *h, int64_t *steps_done, int32_t *kt, int32_t *jt);
 int hb_set_position(hb_handle *h, int64_t steps_done);
+
+/* End-to-end call with host buffers, for callers whose state lives on the
+ * host (the reference driver keeps it in MeshData, benchmark.cu:66-84):
+ * copies H, U, V, Z (reference order, [CELL] fp64) to the device, advances
+ * nsteps steps, and copies H, U, V, Z, W back into the same buffers.  The
+ * copies are asynchronous on `stream` (page-locked buffers make them truly
+ * so); call hb_sync before reading the results. */
+int hb_step_host(hb_handle *h, double *H, double *U, double *V, double *Z, double *W, int32_t nsteps, void *stream);
 
 /* Capture nsteps steps as one CUDA graph owned by the handle; each replay
  * (hb_graph_launch) advances the boundary-table time like hb_step would. */

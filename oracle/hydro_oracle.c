@@ -70,10 +70,21 @@ enum {
     P_H2, P_U2A, P_U2B, P_SQ1, P_SQ2,     /* UpdateCell (:754, :771-772, :770, :777) */
     P_COUNT
 };
+/* Pinned by tests/golden (each differs from the alternatives on some slot):
+ * QL1, QL2, UR, QR2, QL1M, QL2M, UR1, QR2M, ACC0, ACC123, SHALLOW_VT, K10,
+ * FIAL1, FIAR1, K6UN, K6VT, WH, WU, WV, H2, U2A, U2B, SQ1.  No fixture
+ * separates the modes of K1, K3Q, FIAL3, FIAR3 and LAQP, nor of SQ2 (W is not
+ * in the reference dump); those follow the rule the pinned ones obey, that a
+ * product used only by the add is fused. */
 static int pat[P_COUNT] = {
     [P_QL1] = 2, [P_QL2] = 1, [P_UR] = 1, [P_QR2] = 1,
     [P_QL1M] = 2, [P_QL2M] = 2, [P_UR1] = 2, [P_QR2M] = 1,
-    [P_ACC0] = 0, [P_ACC123] = 1,
+    [P_ACC0] = 0, [P_ACC123] = 1, [P_SHALLOW_VT] = 1,
+    [P_K10] = 1, [P_K1] = 1, [P_FIAL1] = 1, [P_FIAR1] = 1,
+    [P_K3Q] = 1, [P_FIAL3] = 1, [P_FIAR3] = 1, [P_LAQP] = 1,
+    [P_K6UN] = 1, [P_K6VT] = 1,
+    [P_WH] = 1, [P_WU] = 1, [P_WV] = 2,
+    [P_H2] = 1, [P_U2A] = 1, [P_U2B] = 1, [P_SQ1] = 1, [P_SQ2] = 1,
 };
 
 void orc_set_pattern(int id, int mode) {

@@ -58,6 +58,10 @@ def main() -> int:
     os.makedirs(args.out, exist_ok=True)
     refdir = os.path.join(ROOT, "oracle", "_ref")
     manifest = {"decks": {}, "dumps": {}}
+    prev = os.path.join(args.out, "manifest.json")
+    if args.only and os.path.exists(prev):      # refresh some decks, keep the others' records
+        with open(prev) as f:
+            manifest = json.load(f)
     for name, spec in DECKS.items():
         if args.only and name not in args.only.split(","):
             continue

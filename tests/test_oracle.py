@@ -66,7 +66,8 @@ def test_oracle_matches_reference_fp64(deck_dir, name, binary):
     least 90 % of all values bit-identical (what differs is CUDA's pow versus
     glibc's, 1-2 ulp). Later steps: H/U/V/Z within 1e-12 on the benchmark's
     channel deck, within 1e-11 on the stress decks, whose dry fronts and
-    jets amplify those pow ulps.
+    jets amplify those pow ulps, and 1e-10 on the probe deck, whose boundary
+    tables jump by orders of magnitude between intervals.
     """
     o = O.OracleDeck(deck_dir[name], O.VARIANT_H if binary == "h64" else O.VARIANT_F)
     done = 0
@@ -82,7 +83,7 @@ def test_oracle_matches_reference_fp64(deck_dir, name, binary):
             frac = np.mean([np.mean(d[k] == g[k]) for k in g.files])
             assert frac >= 0.9, frac
         else:
-            tol = 1e-12 if name == "f1" else 1e-11
+            tol = {"f1": 1e-12, "probe": 1e-10}.get(name, 1e-11)
             for k in STATE:
                 assert normwise(d[k], g[k]) <= tol, (name, binary, steps, k)
 
