@@ -18,6 +18,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace hb {
 
 // ---------------------------------------------------------------------------
@@ -60,6 +62,28 @@ struct F64Exact {
     static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
     static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
     static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    // x / c for a constant c, correctly rounded: RN(x/c) == __ddiv_rn(x, c).
+    // Method: Markstein's theorem (P. Markstein, IBM J. Res. Dev. 34(1), 1990;
+    // J.-M. Muller et al., Handbook of Floating-Point Arithmetic, ch. 4): if y is
+    // within half an ulp of 1/c and q within one ulp of x/c, then
+    // RN(q + RN(x - q*c)*y) = RN(x/c), the remainder being exact in an FMA.
+    // y = RN(1/c) is folded at compile time; one refinement of q0 = RN(x*y)
+    // brings q within one ulp, the second step rounds correctly.  Zeros,
+    // infinities, NaNs and |x| outside [2^-900, 2^900] (far from over/underflow
+    // of every quotient here) take __ddiv_rn.  Five FP64 operations instead
+    // of the ~18 instructions of __ddiv_rn.
+    static __device__ __forceinline__ double divk(double x, double c) {
+        const double y = 1.0 / c;
+        const double ax = ::fabs(x);
+        if (ax >= 0x1p-900 && ax <= 0x1p+900) {
+            double q = __dmul_rn(x, y);
+            double r = __fma_rn(-q, c, x);
+            q = __fma_rn(r, y, q);
+            r = __fma_rn(-q, c, x);
+            return __fma_rn(r, y, q);
+        }
+        return __ddiv_rn(x, c);
+    }
     static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
     static __device__ __forceinline__ double sqrt(double a) { return __dsqrt_rn(a); }
     static __device__ __forceinline__ double pow(double a, double b) { return ::pow(a, b); }
@@ -86,6 +110,7 @@ struct F32Fast {
     static __device__ __forceinline__ float add(float a, float b) { return a + b; }
     static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
     static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+    static __device__ __forceinline__ float divk(float x, double c) { return x / (float)c; }
     static __device__ __forceinline__ float fma(float a, float b, float c) { return fmaf(a, b, c); }
     static __device__ __forceinline__ float sqrt(float a) { return sqrtf(a); }
     static __device__ __forceinline__ float pow(float a, float b) { return powf(a, b); }
@@ -169,11 +194,17 @@ __device__ __forceinline__ void qf_acc(typename A::real out[4], typename A::real
     out[3] = A::madd(sign > 0 ? h4 : -h4, h, out[3], M_ACC123);
 }
 
-// out += QF(h, u, v) (sign +1) or -= (sign -1) when `on`, with the reference
-// build's sums (functors.cu:453-497, :505-511); `out` is untouched otherwise.
-template <class A>
+// Per-piece record of one Osher evaluation, for re-summing FLUX2 with another
+// tangential velocity: f0[i] = h*u of piece i (pieces 1, 2, 3, 5, 6, 7 in that
+// order; 1-3 carry QL's tangent, 5-7 QR's), act/neg bit i = added / subtracted.
+template <class R>
+struct OsherTrace { R f0[6]; unsigned act, neg; };
+
+// out += QF(h, u, v) (or -=, `neg`) when `on`, with the reference build's sums
+// (functors.cu:453-497, :505-511); `out` is untouched otherwise.
+template <class A, class TR>
 __device__ __forceinline__ void qf_acc_if(typename A::real out[4], bool on, bool neg, typename A::real h,
-                                          typename A::real u, typename A::real v) {
+                                          typename A::real u, typename A::real v, TR *tr, int piece) {
     using R = typename A::real;
     R f0 = A::mul(h, u);
     R sh = neg ? -h : h;
@@ -184,6 +215,28 @@ __device__ __forceinline__ void qf_acc_if(typename A::real out[4], bool on, bool
     R o2 = A::madd(sf0, v, out[2], M_ACC123);
     R o3 = A::madd(neg ? -h4 : h4, h, out[3], M_ACC123);
     if (on) { out[0] = o0; out[1] = o1; out[2] = o2; out[3] = o3; }
+    if constexpr (!std::is_same<TR, void>::value) {
+        tr->f0[piece] = f0;
+        tr->act |= (on ? 1u : 0u) << piece;
+        tr->neg |= (neg ? 1u : 0u) << piece;
+    }
+}
+
+// FLUX2 of a traced Osher evaluation re-summed with tangents ql2 / qr2, in the
+// same order and with the same fused sums as qf_acc_if.
+template <class A>
+__device__ __forceinline__ typename A::real osher_f2(const OsherTrace<typename A::real> &tr, typename A::real ql2,
+                                                     typename A::real qr2) {
+    using R = typename A::real;
+    R acc = R(0);
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        const R v = i < 3 ? ql2 : qr2;
+        const R sf0 = ((tr.neg >> i) & 1u) ? -tr.f0[i] : tr.f0[i];
+        const R o2 = A::madd(sf0, v, acc, M_ACC123);
+        if ((tr.act >> i) & 1u) acc = o2;
+    }
+    return acc;
 }
 
 // OSHER(pos, H_pre, QL, QR, FIL, FLR_OSHER), functors.cu:570-712, with the
@@ -199,11 +252,12 @@ __device__ __forceinline__ void qf_acc_if(typename A::real out[4], bool on, bool
 // that would serialise a warp whose lanes fall into different cases.
 // Piece 3 updates FIL and piece 5 updates FIR (QS<3>, QS<5>); no case has
 // both, and piece 6 sees the FIR that piece 5 left.
-template <class A>
+template <class A, class TR = void>
 __device__ __forceinline__ void osher(typename A::real cl, const typename A::real ql[3],
                                       const typename A::real qr[3], typename A::real fil,
-                                      typename A::real out[4]) {
+                                      typename A::real out[4], TR *tr = nullptr) {
     using R = typename A::real;
+    if constexpr (!std::is_same<TR, void>::value) { tr->act = 0; tr->neg = 0; }
     R cr = A::sqrt(A::mul(A::c(9.81), qr[0]));
     R fir = A::sub(qr[1], A::mul(A::c(2.0), cr));
     R ua = A::mul(A::add(fil, fir), A::c(0.5));
@@ -229,34 +283,34 @@ __device__ __forceinline__ void osher(typename A::real cl, const typename A::rea
     const bool n6 = k2 != 4;                                   // piece 6 subtracted
     const bool p7 = any && k1 >= 3;
     // piece 1: QF(QL)
-    qf_acc_if<A>(out, p1, false, ql[0], ql[1], ql[2]);
+    qf_acc_if<A>(out, p1, false, ql[0], ql[1], ql[2], tr, 0);
     // piece 2: US = FIL/3, HS = US^2/9.81
     {
-        R us = A::div(fil, A::c(3.0));
-        R hs = A::div(A::mul(us, us), A::c(9.81));
-        qf_acc_if<A>(out, p2, n2, hs, us, ql[2]);
+        R us = A::divk(fil, 3.0);
+        R hs = A::divk(A::mul(us, us), 9.81);
+        qf_acc_if<A>(out, p2, n2, hs, us, ql[2], tr, 1);
     }
     // pieces 3 and 5 share UA = (FIL + FIR)/2
     const R ua35 = A::mul(A::add(fil, fir), A::c(0.5));
     {
         R fil3 = A::sub(fil, ua35);
-        R ha = A::div(A::mul(fil3, fil3), A::c(39.24));
-        qf_acc_if<A>(out, p3, false, ha, ua35, ql[2]);
+        R ha = A::divk(A::mul(fil3, fil3), 39.24);
+        qf_acc_if<A>(out, p3, false, ha, ua35, ql[2], tr, 2);
     }
     R fir5 = A::sub(fir, ua35);
     {
-        R ha = A::div(A::mul(fir5, fir5), A::c(39.24));
-        qf_acc_if<A>(out, p5, false, ha, ua35, qr[2]);
+        R ha = A::divk(A::mul(fir5, fir5), 39.24);
+        qf_acc_if<A>(out, p5, false, ha, ua35, qr[2], tr, 3);
     }
     // piece 6: US = FIR/3 with FIR as piece 5 left it
     {
         R f6 = p5 ? fir5 : fir;
-        R us = A::div(f6, A::c(3.0));
-        R hs = A::div(A::mul(us, us), A::c(9.81));
-        qf_acc_if<A>(out, p6, n6, hs, us, qr[2]);
+        R us = A::divk(f6, 3.0);
+        R hs = A::divk(A::mul(us, us), 9.81);
+        qf_acc_if<A>(out, p6, n6, hs, us, qr[2], tr, 4);
     }
     // piece 7: QF(QR)
-    qf_acc_if<A>(out, p7, false, qr[0], qr[1], qr[2]);
+    qf_acc_if<A>(out, p7, false, qr[0], qr[1], qr[2], tr, 5);
 }
 
 // ---------------------------------------------------------------------------
@@ -272,7 +326,7 @@ __device__ __forceinline__ typename A::real weir_discharge(typename A::real zl, 
     if (delta <= A::c(0.667)) return A::copysign(A::mul(A::c(0.384), A::pow(h0, A::c(1.5))), A::sub(zl, zr));
     R dh = A::sub(zu, zd);
     if (dh > A::c(0.09)) return A::copysign(A::mul(A::mul(A::c(4.43), hs), A::sqrt(dh)), A::sub(zl, zr));
-    return A::copysign(A::div(A::mul(A::mul(A::mul(A::c(4.43), hs), A::c(0.3)), dh), A::c(0.1)), A::sub(zl, zr));
+    return A::copysign(A::divk(A::mul(A::mul(A::mul(A::c(4.43), hs), A::c(0.3)), dh), 0.1), A::sub(zl, zr));
 }
 
 // LAQP, functors.cu:423-443: y(x) by linear interpolation in the table (a -> b)
@@ -301,7 +355,7 @@ __device__ __forceinline__ typename A::real invariant_iter(typename A::real ql1,
     for (int k = 1; k <= 30; k++) {
         R fiar = A::madd(A::c(-6.264), shb, urb, mfiar);
         R dsum = A::add(fial, fiar), ddif = A::sub(fial, fiar);
-        urb = A::div(A::div(A::mul(A::mul(dsum, ddif), ddif), hb1), A::c(313.92));
+        urb = A::divk(A::div(A::mul(A::mul(dsum, ddif), ddif), hb1), 313.92);
         if (A::fabs(A::sub(urb, ur0)) <= A::c(tol)) break;
         ur0 = urb;
     }
@@ -337,7 +391,7 @@ __device__ __forceinline__ void bounda(const SlotIn<typename A::real> &in, const
         R hb0 = h, hb = R(0);
         for (int k = 1; k <= 20; k++) {
             R w = A::sub(fil, A::div(f0, hb0));
-            hb = A::div(A::mul(w, w), A::c(39.24));
+            hb = A::divk(A::mul(w, w), 39.24);
             if (A::fabs(A::sub(hb0, hb)) <= A::c(0.005)) break;
             hb0 = A::add(A::mul(hb0, A::c(0.5)), A::mul(hb, A::c(0.5)));
         }
@@ -486,8 +540,11 @@ __device__ __forceinline__ typename A::real pow15(typename A::real x) {
     else return A::pow(x, A::c(1.5));
 }
 
+// The branch chain of CalculateFluxKernel (functors.cu:98-200): either the
+// slot's fluxes are final (returns 0, `o` filled) or it needs Osher across the
+// edge: 1 = direct (functors.cu:151-164), 2 = mirrored (:165-200).
 template <class A, int VARIANT, class TableFetch, bool ZERO_LEN = false>
-__device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, typename A::real cl_own,
+__device__ __forceinline__ int flux_chain(const SlotIn<typename A::real> &in, typename A::real cl_own,
                                           const StepParams &p, const TableFetch &fetch,
                                           SlotOut<typename A::real> &o) {
     using R = typename A::real;
@@ -499,7 +556,6 @@ __device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, ty
     ql[0] = h1;
     ql[1] = A::dot(u1, cs, v1, sn, M_QL1);
     ql[2] = A::dot(v1, cs, -u1, sn, M_QL2);
-    R fil = A::add(ql[1], A::mul(A::c(2.0), cl_own));
     R zi = A::fmax(z1, A::add(zbc1, HM1));
     R hc, bc, zc, uc, vc;
     if (!in.has_nb) { hc = R(0); bc = R(0); zc = R(0); uc = R(0); vc = R(0); }
@@ -510,8 +566,8 @@ __device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, ty
         uc = in.nb.u;
         vc = in.nb.v;
     }
-    int route = 0;   // 1: direct Osher (functors.cu:151-164), 2: mirrored Osher (:165-200)
     if (code_is_bounda(in.code)) {
+        R fil = A::add(ql[1], A::mul(A::c(2.0), cl_own));
         bounda<A, VARIANT>(in, p, fil, ql, zc, uc, vc, fetch, o);
     } else if (h1 <= HM1 && hc <= HM1) {
         o.f[0] = R(0); o.f[1] = R(0); o.f[2] = R(0); o.f[3] = R(0);
@@ -555,51 +611,87 @@ __device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, ty
             o.f[3] = A::mul(A::mul(A::c(4.905), h1), h1);
         }
     } else if (in.code == CODE_ZERO && in.own_first) {
-        route = 1;
+        return 1;
     } else if (!in.has_nb) {
         // the reference reads H[-1] here (functors.cu:170)
         o.undefined = true;
         o.f[0] = R(0); o.f[1] = R(0); o.f[2] = R(0); o.f[3] = R(0);
     } else {
-        route = 2;
+        return 2;
     }
+    return 0;
+}
+
+// Osher's inputs across an edge.  Left cell L and right cell R, normal (cs, sn)
+// pointing from L to R: the direct route at L and the mirrored route at R see
+// the same cells and the same normal (the reversed normal of R's slot), and
+// differ only in the fused product of two rotations (M_QL2 vs M_QL2M, M_UR vs
+// M_UR1).  `mir` selects the mirrored route's fusions.
+template <class R>
+struct OsherIn { R cl, fil, hcR, ratio, ur; R ql[3], qr[3]; };
+
+template <class A>
+__device__ __forceinline__ OsherIn<typename A::real> osher_inputs(const CellState<typename A::real> &L,
+                                                                 const CellState<typename A::real> &Rc,
+                                                                 typename A::real cs, typename A::real sn,
+                                                                 typename A::real clL, bool mir, const StepParams &p) {
+    using R = typename A::real;
+    const R HM1 = A::c(p.hm1), HM2 = A::c(p.hm2);
+    OsherIn<R> o;
+    o.cl = clL;
+    o.ql[0] = L.h;
+    o.ql[1] = A::dot(L.u, cs, L.v, sn, M_QL1);                    // M_QL1 == M_QL1M
+    o.ql[2] = mir ? A::dot(L.v, cs, -L.u, sn, M_QL2M) : A::dot(L.v, cs, -L.u, sn, M_QL2);
+    o.fil = A::add(o.ql[1], A::mul(A::c(2.0), clL));
+    o.hcR = A::fmax(Rc.h, HM1);
+    const R zR = A::fmax(Rc.zbc, Rc.z);
+    o.qr[0] = A::fmax(A::sub(zR, L.zbc), HM1);
+    o.ur = mir ? A::dot(Rc.u, cs, Rc.v, sn, M_UR1) : A::dot(Rc.u, cs, Rc.v, sn, M_UR);
+    o.ratio = A::fmin(A::div(o.hcR, o.qr[0]), A::c(1.5));
+    o.qr[1] = A::mul(o.ur, o.ratio);
+    if (o.hcR <= HM2 || o.qr[0] <= HM2) o.qr[1] = A::copysign(A::c(K::VMIN), o.ur);
+    o.qr[2] = A::dot(Rc.v, cs, -Rc.u, sn, M_QR2);                 // M_QR2 == M_QR2M
+    return o;
+}
+
+// FLUX1's correction term and the two routes' epilogues (functors.cu:162-163, :191-199)
+template <class A>
+__device__ __forceinline__ typename A::real osher_f1(typename A::real fo1, typename A::real ratio,
+                                                     typename A::real hcR, typename A::real ur) {
+    return A::add(fo1, A::mul(A::mul(A::mul(A::mul(A::sub(A::c(1.0), ratio), hcR), ur), ur), A::c(0.5)));
+}
+template <class A>
+__device__ __forceinline__ typename A::real mirror_f3(typename A::real fo3, typename A::real zbcL,
+                                                      typename A::real zbc_own) {
+    using R = typename A::real;
+    R za = A::add(A::sqrt(A::divk(fo3, 4.905)), zbcL);
+    R hc3 = R(0);
+    if (za > zbc_own) hc3 = A::sub(za, zbc_own);
+    return A::mul(A::mul(A::c(4.905), hc3), hc3);
+}
+
+// CalculateFluxKernel body for one slot, functors.cu:47-202.
+// `cl_own` is sqrt(9.81*H) of the slot's cell (the caller may compute it once
+// per cell; it is bit-identical to the reference's per-slot value).
+template <class A, int VARIANT, class TableFetch, bool ZERO_LEN = false>
+__device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, typename A::real cl_own,
+                                          const StepParams &p, const TableFetch &fetch,
+                                          SlotOut<typename A::real> &o) {
+    using R = typename A::real;
+    const int route = flux_chain<A, VARIANT, TableFetch, ZERO_LEN>(in, cl_own, p, fetch, o);
     if (route == 0) return;
-    // One Osher evaluation for both routes.  Direct: left = this cell, right =
-    // the neighbour, normal (COSF, SINF).  Mirrored: left = the neighbour, right
-    // = this cell, normal reversed.  The fused products differ between the two
-    // in the reference build (M_QL2 vs M_QL2M, M_UR vs M_UR1).
     const bool mir = route == 2;
-    const R hL = mir ? in.nb.h : h1, uL = mir ? in.nb.u : u1, vL = mir ? in.nb.v : v1;
-    const R zbcL = mir ? in.nb.zbc : zbc1;
-    const R hR = mir ? h1 : in.nb.h, uR = mir ? u1 : in.nb.u, vR = mir ? v1 : in.nb.v;
-    const R zR = mir ? A::fmax(zbc1, z1) : zc;
-    const R c_ = mir ? -cs : cs, s_ = mir ? -sn : sn;
-    const R clL = mir ? A::sqrt(A::mul(A::c(9.81), hL)) : cl_own;
-    R qlx[3], qr[3], fo[4];
-    qlx[0] = hL;
-    qlx[1] = A::dot(uL, c_, vL, s_, M_QL1);                    // M_QL1 == M_QL1M
-    qlx[2] = mir ? A::dot(vL, c_, -uL, s_, M_QL2M) : A::dot(vL, c_, -uL, s_, M_QL2);
-    const R filx = A::add(qlx[1], A::mul(A::c(2.0), clL));
-    const R hcR = A::fmax(hR, HM1);
-    qr[0] = A::fmax(A::sub(zR, zbcL), HM1);
-    const R ur = mir ? A::dot(uR, c_, vR, s_, M_UR1) : A::dot(uR, c_, vR, s_, M_UR);
-    const R ratio = A::fmin(A::div(hcR, qr[0]), A::c(1.5));
-    qr[1] = A::mul(ur, ratio);
-    if (hcR <= HM2 || qr[0] <= HM2) qr[1] = A::copysign(A::c(K::VMIN), ur);
-    qr[2] = A::dot(vR, c_, -uR, s_, M_QR2);                    // M_QR2 == M_QR2M
-    osher<A>(clL, qlx, qr, filx, fo);
-    o.f[1] = A::add(fo[1], A::mul(A::mul(A::mul(A::mul(A::sub(A::c(1.0), ratio), hcR), ur), ur), A::c(0.5)));
+    const CellState<R> &L = mir ? in.nb : in.own;
+    const CellState<R> &Rc = mir ? in.own : in.nb;
+    const R cs = mir ? -in.cosj : in.cosj, sn = mir ? -in.sinj : in.sinj;
+    const R clL = mir ? A::sqrt(A::mul(A::c(9.81), in.nb.h)) : cl_own;
+    const OsherIn<R> oi = osher_inputs<A>(L, Rc, cs, sn, clL, mir, p);
+    R fo[4];
+    osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo);
+    o.f[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, oi.ur);
     o.f[2] = fo[2];
-    if (!mir) {
-        o.f[0] = fo[0];
-        o.f[3] = fo[3];
-    } else {
-        o.f[0] = -fo[0];
-        R za = A::add(A::sqrt(A::div(fo[3], A::c(4.905))), bc);
-        R hc3 = R(0);
-        if (za > zbc1) hc3 = A::sub(za, zbc1);
-        o.f[3] = A::mul(A::mul(A::c(4.905), hc3), hc3);
-    }
+    if (!mir) { o.f[0] = fo[0]; o.f[3] = fo[3]; }
+    else { o.f[0] = -fo[0]; o.f[3] = mirror_f3<A>(fo[3], in.nb.zbc, in.own.zbc); }
 }
 
 // ---------------------------------------------------------------------------
@@ -639,7 +731,7 @@ __device__ __forceinline__ CellUpdateOut<typename A::real> update_cell(const Cel
         R hside = A::fmax(c.h, HM1);
         R dt2 = A::div(c.sidex, A::add(c.u, A::sqrt(A::mul(A::c(9.81), hside))));
         dt2 = A::fmin(DT, dt2);
-        dt2 = A::fmax(dt2, A::div(DT, A::c(10.0)));
+        dt2 = A::fmax(dt2, A::divk(DT, 10.0));
         dta = A::div(dt2, c.dta_or_area);
     } else {
         dta = c.dta_or_area;

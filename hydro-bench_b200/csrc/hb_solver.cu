@@ -82,40 +82,41 @@ namespace hb {
 // ---------------------------------------------------------------------------
 enum : uint8_t { META_CODE = 0x0F, META_OWN_FIRST = 0x10, META_HAS_NB = 0x20 };
 
-// Tile configurations of the step kernel: threads per CTA (= the most real
-// slots and the most cells a tile holds) and the CTAs per SM the compiler is
-// asked to fit (__launch_bounds__), which caps the registers per thread.
-struct TileConfig { int threads, min_blocks; };
-constexpr TileConfig TILE_CONFIGS[] = {{256, 2}, {256, 3}, {256, 4}, {128, 6}, {128, 8}, {512, 2}};
-constexpr int N_TILE_CONFIGS = sizeof(TILE_CONFIGS) / sizeof(TILE_CONFIGS[0]);
-constexpr int DEFAULT_TILE_CONFIG = 2;   // (256, 4): fastest in the 207,234-cell sweep
+// Launch shapes of the flux kernel (threads per CTA, CTAs per SM asked of the
+// compiler through __launch_bounds__, which caps registers per thread).
+// (The cell kernel has 128 threads per CTA and asks for update_min_blocks.)
+struct LaunchConfig { int threads, min_blocks, update_min_blocks; };
+constexpr LaunchConfig LAUNCH_CONFIGS[] = {{128, 6, 6}, {128, 6, 8}, {128, 8, 8}, {256, 3, 6}, {256, 4, 8},
+                                           {128, 4, 6}, {256, 2, 6}, {64, 12, 8}};
+constexpr int N_LAUNCH_CONFIGS = sizeof(LAUNCH_CONFIGS) / sizeof(LAUNCH_CONFIGS[0]);
+constexpr int DEFAULT_LAUNCH_CONFIG = 0;
+constexpr int UPDATE_THREADS = 128;
 
-// Device mesh.  Cells are in reverse Cuthill-McKee order and cut into tiles of
-// consecutive cells holding at most TILE real slots; a tile is one CTA.  Real
-// slots (every slot except the zero-length fourth slot of a triangle) are
-// stored compactly, tile by tile, in slot order within each cell.
+// Device mesh.  Cells are in reverse Cuthill-McKee order.  The flux work is a
+// list of records: first the interior edges whose two slots both have code 0
+// and mirror each other exactly (reciprocal neighbours, negated normal, same
+// length), then every other real slot on its own.  The zero-length fourth slot
+// of a triangle is no record; the cell update evaluates it.
 template <class R>
 struct DevMesh {
     int C;                     // cells
     int per_day;               // steps per table interval (steps_per_day - 1)
-    int ndays, nb, nhq, ntiles;
+    int ndays, nb, nhq;
+    int npairs, nrecords;
     double hm1, hm2, jl, dt;
-    R *H[2], *U[2], *V[2], *Z[2];
+    R *S[2];                   // [C][4] state {H, U, V, Z}; a step reads S[step & 1], writes the other
     R *W;
     const R *zbc, *fnc, *dta;  // dta: DT/AREA (variant H) or AREA (variant F)
     const R *sidex;            // variant F CFL length
     const int32_t *bcell;      // [C] row of the boundary tables, -1 = none
-    const int32_t *cslot0;     // [C] first compact slot of the cell
     const uint8_t *cmask;      // [C] bit j: slot j is a real slot
-    const int32_t *tcell0;     // [ntiles+1] first cell of each tile
-    const int32_t *tslot0;     // [ntiles+1] first compact slot of each tile
-    // compact real slots [NS]
-    const int32_t *scell;      // owning cell
-    const uint8_t *sj;         // slot index j within the cell
-    const int32_t *nbr;        // neighbour (device order), -1 = none
-    uint8_t *meta;             // code | own_first | has_nb (code changes on breach)
-    const R *cosf, *sinf, *side;
-    R *f0, *f1, *f2, *f3;      // [4C] persistent fluxes, index 4*cell + j
+    R *slotw;                  // [4C][4] per-slot terms of the cell sums {F0, dWU, dWV, SIDE}
+    // records [nrecords]
+    const int4 *rix;           // {a, b, sa, sb}: cell of the slot, its neighbour (-1 = none),
+                               // slot 4*a+j, and for a pair the slot of b (-1 otherwise)
+    uint8_t *rmeta;            // code | own_first | has_nb of slot a (code changes on breach)
+    const R *rgeo;             // [nrecords][4] {COSF, SINF, SIDE, 0} of slot a
+    R *f0, *f1, *f2, *f3;      // [4C] fluxes of the last step, index 4*cell + j
     const R *bqt, *bdqt, *bzt, *bdzt;   // [ndays*nb]
     const R *btop;             // [nb]
     const int32_t *bnhq1;      // [nb]
@@ -124,130 +125,283 @@ struct DevMesh {
     const long long *step_ctr;
 };
 
-// One step of one tile.  Phase 1: a thread per real slot computes the slot's
-// flux (CalculateFluxKernel, functors.cu:47-202) into shared memory.
-// Phase 2: a thread per cell sums its four slots in order j = 0..3 and
-// updates the cell (UpdateCellKernel, functors.cu:717-784); the zero-length
-// fourth slot of a triangle is evaluated there, without pow (flux_slot's
-// ZERO_LEN).  The state is double-buffered: read (step & 1), write the other.
-template <class A, int VARIANT, int TILE, int MINB>
-__global__ void __launch_bounds__(TILE, MINB) step_kernel(DevMesh<typename A::real> m, int k, int write_flux) {
-    using R = typename A::real;
-    __shared__ R sf[4][TILE];
-    __shared__ R sg[3][TILE];
-    const long long step = *m.step_ctr + k;
-    const int par = (int)(step & 1);
-    int jt = (int)(step / m.per_day);
-    const int kt = 1 + (int)(step % m.per_day);
-    if (jt >= m.ndays) {   // beyond the boundary tables: never read past them
-        if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(m.err, ERRBIT_TABLE_RANGE);
-        jt = m.ndays - 1;
-    }
-    const R *__restrict__ H = m.H[par];
-    const R *__restrict__ U = m.U[par];
-    const R *__restrict__ V = m.V[par];
-    const R *__restrict__ Z = m.Z[par];
-    const StepParams p{m.hm1, m.hm2, m.jl, m.dt, kt, jt};
-    const int tile = blockIdx.x;
-    const int t = threadIdx.x;
-    const int c0 = m.tcell0[tile], c1 = m.tcell0[tile + 1];
-    const int s0 = m.tslot0[tile], s1 = m.tslot0[tile + 1];
+struct StepIndex { int par, kt, jt; };
 
-    if (s0 + t < s1) {
-        const int s = s0 + t;
-        const int c = m.scell[s];
-        const int j = m.sj[s];
-        SlotIn<R> in;
-        in.own = {H[c], U[c], V[c], Z[c], m.zbc[c]};
-        const uint8_t meta = m.meta[s];
-        const int nb = m.nbr[s];
-        in.code = (int8_t)(meta & META_CODE);
-        in.own_first = meta & META_OWN_FIRST;
-        in.has_nb = meta & META_HAS_NB;
-        if (in.has_nb) in.nb = {H[nb], U[nb], V[nb], Z[nb], m.zbc[nb]};
-        else in.nb = {R(0), R(0), R(0), R(0), R(0)};
-        in.cosj = m.cosf[s];
-        in.sinj = m.sinf[s];
-        in.side = m.side[s];
-        auto fetch = [&]() {
-            BoundaryIn<R> b;
-            const int r = m.bcell[c];
-            if (r >= 0) {
-                const size_t q = (size_t)jt * m.nb + r;
-                b.qt = m.bqt[q]; b.dqt = m.bdqt[q]; b.zt = m.bzt[q]; b.dzt = m.bdzt[q];
-                b.top = m.btop[r]; b.nhq1 = m.bnhq1[r];
-                b.zw = m.bzw + (size_t)r * m.nhq; b.qw = m.bqw + (size_t)r * m.nhq;
-            } else {
-                b.qt = b.dqt = b.zt = b.dzt = b.top = R(0); b.nhq1 = 0;
-                b.zw = m.bzw + (size_t)m.nb * m.nhq; b.qw = m.bqw + (size_t)m.nb * m.nhq;
+template <class R>
+__device__ __forceinline__ StepIndex step_index(const DevMesh<R> &m, int k) {
+    const long long step = *m.step_ctr + k;
+    StepIndex si;
+    si.par = (int)(step & 1);
+    si.jt = (int)(step / m.per_day);
+    si.kt = 1 + (int)(step % m.per_day);
+    if (si.jt >= m.ndays) {   // beyond the boundary tables: never read past them
+        if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(m.err, ERRBIT_TABLE_RANGE);
+        si.jt = m.ndays - 1;
+    }
+    return si;
+}
+
+template <class R> struct Vec4 { R x, y, z, w; };
+__device__ __forceinline__ Vec4<double> ld4(const double *p) {
+    const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+    return {a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ Vec4<float> ld4(const float *p) {
+    const float4 a = *reinterpret_cast<const float4 *>(p);
+    return {a.x, a.y, a.z, a.w};
+}
+__device__ __forceinline__ void st4(double *p, double x, double y, double z, double w) {
+    *reinterpret_cast<double2 *>(p) = make_double2(x, y);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2(z, w);
+}
+__device__ __forceinline__ void st4(float *p, float x, float y, float z, float w) {
+    *reinterpret_cast<float4 *>(p) = make_float4(x, y, z, w);
+}
+
+template <class R>
+__device__ __forceinline__ CellState<R> load_cell(const DevMesh<R> &m, int par, int c) {
+    const Vec4<R> v = ld4(m.S[par] + 4 * (size_t)c);
+    return {v.x, v.y, v.z, v.w, m.zbc[c]};
+}
+
+// the slot's terms of the cell sums (functors.cu:733-741): F0 and SIDE for
+// WH = fma(SIDE, F0, WH), and the complete WU / WV increments
+template <class A>
+__device__ __forceinline__ void store_terms(const DevMesh<typename A::real> &m, int s, const typename A::real f[4],
+                                            typename A::real side, typename A::real cs, typename A::real sn) {
+    using R = typename A::real;
+    const R fr1 = A::add(f[1], f[3]);
+    const R slcos = A::mul(side, cs), slsin = A::mul(side, sn);
+    const R dwu = A::dot(slcos, fr1, -slsin, f[2], M_WU);
+    const R dwv = A::dot(slsin, fr1, slcos, f[2], M_WV);
+    st4(m.slotw + 4 * (size_t)s, f[0], dwu, dwv, side);
+}
+
+template <class R>
+__device__ __forceinline__ void store_flux(const DevMesh<R> &m, int s, const R f[4]) {
+    m.f0[s] = f[0]; m.f1[s] = f[1]; m.f2[s] = f[2]; m.f3[s] = f[3];
+}
+
+// One slot on its own: flux_slot with its boundary tables (functors.cu:47-202).
+template <class A, int VARIANT>
+__device__ __forceinline__ void single_record(const DevMesh<typename A::real> &m, int r, const StepIndex &si,
+                                              const StepParams &p, int write_flux) {
+    using R = typename A::real;
+    const int4 ix = m.rix[r];
+    const int a = ix.x, b = ix.y, sa = ix.z;
+    const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
+    SlotIn<R> in;
+    in.own = load_cell(m, si.par, a);
+    const uint8_t meta = m.rmeta[r];
+    in.code = (int8_t)(meta & META_CODE);
+    in.own_first = meta & META_OWN_FIRST;
+    in.has_nb = meta & META_HAS_NB;
+    in.nb = in.has_nb ? load_cell(m, si.par, b) : CellState<R>{R(0), R(0), R(0), R(0), R(0)};
+    in.cosj = g.x; in.sinj = g.y; in.side = g.z;
+    auto fetch = [&]() {
+        BoundaryIn<R> bi;
+        const int row = m.bcell[a];
+        if (row >= 0) {
+            const size_t q = (size_t)si.jt * m.nb + row;
+            bi.qt = m.bqt[q]; bi.dqt = m.bdqt[q]; bi.zt = m.bzt[q]; bi.dzt = m.bdzt[q];
+            bi.top = m.btop[row]; bi.nhq1 = m.bnhq1[row];
+            bi.zw = m.bzw + (size_t)row * m.nhq; bi.qw = m.bqw + (size_t)row * m.nhq;
+        } else {
+            bi.qt = bi.dqt = bi.zt = bi.dzt = bi.top = R(0); bi.nhq1 = 0;
+            bi.zw = m.bzw + (size_t)m.nb * m.nhq; bi.qw = m.bqw + (size_t)m.nb * m.nhq;
+        }
+        bi.nhq = m.nhq;
+        return bi;
+    };
+    const R cl = A::sqrt(A::mul(A::c(9.81), in.own.h));
+    SlotOut<R> o;
+    flux_slot<A, VARIANT>(in, cl, p, fetch, o);
+    if (o.mask != 0xF) {   // codes that leave fluxes unwritten keep the old values (functors.cu:525-565)
+        if (!(o.mask & 1)) o.f[0] = m.f0[sa];
+        if (!(o.mask & 2)) o.f[1] = m.f1[sa];
+        if (!(o.mask & 4)) o.f[2] = m.f2[sa];
+        if (!(o.mask & 8)) o.f[3] = m.f3[sa];
+    }
+    if (write_flux || o.mask != 0xF) store_flux(m, sa, o.f);
+    store_terms<A>(m, sa, o.f, in.side, in.cosj, in.sinj);
+    if (o.klas_to_zero) m.rmeta[r] = (uint8_t)((meta & ~META_CODE) | CODE_ZERO);
+    if (o.undefined) atomicOr(m.err, ERRBIT_UNDEFINED);
+}
+
+// The mirrored Osher of a pair computed on its own (when its inputs differ
+// from the direct route's in the normal velocity).
+template <class A>
+__device__ __forceinline__ void pair_mirror(const DevMesh<typename A::real> &m, int r, const StepIndex &si,
+                                            const StepParams &p, int write_flux) {
+    using R = typename A::real;
+    const int4 ix = m.rix[r];
+    const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
+    const CellState<R> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
+    const R cs = g.x, sn = g.y;
+    const R clA = A::sqrt(A::mul(A::c(9.81), A_.h));
+    const OsherIn<R> oi = osher_inputs<A>(A_, B_, cs, sn, clA, true, p);
+    R fo[4], fb[4];
+    osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo);
+    fb[0] = -fo[0];
+    fb[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, oi.ur);
+    fb[2] = fo[2];
+    fb[3] = mirror_f3<A>(fo[3], A_.zbc, B_.zbc);
+    if (write_flux) store_flux(m, ix.w, fb);
+    store_terms<A>(m, ix.w, fb, g.z, -cs, -sn);
+}
+
+template <class R>
+__device__ __forceinline__ bool same_bits(R a, R b) {
+    if constexpr (sizeof(R) == 8) return __double_as_longlong((double)a) == __double_as_longlong((double)b);
+    else return __float_as_int((float)a) == __float_as_int((float)b);
+}
+
+// Flux of every record of one step.  A pair evaluates both slots' branch
+// chains (functors.cu:98-150) and, when both reach Osher, runs it once: the
+// direct route at a and the mirrored route at b have the same cells, normal
+// and inputs except two rotations that the reference build rounds
+// differently.  When those agree bit for bit the two Osher evaluations are
+// identical, and the b side's FLUX2 is re-summed with its own tangent if only
+// that differs; otherwise the pair goes to a per-CTA queue whose mirrored
+// Osher evaluations run together after the main pass.
+template <class A, int VARIANT, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<typename A::real> m, int k, int write_flux) {
+    using R = typename A::real;
+    __shared__ int queue[THREADS];
+    __shared__ int qn;
+    if (threadIdx.x == 0) qn = 0;
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
+    const StepIndex si = step_index(m, k);
+    const StepParams p{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
+    __syncthreads();
+    const int r = blockIdx.x * THREADS + threadIdx.x;
+    if (r < m.npairs) {
+        const int4 ix = m.rix[r];
+        const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
+        const CellState<R> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
+        const R cs = g.x, sn = g.y;
+        const R clA = A::sqrt(A::mul(A::c(9.81), A_.h));
+        auto nofetch = []() { return BoundaryIn<R>{}; };
+        SlotIn<R> ia, ib;
+        ia.own = A_; ia.nb = B_; ia.has_nb = true; ia.own_first = true; ia.code = CODE_ZERO;
+        ia.cosj = cs; ia.sinj = sn; ia.side = g.z;
+        ib.own = B_; ib.nb = A_; ib.has_nb = true; ib.own_first = false; ib.code = CODE_ZERO;
+        ib.cosj = -cs; ib.sinj = -sn; ib.side = ia.side;
+        // each side's branch chain; a side whose fluxes are final is written at once
+        int ra_, rb_;
+        {
+            SlotOut<R> oa;
+            ra_ = flux_chain<A, VARIANT>(ia, clA, p, nofetch, oa);   // 0 or 1 (direct)
+            if (!ra_) {
+                if (write_flux) store_flux(m, ix.z, oa.f);
+                store_terms<A>(m, ix.z, oa.f, g.z, cs, sn);
             }
-            b.nhq = m.nhq;
-            return b;
-        };
-        const R cl = A::sqrt(A::mul(A::c(9.81), in.own.h));
-        SlotOut<R> o;
-        flux_slot<A, VARIANT>(in, cl, p, fetch, o);
-        const size_t fs = 4 * (size_t)c + j;
-        if (o.mask != 0xF) {   // codes that leave fluxes unwritten keep the old values
-            if (!(o.mask & 1)) o.f[0] = m.f0[fs];
-            if (!(o.mask & 2)) o.f[1] = m.f1[fs];
-            if (!(o.mask & 4)) o.f[2] = m.f2[fs];
-            if (!(o.mask & 8)) o.f[3] = m.f3[fs];
         }
-        if (write_flux || in.code == CODE_BOUNDA_OTHER) {
-            m.f0[fs] = o.f[0]; m.f1[fs] = o.f[1]; m.f2[fs] = o.f[2]; m.f3[fs] = o.f[3];
+        {
+            SlotOut<R> ob;
+            rb_ = flux_chain<A, VARIANT>(ib, R(0), p, nofetch, ob);  // 0 or 2 (mirrored)
+            if (!rb_) {
+                if (write_flux) store_flux(m, ix.w, ob.f);
+                store_terms<A>(m, ix.w, ob.f, g.z, -cs, -sn);
+            }
         }
-        if (o.klas_to_zero) m.meta[s] = (uint8_t)((meta & ~META_CODE) | CODE_ZERO);
-        if (o.undefined) atomicOr(m.err, ERRBIT_UNDEFINED);
-        sf[0][t] = o.f[0]; sf[1][t] = o.f[1]; sf[2][t] = o.f[2]; sf[3][t] = o.f[3];
-        sg[0][t] = in.side; sg[1][t] = in.cosj; sg[2][t] = in.sinj;
+        if (ra_ | rb_) {
+            // the two routes' inputs differ only in QL2, UR and so QR1 (osher_inputs)
+            OsherIn<R> oi = osher_inputs<A>(A_, B_, cs, sn, clA, ra_ == 0, p);
+            const R ql2_d = oi.ql[2], ur_d = oi.ur, qr1_d = oi.qr[1];
+            const R ql2_m = ra_ ? A::dot(A_.v, cs, -A_.u, sn, M_QL2M) : ql2_d;
+            const R ur_m = ra_ ? A::dot(B_.u, cs, B_.v, sn, M_UR1) : ur_d;
+            R qr1_m = A::mul(ur_m, oi.ratio);
+            if (oi.hcR <= A::c(p.hm2) || oi.qr[0] <= A::c(p.hm2)) qr1_m = A::copysign(A::c(K::VMIN), ur_m);
+            R fo[4];
+            OsherTrace<R> tr;
+            osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo, &tr);
+            if (ra_) {
+                R f[4];
+                f[0] = fo[0];
+                f[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, ur_d);
+                f[2] = fo[2];
+                f[3] = fo[3];
+                if (write_flux) store_flux(m, ix.z, f);
+                store_terms<A>(m, ix.z, f, g.z, cs, sn);
+            }
+            if (rb_) {
+                if (!ra_ || same_bits(qr1_d, qr1_m)) {
+                    R f[4];
+                    f[0] = -fo[0];
+                    f[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, ur_m);
+                    f[2] = (!ra_ || same_bits(ql2_d, ql2_m)) ? fo[2] : osher_f2<A>(tr, ql2_m, oi.qr[2]);
+                    f[3] = mirror_f3<A>(fo[3], A_.zbc, B_.zbc);
+                    if (write_flux) store_flux(m, ix.w, f);
+                    store_terms<A>(m, ix.w, f, g.z, -cs, -sn);
+                } else {
+                    queue[atomicAdd(&qn, 1)] = r;
+                }
+            }
+        }
+    } else if (r < m.nrecords) {
+        single_record<A, VARIANT>(m, r, si, p, write_flux);
     }
     __syncthreads();
-    if (c0 + t >= c1) return;
-    const int c = c0 + t;
-    const R h = H[c], u = U[c], v = V[c], z = Z[c], zbc = m.zbc[c];
+    for (int i = threadIdx.x; i < qn; i += THREADS) pair_mirror<A>(m, queue[i], si, p, write_flux);
+}
+
+// Sums and update of every cell (UpdateCellKernel, functors.cu:717-784).  The
+// zero-length fourth slot of a triangle is evaluated here without pow
+// (flux_slot's ZERO_LEN), exactly when fluxes are written out.
+template <class A, int VARIANT, int UMINB>
+__global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<typename A::real> m, int k, int write_flux) {
+    using R = typename A::real;
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
+    const StepIndex si = step_index(m, k);
+    const StepParams p{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
+    for (int c = blockIdx.x * UPDATE_THREADS + threadIdx.x; c < m.C; c += gridDim.x * UPDATE_THREADS) {
+    const CellState<R> st = load_cell(m, si.par, c);
     const unsigned mask = m.cmask[c];
-    int q = m.cslot0[c] - s0;
+    const R fnc = m.fnc[c], dta = m.dta[c], sidex = VARIANT == 1 ? m.sidex[c] : R(0);
+    Vec4<R> t[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) t[j] = ld4(m.slotw + 16 * (size_t)c + 4 * j);
     R wh = R(0), wu = R(0), wv = R(0);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-        R f0, f1, f2, f3, sd, cs, sn;
+        const int s = 4 * c + j;
         if (mask & (1u << j)) {
-            f0 = sf[0][q]; f1 = sf[1][q]; f2 = sf[2][q]; f3 = sf[3][q];
-            sd = sg[0][q]; cs = sg[1][q]; sn = sg[2][q];
-            q++;
+            // F0 and SIDE for WH; the WU/WV increments were formed by the flux kernel
+            wh = A::madd(t[j].w, t[j].x, wh, M_WH);
+            wu = A::add(wu, t[j].y);
+            wv = A::add(wv, t[j].z);
         } else {
-            // zero-length slot without neighbour, code 0, COSF = SINF = SIDE = 0
             SlotIn<R> in;
-            in.own = {h, u, v, z, zbc};
+            in.own = st;
             in.nb = {R(0), R(0), R(0), R(0), R(0)};
             in.has_nb = false; in.own_first = false; in.code = CODE_ZERO;
             in.cosj = R(0); in.sinj = R(0); in.side = R(0);
             auto nofetch = []() { return BoundaryIn<R>{}; };
-            const R cl = A::sqrt(A::mul(A::c(9.81), h));
             SlotOut<R> o;
             if (write_flux) {
-                flux_slot<A, VARIANT, decltype(nofetch), false>(in, cl, p, nofetch, o);
-                const size_t fs = 4 * (size_t)c + j;
-                m.f0[fs] = o.f[0]; m.f1[fs] = o.f[1]; m.f2[fs] = o.f[2]; m.f3[fs] = o.f[3];
+                flux_slot<A, VARIANT, decltype(nofetch), false>(in, A::sqrt(A::mul(A::c(9.81), st.h)), p, nofetch, o);
+                store_flux(m, s, o.f);
             } else {
-                flux_slot<A, VARIANT, decltype(nofetch), true>(in, cl, p, nofetch, o);
+                flux_chain<A, VARIANT, decltype(nofetch), true>(in, R(0), p, nofetch, o);
             }
-            f0 = o.f[0]; f1 = o.f[1]; f2 = o.f[2]; f3 = o.f[3];
-            sd = R(0); cs = R(0); sn = R(0);
+            // zero-length slot: SIDE = SLCOS = SLSIN = 0 (mesh.cpp:293-306, :347-370)
+            wsum_add<A>(wh, wu, wv, o.f[0], o.f[1], o.f[2], o.f[3], R(0), R(0), R(0));
         }
-        // SLCOS = SIDE*COSF, SLSIN = SIDE*SINF (mesh.cpp:368-369): one rounded product each
-        wsum_add<A>(wh, wu, wv, f0, f1, f2, f3, sd, A::mul(sd, cs), A::mul(sd, sn));
     }
     CellUpdateIn<R> ci;
-    ci.h = h; ci.u = u; ci.v = v; ci.zbc = zbc;
-    ci.fnc = m.fnc[c];
-    ci.dta_or_area = m.dta[c];
-    ci.sidex = VARIANT == 1 ? m.sidex[c] : R(0);
-    CellUpdateOut<R> r = update_cell<A, VARIANT>(ci, wh, wu, wv, p);
-    const int np = par ^ 1;
-    m.H[np][c] = r.h; m.U[np][c] = r.u; m.V[np][c] = r.v; m.Z[np][c] = r.z; m.W[c] = r.w;
-    if (!(isfinite((double)r.h) && isfinite((double)r.u) && isfinite((double)r.v))) atomicOr(m.err, ERRBIT_NONFINITE);
+    ci.h = st.h; ci.u = st.u; ci.v = st.v; ci.zbc = st.zbc;
+    ci.fnc = fnc;
+    ci.dta_or_area = dta;
+    ci.sidex = sidex;
+    CellUpdateOut<R> o = update_cell<A, VARIANT>(ci, wh, wu, wv, p);
+    const int np = si.par ^ 1;
+    st4(m.S[np] + 4 * (size_t)c, o.h, o.u, o.v, o.z);
+    m.W[c] = o.w;
+    if (!(isfinite((double)o.h) && isfinite((double)o.u) && isfinite((double)o.v))) atomicOr(m.err, ERRBIT_NONFINITE);
+    }
 }
 
 __global__ void tick_kernel(long long *ctr, int n) { *ctr += n; }
@@ -255,28 +409,27 @@ __global__ void tick_kernel(long long *ctr, int n) { *ctr += n; }
 // reference-order staging <-> device-order state (perm[new] = old)
 template <class R>
 __global__ void stage_in_kernel(int C, const int32_t *__restrict__ perm, const double *__restrict__ stage,
-                                const long long *ctr, R *H0, R *U0, R *V0, R *Z0, R *H1, R *U1, R *V1, R *Z1) {
+                                const long long *ctr, R *S0, R *S1) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C) return;
     const int o = perm[i];
-    const bool odd = (*ctr) & 1;
-    (odd ? H1 : H0)[i] = (R)stage[o];
-    (odd ? U1 : U0)[i] = (R)stage[(size_t)C + o];
-    (odd ? V1 : V0)[i] = (R)stage[2 * (size_t)C + o];
-    (odd ? Z1 : Z0)[i] = (R)stage[3 * (size_t)C + o];
+    R *d = (((*ctr) & 1) ? S1 : S0) + 4 * (size_t)i;
+    d[0] = (R)stage[o];
+    d[1] = (R)stage[(size_t)C + o];
+    d[2] = (R)stage[2 * (size_t)C + o];
+    d[3] = (R)stage[3 * (size_t)C + o];
 }
 template <class R>
 __global__ void stage_out_kernel(int C, const int32_t *__restrict__ perm, double *__restrict__ stage,
-                                 const long long *ctr, const R *H0, const R *U0, const R *V0, const R *Z0,
-                                 const R *H1, const R *U1, const R *V1, const R *Z1, const R *W) {
+                                 const long long *ctr, const R *S0, const R *S1, const R *W) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C) return;
     const int o = perm[i];
-    const bool odd = (*ctr) & 1;
-    stage[o] = (double)(odd ? H1 : H0)[i];
-    stage[(size_t)C + o] = (double)(odd ? U1 : U0)[i];
-    stage[2 * (size_t)C + o] = (double)(odd ? V1 : V0)[i];
-    stage[3 * (size_t)C + o] = (double)(odd ? Z1 : Z0)[i];
+    const R *d = (((*ctr) & 1) ? S1 : S0) + 4 * (size_t)i;
+    stage[o] = (double)d[0];
+    stage[(size_t)C + o] = (double)d[1];
+    stage[2 * (size_t)C + o] = (double)d[2];
+    stage[3 * (size_t)C + o] = (double)d[3];
     stage[4 * (size_t)C + o] = (double)W[i];
 }
 
@@ -375,13 +528,12 @@ struct hb_handle {
     int32_t *d_perm = nullptr;       // perm on the device
     std::vector<int32_t> slot_index; // [4C] device-order slot -> compact real slot, -1 = zero-length slot
     int nslots = 0;
-    int ntiles() const { return fp32() ? m32.ntiles : m64.ntiles; }
     double *d_stage = nullptr;       // [5C] reference-order staging for hb_step_host
     long long steps_done = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int graph_steps = 0;
-    int tile_config = 0;             // index into TILE_CONFIGS
+    int launch_config = 0;           // index into LAUNCH_CONFIGS
     bool fp32() const { return opt.precision == HB_FP32; }
     ~hb_handle() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -467,39 +619,53 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
                 needs_table[i] = 1;
         }
     }
-    // tiles of consecutive cells with at most TILE real slots (and TILE cells)
-    std::vector<int32_t> tcell0{0}, tslot0{0}, cslot0(C), scell, nbr;
-    std::vector<uint8_t> cmask(C), sj, meta;
-    std::vector<R> scos, ssin, sside;
-    h->slot_index.assign(S, -1);
-    int tile_slots = 0, tile_cells = 0;
+    // records: exact mirror pairs first, then every other real slot
+    std::vector<uint8_t> cmask(C, 0);
+    for (int i = 0; i < C; i++)
+        for (int j = 0; j < 4; j++)
+            if (real4[4 * (size_t)i + j]) cmask[i] |= (uint8_t)(1u << j);
+    std::vector<char> paired(S, 0);
+    std::vector<int32_t> ra, rb, rsa, rsb;
+    std::vector<uint8_t> rmeta;
+    std::vector<R> rcos, rsin, rside;
+    auto slot_of = [&](int i, int j) { return 4 * (size_t)perm[i] + j; };   // reference slot of device slot
     for (int i = 0; i < C; i++) {
-        int nreal = 0;
-        for (int j = 0; j < 4; j++) nreal += real4[4 * (size_t)i + j];
-        const int TILE = hb::TILE_CONFIGS[h->tile_config].threads;
-        if (tile_slots + nreal > TILE || tile_cells + 1 > TILE) {
-            tcell0.push_back(i);
-            tslot0.push_back((int32_t)scell.size());
-            tile_slots = 0; tile_cells = 0;
-        }
-        cslot0[i] = (int32_t)scell.size();
-        uint8_t mk = 0;
         for (int j = 0; j < 4; j++) {
-            const size_t sn = 4 * (size_t)i + j, so = 4 * (size_t)perm[i] + j;
-            if (!real4[sn]) continue;
-            mk |= (uint8_t)(1u << j);
-            h->slot_index[sn] = (int32_t)scell.size();
-            scell.push_back(i); sj.push_back((uint8_t)j); nbr.push_back(nbr4[sn]); meta.push_back(meta4[sn]);
-            scos.push_back((R)md->cosf[so]); ssin.push_back((R)md->sinf[so]); sside.push_back((R)md->side[so]);
+            const size_t sn = 4 * (size_t)i + j;
+            if (!real4[sn] || paired[sn] || (meta4[sn] & hb::META_CODE) != hb::CODE_ZERO || nbr4[sn] < 0) continue;
+            if (!(meta4[sn] & hb::META_OWN_FIRST)) continue;      // the pair is listed from its lower-numbered side
+            const int nb = nbr4[sn];
+            int jb = -1;
+            for (int q = 0; q < 4; q++)
+                if (nbr4[4 * (size_t)nb + q] == i && !paired[4 * (size_t)nb + q]) { jb = q; break; }
+            if (jb < 0) continue;
+            const size_t sb = 4 * (size_t)nb + jb;
+            const size_t oa = slot_of(i, j), ob = slot_of(nb, jb);
+            // the two slots must see one edge: code 0 both, negated normal, same length
+            if ((meta4[sb] & hb::META_CODE) != hb::CODE_ZERO || !real4[sb] || md->cosf[ob] != -md->cosf[oa] ||
+                md->sinf[ob] != -md->sinf[oa] || md->side[ob] != md->side[oa])
+                continue;
+            paired[sn] = paired[sb] = 1;
+            ra.push_back(i); rb.push_back(nb); rsa.push_back((int32_t)sn); rsb.push_back((int32_t)sb);
+            rmeta.push_back(meta4[sn]);
+            rcos.push_back((R)md->cosf[oa]); rsin.push_back((R)md->sinf[oa]); rside.push_back((R)md->side[oa]);
         }
-        cmask[i] = mk;
-        tile_slots += nreal;
-        tile_cells += 1;
     }
-    tcell0.push_back(C);
-    tslot0.push_back((int32_t)scell.size());
-    m.ntiles = (int)tcell0.size() - 1;
-    h->nslots = (int)scell.size();
+    m.npairs = (int)ra.size();
+    h->slot_index.assign(S, -1);
+    for (int i = 0; i < C; i++) {
+        for (int j = 0; j < 4; j++) {
+            const size_t sn = 4 * (size_t)i + j;
+            if (!real4[sn] || paired[sn]) continue;
+            h->slot_index[sn] = (int32_t)ra.size();
+            const size_t so = slot_of(i, j);
+            ra.push_back(i); rb.push_back(nbr4[sn]); rsa.push_back((int32_t)sn); rsb.push_back(-1);
+            rmeta.push_back(meta4[sn]);
+            rcos.push_back((R)md->cosf[so]); rsin.push_back((R)md->sinf[so]); rside.push_back((R)md->side[so]);
+        }
+    }
+    m.nrecords = (int)ra.size();
+    h->nslots = m.nrecords;
     // compact boundary tables
     std::vector<int32_t> bcell(C, -1);
     std::vector<int> rows;
@@ -532,17 +698,19 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
     R *area_d = nullptr, *side_d = nullptr;
     TRY(dev_upload(h, &area_d, cellv(md->area)));
     TRY(dev_upload(h, &side_d, slotv(md->side)));   // [4C], for the per-cell setup only
-    TRY(dev_upload(h, &rp, sside)); m.side = rp;
-    TRY(dev_upload(h, &rp, scos)); m.cosf = rp;
-    TRY(dev_upload(h, &rp, ssin)); m.sinf = rp;
-    TRY(dev_upload(h, &ip, nbr)); m.nbr = ip;
-    TRY(dev_upload(h, &up, meta)); m.meta = up;
-    TRY(dev_upload(h, &ip, scell)); m.scell = ip;
-    TRY(dev_upload(h, &up, sj)); m.sj = up;
-    TRY(dev_upload(h, &ip, cslot0)); m.cslot0 = ip;
     TRY(dev_upload(h, &up, cmask)); m.cmask = up;
-    TRY(dev_upload(h, &ip, tcell0)); m.tcell0 = ip;
-    TRY(dev_upload(h, &ip, tslot0)); m.tslot0 = ip;
+    {
+        std::vector<int4> rix(ra.size());
+        std::vector<R> rgeo(4 * ra.size(), R(0));
+        for (size_t r = 0; r < ra.size(); r++) {
+            rix[r] = make_int4(ra[r], rb[r], rsa[r], rsb[r]);
+            rgeo[4 * r] = rcos[r]; rgeo[4 * r + 1] = rsin[r]; rgeo[4 * r + 2] = rside[r];
+        }
+        int4 *ixp; R *gp;
+        TRY(dev_upload(h, &ixp, rix)); m.rix = ixp;
+        TRY(dev_upload(h, &gp, rgeo)); m.rgeo = gp;
+    }
+    TRY(dev_upload(h, &up, rmeta)); m.rmeta = up;
     TRY(dev_upload(h, &ip, bcell)); m.bcell = ip;
     TRY(dev_upload(h, &rp, bqt)); m.bqt = rp;
     TRY(dev_upload(h, &rp, bdqt)); m.bdqt = rp;
@@ -552,10 +720,8 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
     TRY(dev_upload(h, &ip, bnhq1)); m.bnhq1 = ip;
     TRY(dev_upload(h, &rp, bzw)); m.bzw = rp;
     TRY(dev_upload(h, &rp, bqw)); m.bqw = rp;
-    for (int b = 0; b < 2; b++) {
-        TRY(dev_alloc(h, &m.H[b], C)); TRY(dev_alloc(h, &m.U[b], C));
-        TRY(dev_alloc(h, &m.V[b], C)); TRY(dev_alloc(h, &m.Z[b], C));
-    }
+    for (int b = 0; b < 2; b++) TRY(dev_alloc(h, &m.S[b], 4 * (size_t)C));
+    TRY(dev_alloc(h, &m.slotw, 16 * (size_t)C));
     TRY(dev_alloc(h, &m.W, C));
     TRY(dev_alloc(h, &m.f0, S)); TRY(dev_alloc(h, &m.f1, S));
     TRY(dev_alloc(h, &m.f2, S)); TRY(dev_alloc(h, &m.f3, S));
@@ -578,18 +744,43 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
 
 template <class A, int VARIANT>
 int launch_steps(hb_handle *h, hb::DevMesh<typename A::real> &m, int n, cudaStream_t st) {
-    const int grid = m.ntiles;
-    auto go = [&](auto kern, int threads) {
-        for (int k = 0; k < n; k++) kern<<<grid, threads, 0, st>>>(m, k, k == n - 1);
+    // Programmatic dependent launch: each kernel may start while its predecessor
+    // drains and waits in cudaGridDependencySynchronize for its results.
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg_u{};
+    int nsm = 0, per_sm = 0;
+    HB_CUDA_RET(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->opt.device));
+    (void)per_sm;
+    cfg_u.gridDim = dim3((unsigned)std::max(1, (h->C + hb::UPDATE_THREADS - 1) / hb::UPDATE_THREADS));
+    cfg_u.blockDim = dim3(hb::UPDATE_THREADS);
+    cfg_u.stream = st;
+    cfg_u.attrs = attr;
+    cfg_u.numAttrs = 1;
+    auto go = [&](auto flux, int threads, auto update) -> int {
+        cudaLaunchConfig_t cfg_f = cfg_u;
+        cfg_f.gridDim = dim3((unsigned)std::max(1, (m.nrecords + threads - 1) / threads));
+        cfg_f.blockDim = dim3(threads);
+        for (int k = 0; k < n; k++) {
+            HB_CUDA_RET(cudaLaunchKernelEx(&cfg_f, flux, m, k, (int)(k == n - 1)));
+            HB_CUDA_RET(cudaLaunchKernelEx(&cfg_u, update, m, k, (int)(k == n - 1)));
+        }
+        return HB_OK;
     };
-    switch (h->tile_config) {
-    case 0: go(hb::step_kernel<A, VARIANT, 256, 2>, 256); break;
-    case 1: go(hb::step_kernel<A, VARIANT, 256, 3>, 256); break;
-    case 2: go(hb::step_kernel<A, VARIANT, 256, 4>, 256); break;
-    case 3: go(hb::step_kernel<A, VARIANT, 128, 6>, 128); break;
-    case 4: go(hb::step_kernel<A, VARIANT, 128, 8>, 128); break;
-    default: go(hb::step_kernel<A, VARIANT, 512, 2>, 512); break;
+    int rc;
+    using namespace hb;
+    switch (h->launch_config) {
+    case 0: rc = go(flux_kernel<A, VARIANT, 128, 6>, 128, update_kernel<A, VARIANT, 6>); break;
+    case 1: rc = go(flux_kernel<A, VARIANT, 128, 6>, 128, update_kernel<A, VARIANT, 8>); break;
+    case 2: rc = go(flux_kernel<A, VARIANT, 128, 8>, 128, update_kernel<A, VARIANT, 8>); break;
+    case 3: rc = go(flux_kernel<A, VARIANT, 256, 3>, 256, update_kernel<A, VARIANT, 6>); break;
+    case 4: rc = go(flux_kernel<A, VARIANT, 256, 4>, 256, update_kernel<A, VARIANT, 8>); break;
+    case 5: rc = go(flux_kernel<A, VARIANT, 128, 4>, 128, update_kernel<A, VARIANT, 6>); break;
+    case 6: rc = go(flux_kernel<A, VARIANT, 256, 2>, 256, update_kernel<A, VARIANT, 6>); break;
+    default: rc = go(flux_kernel<A, VARIANT, 64, 12>, 64, update_kernel<A, VARIANT, 8>); break;
     }
+    if (rc != HB_OK) return rc;
     hb::tick_kernel<<<1, 1, 0, st>>>(h->d_ctr, n);
     HB_CUDA_RET(cudaGetLastError());
     return HB_OK;
@@ -613,11 +804,11 @@ int check_range(hb_handle *h, long long n) {
 }  // namespace
 
 extern "C" int hb_tile_configs(int32_t *threads, int32_t *min_blocks, int32_t capacity) {
-    for (int i = 0; i < hb::N_TILE_CONFIGS && i < capacity; i++) {
-        if (threads) threads[i] = hb::TILE_CONFIGS[i].threads;
-        if (min_blocks) min_blocks[i] = hb::TILE_CONFIGS[i].min_blocks;
+    for (int i = 0; i < hb::N_LAUNCH_CONFIGS && i < capacity; i++) {
+        if (threads) threads[i] = hb::LAUNCH_CONFIGS[i].threads;
+        if (min_blocks) min_blocks[i] = hb::LAUNCH_CONFIGS[i].min_blocks * 100 + hb::LAUNCH_CONFIGS[i].update_min_blocks;
     }
-    return hb::N_TILE_CONFIGS;
+    return hb::N_LAUNCH_CONFIGS;
 }
 
 extern "C" int hb_create(const hb_mesh_desc *md, const hb_options *opt_in, hb_handle **out) {
@@ -641,11 +832,11 @@ extern "C" int hb_create(const hb_mesh_desc *md, const hb_options *opt_in, hb_ha
     h->C = md->cells; h->ndays = md->ndays; h->nhq = md->nhq;
     h->steps_per_day = md->steps_per_day; h->per_day = md->steps_per_day - 1;
     h->dt = md->dt; h->hm1 = md->hm1; h->hm2 = md->hm2; h->jl = md->jl;
-    if (opt.tile_config < 0 || opt.tile_config > hb::N_TILE_CONFIGS) {
+    if (opt.tile_config < 0 || opt.tile_config > hb::N_LAUNCH_CONFIGS) {
         delete h;
-        return hb::set_error(HB_E_INVALID, "hb_create: tile_config %d outside 0..%d", opt.tile_config, hb::N_TILE_CONFIGS);
+        return hb::set_error(HB_E_INVALID, "hb_create: tile_config %d outside 0..%d", opt.tile_config, hb::N_LAUNCH_CONFIGS);
     }
-    h->tile_config = opt.tile_config == 0 ? hb::DEFAULT_TILE_CONFIG : opt.tile_config - 1;
+    h->launch_config = opt.tile_config == 0 ? hb::DEFAULT_LAUNCH_CONFIG : opt.tile_config - 1;
     const int C = h->C;
     // neighbour lists in input order, for the renumbering
     std::vector<int32_t> nbr_old(4 * (size_t)C, -1);
@@ -685,13 +876,17 @@ int set_state_t(hb_handle *h, hb::DevMesh<R> &m, const double *H, const double *
                 const double *W) {
     const int C = h->C;
     const int par = (int)(h->steps_done & 1);
-    std::vector<R> buf(C);
     const double *src[5] = {H, U, V, Z, W};
-    R *dst[5] = {m.H[par], m.U[par], m.V[par], m.Z[par], m.W};
-    for (int k = 0; k < 5; k++) {
-        if (!src[k]) { if (k < 4) return hb::set_error(HB_E_INVALID, "hb_set_state: missing array"); continue; }
-        for (int i = 0; i < C; i++) buf[i] = (R)src[k][h->perm[i]];
-        HB_CUDA_RET(cudaMemcpy(dst[k], buf.data(), C * sizeof(R), cudaMemcpyHostToDevice));
+    for (int k = 0; k < 4; k++)
+        if (!src[k]) return hb::set_error(HB_E_INVALID, "hb_set_state: missing array");
+    std::vector<R> buf(4 * (size_t)C);
+    for (int i = 0; i < C; i++)
+        for (int k = 0; k < 4; k++) buf[4 * (size_t)i + k] = (R)src[k][h->perm[i]];
+    HB_CUDA_RET(cudaMemcpy(m.S[par], buf.data(), buf.size() * sizeof(R), cudaMemcpyHostToDevice));
+    if (W) {
+        std::vector<R> w(C);
+        for (int i = 0; i < C; i++) w[i] = (R)W[h->perm[i]];
+        HB_CUDA_RET(cudaMemcpy(m.W, w.data(), C * sizeof(R), cudaMemcpyHostToDevice));
     }
     return HB_OK;
 }
@@ -699,14 +894,16 @@ template <class R>
 int get_state_t(hb_handle *h, hb::DevMesh<R> &m, double *H, double *U, double *V, double *Z, double *W) {
     const int C = h->C;
     const int par = (int)(h->steps_done & 1);
-    std::vector<R> buf(C);
     double *dst[5] = {H, U, V, Z, W};
-    R *src[5] = {m.H[par], m.U[par], m.V[par], m.Z[par], m.W};
     HB_CUDA_RET(cudaDeviceSynchronize());
-    for (int k = 0; k < 5; k++) {
-        if (!dst[k]) continue;
-        HB_CUDA_RET(cudaMemcpy(buf.data(), src[k], C * sizeof(R), cudaMemcpyDeviceToHost));
-        for (int i = 0; i < C; i++) dst[k][h->perm[i]] = (double)buf[i];
+    std::vector<R> buf(4 * (size_t)C);
+    HB_CUDA_RET(cudaMemcpy(buf.data(), m.S[par], buf.size() * sizeof(R), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 4; k++)
+        if (dst[k])
+            for (int i = 0; i < C; i++) dst[k][h->perm[i]] = (double)buf[4 * (size_t)i + k];
+    if (W) {
+        HB_CUDA_RET(cudaMemcpy(buf.data(), m.W, C * sizeof(R), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < C; i++) W[h->perm[i]] = (double)buf[i];
     }
     return HB_OK;
 }
@@ -732,7 +929,7 @@ int get_klas_t(hb_handle *h, hb::DevMesh<R> &m, double *klas) {
     const size_t S = 4 * (size_t)C;
     std::vector<uint8_t> meta(std::max(h->nslots, 1));
     HB_CUDA_RET(cudaDeviceSynchronize());
-    HB_CUDA_RET(cudaMemcpy(meta.data(), m.meta, h->nslots, cudaMemcpyDeviceToHost));
+    HB_CUDA_RET(cudaMemcpy(meta.data(), m.rmeta, h->nslots, cudaMemcpyDeviceToHost));
     for (int i = 0; i < C; i++)
         for (int j = 0; j < 4; j++) {
             const size_t so = 4 * (size_t)h->perm[i] + j;
@@ -780,12 +977,10 @@ int step_host_t(hb_handle *h, hb::DevMesh<R> &m, double *H, double *U, double *V
     double *io[5] = {H, U, V, Z, W};
     for (int k = 0; k < 4; k++) HB_CUDA_RET(cudaMemcpyAsync(h->d_stage + (size_t)k * C, io[k], b, cudaMemcpyHostToDevice, st));
     const int blocks = (C + 255) / 256;
-    hb::stage_in_kernel<R><<<blocks, 256, 0, st>>>(C, h->d_perm, h->d_stage, h->d_ctr, m.H[0], m.U[0], m.V[0], m.Z[0],
-                                                    m.H[1], m.U[1], m.V[1], m.Z[1]);
+    hb::stage_in_kernel<R><<<blocks, 256, 0, st>>>(C, h->d_perm, h->d_stage, h->d_ctr, m.S[0], m.S[1]);
     HB_CUDA_RET(cudaGetLastError());
     TRY(enqueue_steps(h, n, st));
-    hb::stage_out_kernel<R><<<blocks, 256, 0, st>>>(C, h->d_perm, h->d_stage, h->d_ctr, m.H[0], m.U[0], m.V[0], m.Z[0],
-                                                     m.H[1], m.U[1], m.V[1], m.Z[1], m.W);
+    hb::stage_out_kernel<R><<<blocks, 256, 0, st>>>(C, h->d_perm, h->d_stage, h->d_ctr, m.S[0], m.S[1], m.W);
     HB_CUDA_RET(cudaGetLastError());
     for (int k = 0; k < 5; k++)
         if (io[k]) HB_CUDA_RET(cudaMemcpyAsync(io[k], h->d_stage + (size_t)k * C, b, cudaMemcpyDeviceToHost, st));
@@ -835,13 +1030,8 @@ extern "C" int hb_set_position(hb_handle *h, int64_t steps_done) {
     if ((steps_done & 1) != (h->steps_done & 1)) {
         const size_t bytes = (size_t)h->C * (h->fp32() ? sizeof(float) : sizeof(double));
         const int from = (int)(h->steps_done & 1), to = from ^ 1;
-        if (h->fp32()) {
-            float **B[4] = {h->m32.H, h->m32.U, h->m32.V, h->m32.Z};
-            for (auto b : B) HB_CUDA_RET(cudaMemcpy(b[to], b[from], bytes, cudaMemcpyDeviceToDevice));
-        } else {
-            double **B[4] = {h->m64.H, h->m64.U, h->m64.V, h->m64.Z};
-            for (auto b : B) HB_CUDA_RET(cudaMemcpy(b[to], b[from], bytes, cudaMemcpyDeviceToDevice));
-        }
+        if (h->fp32()) HB_CUDA_RET(cudaMemcpy(h->m32.S[to], h->m32.S[from], 4 * bytes, cudaMemcpyDeviceToDevice));
+        else HB_CUDA_RET(cudaMemcpy(h->m64.S[to], h->m64.S[from], 4 * bytes, cudaMemcpyDeviceToDevice));
     }
     long long v = steps_done;
     HB_CUDA_RET(cudaMemcpy(h->d_ctr, &v, sizeof v, cudaMemcpyHostToDevice));
@@ -878,16 +1068,19 @@ extern "C" int hb_graph_launch(hb_handle *h, void *stream) {
     return HB_OK;
 }
 
-extern "C" int hb_device_state(hb_handle *h, void **H, void **U, void **V, void **Z, void **W) {
+extern "C" int hb_device_state(hb_handle *h, void **H, void **U, void **V, void **Z, void **W, int32_t *stride) {
     if (!h) return hb::set_error(HB_E_INVALID, "null handle");
     const int par = (int)(h->steps_done & 1);
     if (h->fp32()) {
-        if (H) *H = h->m32.H[par]; if (U) *U = h->m32.U[par]; if (V) *V = h->m32.V[par]; if (Z) *Z = h->m32.Z[par];
+        float *b = h->m32.S[par];
+        if (H) *H = b; if (U) *U = b + 1; if (V) *V = b + 2; if (Z) *Z = b + 3;
         if (W) *W = h->m32.W;
     } else {
-        if (H) *H = h->m64.H[par]; if (U) *U = h->m64.U[par]; if (V) *V = h->m64.V[par]; if (Z) *Z = h->m64.Z[par];
+        double *b = h->m64.S[par];
+        if (H) *H = b; if (U) *U = b + 1; if (V) *V = b + 2; if (Z) *Z = b + 3;
         if (W) *W = h->m64.W;
     }
+    if (stride) *stride = 4;
     return HB_OK;
 }
 

@@ -91,7 +91,7 @@ def lib():
         "hb_step_host": (C.c_int, [vp, _dp, _dp, _dp, _dp, _dp, C.c_int32, vp]),
         "hb_capture_graph": (C.c_int, [vp, C.c_int32, vp]),
         "hb_graph_launch": (C.c_int, [vp, vp]),
-        "hb_device_state": (C.c_int, [vp] + [C.POINTER(vp)] * 5),
+        "hb_device_state": (C.c_int, [vp] + [C.POINTER(vp)] * 5 + [C.POINTER(C.c_int32)]),
         "hb_get_permutation": (C.c_int, [vp, _ip]),
         "hb_device_errors": (C.c_int, [vp, C.POINTER(C.c_uint32)]),
         "hb_last_error": (C.c_int, []),

@@ -175,14 +175,18 @@ class Solver:
         """Zero-copy torch views of the device state (renumbered order): H, U, V, Z, W."""
         import torch
         ptrs = [C.c_void_p() for _ in range(5)]
-        check(lib().hb_device_state(self._h, *[C.byref(p) for p in ptrs]))
+        stride = C.c_int32()
+        check(lib().hb_device_state(self._h, *[C.byref(p) for p in ptrs], C.byref(stride)))
         dt = "<f8" if self.precision == FP64 else "<f4"
+        item = 8 if self.precision == FP64 else 4
 
         class _CAI:
-            def __init__(self, ptr, n):
-                self.__cuda_array_interface__ = {"shape": (n,), "typestr": dt, "data": (ptr, False), "version": 3}
+            def __init__(self, ptr, n, st):
+                self.__cuda_array_interface__ = {"shape": (n,), "typestr": dt, "data": (ptr, False), "version": 3,
+                                                 "strides": (st * item,)}
 
-        return {k: torch.as_tensor(_CAI(p.value, self.cells), device="cuda") for k, p in zip("HUVZW", ptrs)}
+        return {k: torch.as_tensor(_CAI(p.value, self.cells, stride.value if k != "W" else 1), device="cuda")
+                for k, p in zip("HUVZW", ptrs)}
 
 
 class RefLayoutMesh:

@@ -68,8 +68,9 @@ typedef struct hb_options {
     int32_t reserved[3];
 } hb_options;
 
-/* The step kernel's compiled tile shapes: threads (= real slots and cells
- * per tile) and CTAs per SM; returns how many there are. */
+/* The compiled launch shapes of the flux kernel: threads per CTA, and
+ * 100 * (flux CTAs per SM) + (cell-update CTAs per SM) asked of the compiler;
+ * returns how many there are (hb_options.tile_config = index + 1). */
 int hb_tile_configs(int32_t *threads, int32_t *min_blocks, int32_t capacity);
 
 /* Default options: variant H, fp64, device 0, renumbered. */
@@ -112,8 +113,10 @@ int hb_capture_graph(hb_handle *h, int32_t nsteps, void *stream);
 int hb_graph_launch(hb_handle *h, void *stream);
 
 /* Device-resident state pointers (renumbered order) for zero-copy use from
- * PyTorch: H, U, V, Z, W as fp64 [CELL] (fp32 for HB_FP32). */
-int hb_device_state(hb_handle *h, void **H, void **U, void **V, void **Z, void **W);
+ * PyTorch: H, U, V, Z, W, fp64 (fp32 for HB_FP32).  H, U, V and Z are
+ * interleaved per cell: element i of H is H[i * stride] (stride from *stride);
+ * W is contiguous. */
+int hb_device_state(hb_handle *h, void **H, void **U, void **V, void **Z, void **W, int32_t *stride);
 /* Renumbering: perm[new] = old (cell ids, 0-based). */
 int hb_get_permutation(hb_handle *h, int32_t *perm);
 /* Sticky device error word (bit set of hb_status codes seen by kernels). */
