@@ -163,3 +163,149 @@ void UpdateCell(const MeshView &mesh) {
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) fprintf(stderr, "hydrob200: UpdateCell: %s\n", cudaGetErrorString(e));
 }
+
+// ---------------------------------------------------------------------------
+// hb_ref_step_static: one step with a fixed, library-owned scratch array
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace hb {
+
+// [HB_REF_STEP_STATIC_MAX_CELLS * 4 slots][4] = {F0, dWU, dWV, SIDE} per slot.
+// Host code must not take this name as a device address: it is a host-side
+// stand-in; the device address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) double g_static_terms[(size_t)HB_REF_STEP_STATIC_MAX_CELLS * 16];
+
+constexpr int MAX_DEVICES = 64;
+static std::mutex g_static_mu;
+static double *g_static_ptr[MAX_DEVICES];
+
+// device address of g_static_terms on the current device (looked up once per device)
+static int static_terms_ptr(double **out) {
+    int dev = -1;
+    HB_CUDA_RET(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= MAX_DEVICES) return set_error(HB_E_INVALID, "hb_ref_step_static: device %d", dev);
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_terms);
+        if (e != cudaSuccess || !p)
+            return set_error(HB_E_CUDA, "hb_ref_step_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        g_static_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_static_ptr[dev];
+    return HB_OK;
+}
+
+// CalculateFluxKernel's writes (FLUX0..3 by the slot's mask, KLAS on breach)
+// plus the slot's terms of the cell sums (functors.cu:733-741) into `terms`.
+template <int VARIANT>
+__global__ void __launch_bounds__(256) static_flux_kernel(hb_ref_mesh_view m, int kt, int jt, double *terms) {
+    using A = F64Exact;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 4 * m.CELL) return;
+    const int pos = idx >> 2;
+    const auto &c = m.cells;
+    const auto &sd = m.sides;
+    SlotIn<double> in;
+    in.own = {c.H[pos], c.U[pos], c.V[pos], c.Z[pos], c.ZBC[pos]};
+    const int nc = (int)(sd.NAC[idx] - 1.0);
+    in.has_nb = nc != -1;
+    in.own_first = pos < nc;
+    if (in.has_nb) in.nb = {c.H[nc], c.U[nc], c.V[nc], c.Z[nc], c.ZBC[nc]};
+    else in.nb = {0.0, 0.0, 0.0, 0.0, 0.0};
+    in.code = klas_code(sd.KLAS[idx]);
+    in.cosj = sd.COSF[idx];
+    in.sinj = sd.SINF[idx];
+    in.side = sd.SIDE[idx];
+    StepParams p{m.HM1, m.HM2, m.JL, m.DT, kt, jt};
+    auto fetch = [&]() {
+        BoundaryIn<double> b;
+        const size_t t = (size_t)jt * (size_t)m.CELL + (size_t)pos;
+        b.qt = c.QT[t]; b.dqt = c.DQT[t]; b.zt = c.ZT[t]; b.dzt = c.DZT[t];
+        b.top = c.BoundaryFeature[pos];
+        b.zw = c.ZW + (size_t)pos * (size_t)m.NHQ;
+        b.qw = c.QW + (size_t)pos * (size_t)m.NHQ;
+        b.nhq1 = c.NHQ1[pos];
+        b.nhq = m.NHQ;
+        return b;
+    };
+    SlotOut<double> o;
+    flux_slot<A, VARIANT>(in, A::sqrt(A::mul(9.81, in.own.h)), p, fetch, o);
+    if (o.undefined) atomicOr(&g_ref_errors, ERRBIT_UNDEFINED);
+    if (o.klas_to_zero) sd.KLAS[idx] = 0.0;
+    // fluxes this slot does not write keep their values (functors.cu:525-565)
+    if (o.mask & 1) sd.FLUX0[idx] = o.f[0]; else o.f[0] = sd.FLUX0[idx];
+    if (o.mask & 2) sd.FLUX1[idx] = o.f[1]; else o.f[1] = sd.FLUX1[idx];
+    if (o.mask & 4) sd.FLUX2[idx] = o.f[2]; else o.f[2] = sd.FLUX2[idx];
+    if (o.mask & 8) sd.FLUX3[idx] = o.f[3]; else o.f[3] = sd.FLUX3[idx];
+    const double fr1 = A::add(o.f[1], o.f[3]);
+    const double slcos = sd.SLCOS[idx], slsin = sd.SLSIN[idx];
+    double *t = terms + 4 * (size_t)idx;
+    t[0] = o.f[0];
+    t[1] = A::dot(slcos, fr1, -slsin, o.f[2], M_WU);
+    t[2] = A::dot(slsin, fr1, slcos, o.f[2], M_WV);
+    t[3] = in.side;
+}
+
+// UpdateCellKernel (functors.cu:717-784) with the sums taken from `terms`.
+template <int VARIANT>
+__global__ void __launch_bounds__(256) static_update_kernel(hb_ref_mesh_view m, const double *terms) {
+    using A = F64Exact;
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= m.CELL) return;
+    const auto &c = m.cells;
+    const auto &sd = m.sides;
+    double wh = 0.0, wu = 0.0, wv = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const double *t = terms + 16 * (size_t)pos + 4 * j;
+        wh = A::madd(t[3], t[0], wh, M_WH);
+        wu = A::add(wu, t[1]);
+        wv = A::add(wv, t[2]);
+    }
+    CellUpdateIn<double> ci;
+    ci.h = c.H[pos]; ci.u = c.U[pos]; ci.v = c.V[pos]; ci.zbc = c.ZBC[pos]; ci.fnc = c.FNC[pos];
+    if (VARIANT == 1) {
+        const double s0 = sd.SIDE[4 * pos], s1 = sd.SIDE[4 * pos + 1], s2 = sd.SIDE[4 * pos + 2], s3 = sd.SIDE[4 * pos + 3];
+        if (s3 > 0.0) {
+            ci.sidex = A::fmin(A::mul(0.5, A::add(s0, s2)), A::mul(0.5, A::add(s1, s3)));
+        } else {
+            double ss = A::mul(0.5, A::add(A::add(s0, s1), s2));
+            ci.sidex = A::sqrt(A::div(A::mul(A::mul(A::sub(ss, s0), A::sub(ss, s1)), A::sub(ss, s2)), ss));
+        }
+        ci.dta_or_area = c.AREA[pos];
+    } else {
+        ci.sidex = 0.0;
+        ci.dta_or_area = A::div(m.DT, c.AREA[pos]);
+    }
+    StepParams p{m.HM1, m.HM2, m.JL, m.DT, 0, 0};
+    CellUpdateOut<double> o = update_cell<A, VARIANT>(ci, wh, wu, wv, p);
+    c.H[pos] = o.h; c.U[pos] = o.u; c.V[pos] = o.v; c.Z[pos] = o.z; c.W[pos] = o.w;
+}
+
+}  // namespace hb
+
+extern "C" int hb_ref_step_static(const hb_ref_mesh_view *m, int32_t kt, int32_t jt, int32_t variant, void *stream) {
+    if (!m || m->CELL < 0) return hb::set_error(HB_E_INVALID, "hb_ref_step_static: bad mesh view");
+    if (m->CELL > HB_REF_STEP_STATIC_MAX_CELLS)
+        return hb::set_error(HB_E_TOO_LARGE, "hb_ref_step_static: %d cells, the fixed scratch holds %d", m->CELL,
+                             HB_REF_STEP_STATIC_MAX_CELLS);
+    if (m->CELL == 0) return HB_OK;
+    if (jt < 0 || jt >= m->NDAYS)
+        return hb::set_error(HB_E_INVALID, "hb_ref_step_static: jt=%d outside [0,%d)", jt, m->NDAYS);
+    double *terms = nullptr;
+    int st = hb::static_terms_ptr(&terms);
+    if (st != HB_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int fb = (4 * m->CELL + 255) / 256, ub = (m->CELL + 255) / 256;
+    if (variant == HB_VARIANT_F) {
+        hb::static_flux_kernel<1><<<fb, 256, 0, s>>>(*m, kt, jt, terms);
+        hb::static_update_kernel<1><<<ub, 256, 0, s>>>(*m, terms);
+    } else {
+        hb::static_flux_kernel<0><<<fb, 256, 0, s>>>(*m, kt, jt, terms);
+        hb::static_update_kernel<0><<<ub, 256, 0, s>>>(*m, terms);
+    }
+    HB_CUDA_RET(cudaGetLastError());
+    return HB_OK;
+}

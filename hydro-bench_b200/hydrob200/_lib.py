@@ -12,6 +12,7 @@ HB_OK = 0
 STATUS = {0: "HB_OK", 1: "HB_E_INVALID", 2: "HB_E_BADMESH", 3: "HB_E_CUDA", 4: "HB_E_NONFINITE",
           5: "HB_E_BARRIER_TIMEOUT", 6: "HB_E_IO", 7: "HB_E_UNDEFINED_REF", 8: "HB_E_NOMEM", 9: "HB_E_TOO_LARGE"}
 VARIANT_H, VARIANT_F = 0, 1
+REF_STEP_STATIC_MAX_CELLS = 65536   # HB_REF_STEP_STATIC_MAX_CELLS
 FP64, FP32, SPLIT = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)
@@ -106,6 +107,7 @@ def lib():
         "hb_ref_calculate_flux_f32": (C.c_int, [C.POINTER(RefMeshViewF32), C.c_int32, C.c_int32, C.c_int32, vp]),
         "hb_ref_update_cell_f32": (C.c_int, [C.POINTER(RefMeshViewF32), C.c_int32, vp]),
         "hb_ref_take_device_errors": (C.c_int, [C.POINTER(C.c_uint32)]),
+        "hb_ref_step_static": (C.c_int, [C.POINTER(RefMeshView), C.c_int32, C.c_int32, C.c_int32, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(l, name)
@@ -127,4 +129,4 @@ EXPORTED = ["hb_options_default", "hb_tile_configs", "hb_create", "hb_destroy", 
             "hb_graph_launch", "hb_device_state", "hb_get_permutation", "hb_device_errors", "hb_last_error",
             "hb_last_error_string", "hb_status_string", "hb_deck_load", "hb_deck_mesh", "hb_deck_state",
             "hb_deck_free", "hb_ref_calculate_flux", "hb_ref_update_cell", "hb_ref_calculate_flux_f32",
-            "hb_ref_update_cell_f32", "hb_ref_take_device_errors"]
+            "hb_ref_update_cell_f32", "hb_ref_take_device_errors", "hb_ref_step_static"]

@@ -72,6 +72,33 @@ int hb_ref_update_cell_f32(const hb_ref_mesh_view_f32 *mesh, int32_t variant, vo
 /* Bits of hb_status codes raised by these kernels since the last call (then cleared). */
 int hb_ref_take_device_errors(uint32_t *bits);
 
+/* One whole timestep (CalculateFlux then UpdateCell, fp64) over the caller's
+ * reference-layout arrays that allocates no device memory at all.  This entry
+ * point has no counterpart in the reference.
+ *
+ * It is meant for callers that cannot call cudaMalloc: a host framework that
+ * owns the device allocator (a caching allocator that must see every byte), a
+ * program whose memory budget is fixed when it starts, or code running where
+ * an allocation would synchronise or fail.  The scratch that carries each
+ * slot's terms of the cell sums from the flux pass to the update pass lives in
+ * a fixed array inside the library instead, HB_REF_STEP_STATIC_MAX_CELLS cells
+ * (8 MiB), which every GPU that loads the library holds until the process
+ * exits.
+ *
+ * - Meshes with more cells are rejected with HB_E_TOO_LARGE before anything is
+ *   launched.
+ * - The first call on a device looks up the array's device address
+ *   (cudaGetSymbolAddress) with that device current; make that first call
+ *   before any stream capture.
+ * - Every call shares the one array: calls whose work overlaps on the GPU
+ *   (other streams, other threads) race on it.  Each call writes every term it
+ *   later reads, so nothing needs clearing between calls.
+ * - Results are bit-identical to hb_ref_calculate_flux followed by
+ *   hb_ref_update_cell: state updated in place, FLUX0..3 and KLAS written as
+ *   CalculateFlux writes them. */
+#define HB_REF_STEP_STATIC_MAX_CELLS 65536
+int hb_ref_step_static(const hb_ref_mesh_view *mesh, int32_t kt, int32_t jt, int32_t variant, void *stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 
