@@ -56,8 +56,13 @@ __host__ __device__ inline bool code_is_bounda(int8_t c) { return c != CODE_ZERO
 // ---------------------------------------------------------------------------
 // arithmetic policies
 // ---------------------------------------------------------------------------
+// Every policy has a `real` type for the flux/state arithmetic and a `level`
+// type for water levels and bed elevations (Z, ZBC, ZT, ZW, crest heights).
+// A depth rebuilt from levels (level minus bed) is formed in `level`
+// precision and then rounded to `real` (depth()).
 struct F64Exact {
     using real = double;
+    using level = double;
     static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
     static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
     static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
@@ -92,6 +97,17 @@ struct F64Exact {
     static __device__ __forceinline__ double fabs(double a) { return ::fabs(a); }
     static __device__ __forceinline__ double copysign(double a, double b) { return ::copysign(a, b); }
     static __device__ __forceinline__ double c(double v) { return v; }
+    static __device__ __forceinline__ double lc(double v) { return v; }
+    static __device__ __forceinline__ double depth(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double lvl(double h) { return h; }
+    static __device__ __forceinline__ double ladd(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double lsub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double ldiv(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double lmax(double a, double b) { return ::fmax(a, b); }
+    static __device__ __forceinline__ double lmin(double a, double b) { return ::fmin(a, b); }
+    static __device__ __forceinline__ double lmadd(double a, double b, double c, int mode) {
+        return mode ? __fma_rn(a, b, c) : __dadd_rn(c, __dmul_rn(a, b));
+    }
     // a*b + c*d; mode 0 rounds both products, 1 fuses a*b, 2 fuses c*d
     static __device__ __forceinline__ double dot(double a, double b, double c, double d, int mode) {
         return mode == 1 ? __fma_rn(a, b, __dmul_rn(c, d))
@@ -106,6 +122,7 @@ struct F64Exact {
 
 struct F32Fast {
     using real = float;
+    using level = float;
     static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
     static __device__ __forceinline__ float add(float a, float b) { return a + b; }
     static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
@@ -119,9 +136,48 @@ struct F32Fast {
     static __device__ __forceinline__ float fabs(float a) { return fabsf(a); }
     static __device__ __forceinline__ float copysign(float a, float b) { return copysignf(a, b); }
     static __device__ __forceinline__ float c(double v) { return (float)v; }
+    static __device__ __forceinline__ float lc(double v) { return (float)v; }
+    static __device__ __forceinline__ float depth(float a, float b) { return a - b; }
+    static __device__ __forceinline__ float lvl(float h) { return h; }
+    static __device__ __forceinline__ float ladd(float a, float b) { return a + b; }
+    static __device__ __forceinline__ float lsub(float a, float b) { return a - b; }
+    static __device__ __forceinline__ float ldiv(float a, float b) { return a / b; }
+    static __device__ __forceinline__ float lmax(float a, float b) { return fmaxf(a, b); }
+    static __device__ __forceinline__ float lmin(float a, float b) { return fminf(a, b); }
+    static __device__ __forceinline__ float lmadd(float a, float b, float c, int) { return fmaf(a, b, c); }
     static __device__ __forceinline__ float dot(float a, float b, float c, float d, int) { return fmaf(a, b, c * d); }
     static __device__ __forceinline__ float madd(float a, float b, float c, int) { return fmaf(a, b, c); }
 };
+
+// Split precision: fluxes, velocities and the depth itself in fp32; water
+// levels and bed elevations in fp64, so that a depth rebuilt as level minus
+// bed (shallow water over a high bed) keeps its digits.  The depth update is
+// Kahan-compensated (update_cell): the state carries the fp32 depth and its
+// fp32 compensation term, and the level of a cell is rebuilt in fp64 from both.
+struct F32Split : F32Fast {
+    using level = double;
+    static __device__ __forceinline__ double lc(double v) { return v; }
+    static __device__ __forceinline__ float depth(double a, double b) { return __double2float_rn(a - b); }
+    static __device__ __forceinline__ double lvl(float h) { return (double)h; }
+    static __device__ __forceinline__ double ladd(double a, double b) { return a + b; }
+    static __device__ __forceinline__ double lsub(double a, double b) { return a - b; }
+    static __device__ __forceinline__ double ldiv(double a, double b) { return a / b; }
+    static __device__ __forceinline__ double lmax(double a, double b) { return ::fmax(a, b); }
+    static __device__ __forceinline__ double lmin(double a, double b) { return ::fmin(a, b); }
+    static __device__ __forceinline__ double lmadd(double a, double b, double c, int) { return ::fma(a, b, c); }
+};
+template <class A> struct is_split : std::false_type {};
+template <> struct is_split<F32Split> : std::true_type {};
+
+// Water level of a split-precision cell, in fp64: bed + depth + compensation.
+// The state keeps no level of its own.  At the dry threshold (h == HM1) the
+// update always leaves hlo = 0, so there hlo is free to carry the offset of
+// an initial level below bed + HM1 (the reference's dry cells keep Z < ZBC
+// while H = HM1, mesh.cpp:350-361); the depth update ignores it.
+template <class A>
+__device__ __forceinline__ double split_level(float h, float hlo, double zbc) {
+    return (double)h + ((double)hlo + zbc);
+}
 
 // Fusion modes of the reference sm_100a build (see file comment).
 enum : int {
@@ -141,13 +197,13 @@ static_assert(M_QL1 == M_QL1M && M_QR2 == M_QR2M, "flux_slot shares these modes 
 // ---------------------------------------------------------------------------
 // inputs / outputs of one slot
 // ---------------------------------------------------------------------------
-template <class R>
-struct CellState { R h, u, v, z, zbc; };
+template <class R, class L = R>
+struct CellState { R h, u, v; L z, zbc; };
 
-template <class R>
+template <class R, class L = R>
 struct SlotIn {
-    CellState<R> own;       // H1, U1, V1, Z1 and ZBC of the slot's cell
-    CellState<R> nb;        // raw H, U, V, Z, ZBC of the neighbour (unused when has_nb == false)
+    CellState<R, L> own;    // H1, U1, V1, Z1 and ZBC of the slot's cell
+    CellState<R, L> nb;     // raw H, U, V, Z, ZBC of the neighbour (unused when has_nb == false)
     bool has_nb;            // NAC != 0
     bool own_first;         // pos < NC in the reference numbering
     int8_t code;            // klas_code(KLAS)
@@ -155,13 +211,18 @@ struct SlotIn {
 };
 
 // boundary tables at (jt, pos), fetched only for boundary slots
-template <class R>
+template <class R, class L = R>
 struct BoundaryIn {
-    R qt, dqt, zt, dzt, top;        // QT, DQT, ZT, DZT at [jt][pos]; BoundaryFeature[pos]
-    const R *zw, *qw;               // rating-curve row of the cell
+    R qt, dqt;                      // QT, DQT at [jt][pos]
+    L zt, dzt, top;                 // ZT, DZT at [jt][pos]; BoundaryFeature[pos]
+    const L *zw;                    // rating-curve levels of the cell
+    const R *qw;                    // rating-curve discharges of the cell
     int nhq1;                       // points used (NHQ1[pos])
     int nhq;                        // row width (NHQ)
 };
+template <class A> using CellStateA = CellState<typename A::real, typename A::level>;
+template <class A> using SlotInA = SlotIn<typename A::real, typename A::level>;
+template <class A> using BoundaryInA = BoundaryIn<typename A::real, typename A::level>;
 
 template <class R>
 struct SlotOut {
@@ -318,27 +379,30 @@ __device__ __forceinline__ void osher(typename A::real cl, const typename A::rea
 // ---------------------------------------------------------------------------
 // QD, functors.cu:394-421
 template <class A>
-__device__ __forceinline__ typename A::real weir_discharge(typename A::real zl, typename A::real zr, typename A::real zb) {
+__device__ __forceinline__ typename A::real weir_discharge(typename A::level zl, typename A::level zr,
+                                                           typename A::level zb) {
     using R = typename A::real;
-    R zu = A::fmax(zl, zr), zd = A::fmin(zl, zr);
-    R h0 = A::sub(zu, zb), hs = A::sub(zd, zb);
+    using L = typename A::level;
+    L zu = A::lmax(zl, zr), zd = A::lmin(zl, zr);
+    R h0 = A::depth(zu, zb), hs = A::depth(zd, zb);
     R delta = A::div(hs, h0);
-    if (delta <= A::c(0.667)) return A::copysign(A::mul(A::c(0.384), A::pow(h0, A::c(1.5))), A::sub(zl, zr));
-    R dh = A::sub(zu, zd);
-    if (dh > A::c(0.09)) return A::copysign(A::mul(A::mul(A::c(4.43), hs), A::sqrt(dh)), A::sub(zl, zr));
-    return A::copysign(A::divk(A::mul(A::mul(A::mul(A::c(4.43), hs), A::c(0.3)), dh), 0.1), A::sub(zl, zr));
+    if (delta <= A::c(0.667)) return A::copysign(A::mul(A::c(0.384), A::pow(h0, A::c(1.5))), A::depth(zl, zr));
+    R dh = A::depth(zu, zd);
+    if (dh > A::c(0.09)) return A::copysign(A::mul(A::mul(A::c(4.43), hs), A::sqrt(dh)), A::depth(zl, zr));
+    return A::copysign(A::divk(A::mul(A::mul(A::mul(A::c(4.43), hs), A::c(0.3)), dh), 0.1), A::depth(zl, zr));
 }
 
 // LAQP, functors.cu:423-443: y(x) by linear interpolation in the table (a -> b)
 template <class A>
-__device__ __forceinline__ void table_lookup(typename A::real x, typename A::real &y, const typename A::real *a,
-                                             const typename A::real *b, int ms) {
+__device__ __forceinline__ void table_lookup(typename A::real x, typename A::level &y, const typename A::real *a,
+                                             const typename A::level *b, int ms) {
     if (ms <= 0) return;
     if (x < a[0]) { y = b[0]; return; }
     if (x > a[ms - 1]) { y = b[ms - 1]; return; }
     for (int i = 0; i < ms - 1; i++) {
         if (x >= a[i] && x <= a[i + 1]) {
-            y = A::madd(A::div(A::sub(b[i + 1], b[i]), A::sub(a[i + 1], a[i])), A::sub(x, a[i]), b[i], M_LAQP);
+            y = A::lmadd(A::ldiv(A::lsub(b[i + 1], b[i]), A::lvl(A::sub(a[i + 1], a[i]))), A::lvl(A::sub(x, a[i])),
+                         b[i], M_LAQP);
             return;
         }
     }
@@ -363,10 +427,11 @@ __device__ __forceinline__ typename A::real invariant_iter(typename A::real ql1,
 }
 
 template <class A, int VARIANT, class TableFetch>
-__device__ __forceinline__ void bounda(const SlotIn<typename A::real> &in, const StepParams &p, typename A::real fil,
-                                       typename A::real ql[3], typename A::real zc, typename A::real uc,
+__device__ __forceinline__ void bounda(const SlotInA<A> &in, const StepParams &p, typename A::real fil,
+                                       typename A::real ql[3], typename A::level zc, typename A::real uc,
                                        typename A::real vc, const TableFetch &fetch, SlotOut<typename A::real> &o) {
     using R = typename A::real;
+    using L = typename A::level;
     const R h = in.own.h;
     const R hm2 = A::c(p.hm2);
     R cl = A::sqrt(A::mul(A::c(9.81), h));
@@ -384,7 +449,7 @@ __device__ __forceinline__ void bounda(const SlotIn<typename A::real> &in, const
     o.mask = 0x4;
     switch (in.code) {
     case CODE_K10: {
-        BoundaryIn<R> b = fetch();
+        BoundaryInA<A> b = fetch();
         R f0 = -A::madd(b.dqt, A::c((double)p.kt), b.qt, M_K10);
         f0 = A::div(f0, in.side);
         R qb2 = A::mul(f0, f0);
@@ -403,13 +468,13 @@ __device__ __forceinline__ void bounda(const SlotIn<typename A::real> &in, const
         break;
     }
     case CODE_K3: {
-        BoundaryIn<R> b = fetch();
+        BoundaryInA<A> b = fetch();
         R q3 = A::mul(A::mul(A::dot(in.own.u, in.cosj, in.own.v, in.sinj, M_K3Q), h), in.side);
         q3 = A::fmax(q3, R(0));
-        R zq = R(0);   // the reference leaves ZQH1 unset when the cell has no table (NHQ1 = 0)
+        L zq = L(0);   // the reference leaves ZQH1 unset when the cell has no table (NHQ1 = 0)
         table_lookup<A>(q3, zq, b.qw, b.zw, b.nhq1);
-        R dzq = A::sub(zq, in.own.z);
-        R hb1 = A::fmax(A::sub(zq, in.own.zbc), hm2);
+        R dzq = A::depth(zq, in.own.z);
+        R hb1 = A::fmax(A::depth(zq, in.own.zbc), hm2);
         R qw1 = b.nhq > 1 ? b.qw[1] : R(0);   // QW_row[1] (functors.cu:347)
         ql[1] = A::fmax(ql[1], R(0));
         if (q3 <= qw1 || hb1 <= hm2 || dzq >= A::c(0.1)) {
@@ -426,9 +491,9 @@ __device__ __forceinline__ void bounda(const SlotIn<typename A::real> &in, const
         break;
     }
     case CODE_K1: {
-        BoundaryIn<R> b = fetch();
+        BoundaryInA<A> b = fetch();
         int mult = VARIANT == 1 ? p.kt : p.jt;
-        R hb1 = A::sub(A::madd(b.dzt, A::c((double)mult), b.zt, M_K1), in.own.zbc);
+        R hb1 = A::depth(A::lmadd(b.dzt, A::lc((double)mult), b.zt, M_K1), in.own.zbc);
         hb1 = A::fmax(hb1, hm2);
         R urb = invariant_iter<A>(ql[1], h, hb1, 0.0001, M_FIAL1, M_FIAR1);
         o.f[0] = A::mul(hb1, urb);
@@ -452,54 +517,54 @@ __device__ __forceinline__ void bounda(const SlotIn<typename A::real> &in, const
         break;
     }
     case CODE_K6: {   // CalculataKlas6, functors.cu:258-318
-        BoundaryIn<R> b = fetch();
-        const R top = b.top, zb = in.own.zbc, zp = in.own.z;
+        BoundaryInA<A> b = fetch();
+        const L top = b.top, zb = in.own.zbc, zp = in.own.z;
         const R cs = in.cosj, sn = in.sinj;
         if (zp <= top && zc <= top) {
             o.f[0] = R(0); o.f[1] = R(0); o.f[2] = R(0);
             o.f[3] = A::mul(A::mul(A::c(4.905), h), h);
         } else if (zp > top && zc <= top) {
-            o.f[0] = A::mul(A::c(K::C0), A::pow(A::sub(zp, top), A::c(1.5)));
+            o.f[0] = A::mul(A::c(K::C0), A::pow(A::depth(zp, top), A::c(1.5)));
             o.f[1] = A::mul(o.f[0], ql[1]);
             o.f[2] = A::mul(o.f[0], ql[2]);
-            o.f[3] = A::mul(A::c(4.905), A::pow(A::sub(top, zb), A::c(2.0)));
+            o.f[3] = A::mul(A::c(4.905), A::pow(A::depth(top, zb), A::c(2.0)));
         } else if (zp <= top && zc > top) {
-            o.f[0] = A::mul(A::c(-K::C0), A::pow(A::sub(zc, top), A::c(1.5)));
+            o.f[0] = A::mul(A::c(-K::C0), A::pow(A::depth(zc, top), A::c(1.5)));
             o.f[1] = A::mul(o.f[0], A::fmin(A::dot(uc, cs, vc, sn, M_K6UN), R(0)));
             o.f[2] = A::mul(o.f[0], A::dot(vc, cs, -uc, sn, M_K6VT));
-            o.f[3] = A::mul(A::c(4.905), A::pow(A::sub(zp, zb), A::c(2.0)));
+            o.f[3] = A::mul(A::c(4.905), A::pow(A::depth(zp, zb), A::c(2.0)));
         } else if (zp > top && zc > top) {
-            R dz = A::fabs(A::sub(zp, zc));
+            R dz = A::fabs(A::depth(zp, zc));
             if (zp <= zc) {
-                R hd = A::sub(zp, top);
+                R hd = A::depth(zp, top);
                 R un = A::fmin(A::dot(uc, cs, vc, sn, M_K6UN), R(0));
                 R vt = A::dot(vc, cs, -uc, sn, M_K6VT);
                 R sh = A::add(hd, dz);
                 R ce = A::fmin(A::c(1.0), A::mul(A::c(1.05), A::pow(A::div(dz, sh), A::c(0.33333))));
                 if (zp < zc && un > R(0)) un = R(0);
-                o.f[0] = A::copysign(A::mul(A::mul(ce, A::c(K::C1)), A::pow(sh, A::c(1.5))), A::sub(zp, zc));
+                o.f[0] = A::copysign(A::mul(A::mul(ce, A::c(K::C1)), A::pow(sh, A::c(1.5))), A::depth(zp, zc));
                 o.f[1] = A::mul(o.f[0], A::fabs(un));
                 o.f[2] = A::mul(o.f[0], vt);
-                o.f[3] = A::mul(A::c(4.905), A::pow(A::sub(top, zb), A::c(2.0)));
+                o.f[3] = A::mul(A::c(4.905), A::pow(A::depth(top, zb), A::c(2.0)));
             } else {
-                R hd = A::sub(zc, top);
+                R hd = A::depth(zc, top);
                 R un = A::fmax(ql[1], R(0));
                 R vt = ql[2];
                 R sh = A::add(hd, dz);
                 R ce = A::fmin(A::c(1.0), A::mul(A::c(1.05), A::pow(A::div(dz, sh), A::c(0.33333))));
-                o.f[0] = A::copysign(A::mul(A::mul(ce, A::c(K::C1)), A::pow(sh, A::c(1.5))), A::sub(zp, zc));
-                R dzs = A::sub(zp, zc);
+                o.f[0] = A::copysign(A::mul(A::mul(ce, A::c(K::C1)), A::pow(sh, A::c(1.5))), A::depth(zp, zc));
+                R dzs = A::depth(zp, zc);
                 o.f[1] = A::mul(A::mul(dzs, A::fabs(un)), un);
                 o.f[2] = A::mul(A::mul(dzs, A::fabs(un)), vt);
-                o.f[3] = A::mul(A::c(4.905), A::pow(A::sub(top, zb), A::c(2.0)));
+                o.f[3] = A::mul(A::c(4.905), A::pow(A::depth(top, zb), A::c(2.0)));
             }
         }
         o.mask = 0xF;
         break;
     }
     case CODE_K7: {   // CalculateKlas7, functors.cu:234-256
-        BoundaryIn<R> b = fetch();
-        const R top = b.top, zp = in.own.z;
+        BoundaryInA<A> b = fetch();
+        const L top = b.top, zp = in.own.z;
         if (zp > top || zc > top) {
             o.klas_to_zero = true;
             // The reference reads an uninitialised HB here (functors.cu:246-247); the
@@ -544,25 +609,28 @@ __device__ __forceinline__ typename A::real pow15(typename A::real x) {
 // slot's fluxes are final (returns 0, `o` filled) or it needs Osher across the
 // edge: 1 = direct (functors.cu:151-164), 2 = mirrored (:165-200).
 template <class A, int VARIANT, class TableFetch, bool ZERO_LEN = false>
-__device__ __forceinline__ int flux_chain(const SlotIn<typename A::real> &in, typename A::real cl_own,
+__device__ __forceinline__ int flux_chain(const SlotInA<A> &in, typename A::real cl_own,
                                           const StepParams &p, const TableFetch &fetch,
                                           SlotOut<typename A::real> &o) {
     using R = typename A::real;
+    using L = typename A::level;
     o.mask = 0xF; o.klas_to_zero = false; o.undefined = false;
     const R HM1 = A::c(p.hm1), HM2 = A::c(p.hm2);
-    const R h1 = in.own.h, u1 = in.own.u, v1 = in.own.v, z1 = in.own.z, zbc1 = in.own.zbc;
+    const R h1 = in.own.h, u1 = in.own.u, v1 = in.own.v;
+    const L z1 = in.own.z, zbc1 = in.own.zbc;
     const R cs = in.cosj, sn = in.sinj;
     R ql[3];
     ql[0] = h1;
     ql[1] = A::dot(u1, cs, v1, sn, M_QL1);
     ql[2] = A::dot(v1, cs, -u1, sn, M_QL2);
-    R zi = A::fmax(z1, A::add(zbc1, HM1));
-    R hc, bc, zc, uc, vc;
-    if (!in.has_nb) { hc = R(0); bc = R(0); zc = R(0); uc = R(0); vc = R(0); }
+    L zi = A::lmax(z1, A::ladd(zbc1, A::lc(p.hm1)));
+    R hc, uc, vc;
+    L bc, zc;
+    if (!in.has_nb) { hc = R(0); bc = L(0); zc = L(0); uc = R(0); vc = R(0); }
     else {
         hc = A::fmax(in.nb.h, HM1);
         bc = in.nb.zbc;
-        zc = A::fmax(bc, in.nb.z);
+        zc = A::lmax(bc, in.nb.z);
         uc = in.nb.u;
         vc = in.nb.v;
     }
@@ -584,7 +652,7 @@ __device__ __forceinline__ int flux_chain(const SlotIn<typename A::real> &in, ty
         o.f[3] = R(0);
     } else if (h1 <= HM2) {
         if (zc > zi) {
-            R dh = A::fmax(A::sub(zc, zbc1), HM1);
+            R dh = A::fmax(A::depth(zc, zbc1), HM1);
             R un = A::mul(A::c(-K::C1), A::sqrt(dh));
             o.f[0] = A::mul(dh, un);
             o.f[1] = A::mul(o.f[0], un);
@@ -597,9 +665,9 @@ __device__ __forceinline__ int flux_chain(const SlotIn<typename A::real> &in, ty
         }
     } else if (hc <= HM2) {
         if (zi > zc) {
-            R dh = A::fmax(A::sub(zi, bc), HM1);
+            R dh = A::fmax(A::depth(zi, bc), HM1);
             R un = A::mul(A::c(K::C1), A::sqrt(dh));
-            R hc1 = A::sub(zc, zbc1);
+            R hc1 = A::depth(zc, zbc1);
             o.f[0] = A::mul(dh, un);
             o.f[1] = A::mul(o.f[0], un);
             o.f[2] = A::mul(o.f[0], ql[2]);
@@ -631,8 +699,8 @@ template <class R>
 struct OsherIn { R cl, fil, hcR, ratio, ur; R ql[3], qr[3]; };
 
 template <class A>
-__device__ __forceinline__ OsherIn<typename A::real> osher_inputs(const CellState<typename A::real> &L,
-                                                                 const CellState<typename A::real> &Rc,
+__device__ __forceinline__ OsherIn<typename A::real> osher_inputs(const CellStateA<A> &L,
+                                                                 const CellStateA<A> &Rc,
                                                                  typename A::real cs, typename A::real sn,
                                                                  typename A::real clL, bool mir, const StepParams &p) {
     using R = typename A::real;
@@ -644,8 +712,8 @@ __device__ __forceinline__ OsherIn<typename A::real> osher_inputs(const CellStat
     o.ql[2] = mir ? A::dot(L.v, cs, -L.u, sn, M_QL2M) : A::dot(L.v, cs, -L.u, sn, M_QL2);
     o.fil = A::add(o.ql[1], A::mul(A::c(2.0), clL));
     o.hcR = A::fmax(Rc.h, HM1);
-    const R zR = A::fmax(Rc.zbc, Rc.z);
-    o.qr[0] = A::fmax(A::sub(zR, L.zbc), HM1);
+    const typename A::level zR = A::lmax(Rc.zbc, Rc.z);
+    o.qr[0] = A::fmax(A::depth(zR, L.zbc), HM1);
     o.ur = mir ? A::dot(Rc.u, cs, Rc.v, sn, M_UR1) : A::dot(Rc.u, cs, Rc.v, sn, M_UR);
     o.ratio = A::fmin(A::div(o.hcR, o.qr[0]), A::c(1.5));
     o.qr[1] = A::mul(o.ur, o.ratio);
@@ -661,12 +729,12 @@ __device__ __forceinline__ typename A::real osher_f1(typename A::real fo1, typen
     return A::add(fo1, A::mul(A::mul(A::mul(A::mul(A::sub(A::c(1.0), ratio), hcR), ur), ur), A::c(0.5)));
 }
 template <class A>
-__device__ __forceinline__ typename A::real mirror_f3(typename A::real fo3, typename A::real zbcL,
-                                                      typename A::real zbc_own) {
+__device__ __forceinline__ typename A::real mirror_f3(typename A::real fo3, typename A::level zbcL,
+                                                      typename A::level zbc_own) {
     using R = typename A::real;
-    R za = A::add(A::sqrt(A::divk(fo3, 4.905)), zbcL);
+    typename A::level za = A::ladd(A::lvl(A::sqrt(A::divk(fo3, 4.905))), zbcL);
     R hc3 = R(0);
-    if (za > zbc_own) hc3 = A::sub(za, zbc_own);
+    if (za > zbc_own) hc3 = A::depth(za, zbc_own);
     return A::mul(A::mul(A::c(4.905), hc3), hc3);
 }
 
@@ -674,15 +742,15 @@ __device__ __forceinline__ typename A::real mirror_f3(typename A::real fo3, type
 // `cl_own` is sqrt(9.81*H) of the slot's cell (the caller may compute it once
 // per cell; it is bit-identical to the reference's per-slot value).
 template <class A, int VARIANT, class TableFetch, bool ZERO_LEN = false>
-__device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, typename A::real cl_own,
+__device__ __forceinline__ void flux_slot(const SlotInA<A> &in, typename A::real cl_own,
                                           const StepParams &p, const TableFetch &fetch,
                                           SlotOut<typename A::real> &o) {
     using R = typename A::real;
     const int route = flux_chain<A, VARIANT, TableFetch, ZERO_LEN>(in, cl_own, p, fetch, o);
     if (route == 0) return;
     const bool mir = route == 2;
-    const CellState<R> &L = mir ? in.nb : in.own;
-    const CellState<R> &Rc = mir ? in.own : in.nb;
+    const CellStateA<A> &L = mir ? in.nb : in.own;
+    const CellStateA<A> &Rc = mir ? in.own : in.nb;
     const R cs = mir ? -in.cosj : in.cosj, sn = mir ? -in.sinj : in.sinj;
     const R clL = mir ? A::sqrt(A::mul(A::c(9.81), in.nb.h)) : cl_own;
     const OsherIn<R> oi = osher_inputs<A>(L, Rc, cs, sn, clL, mir, p);
@@ -697,14 +765,16 @@ __device__ __forceinline__ void flux_slot(const SlotIn<typename A::real> &in, ty
 // ---------------------------------------------------------------------------
 // UpdateCellKernel body, functors.cu:717-784 (variant F: v0 functors.cu:719-803)
 // ---------------------------------------------------------------------------
-template <class R>
+template <class R, class L = R>
 struct CellUpdateIn {
-    R h, u, v, zbc, fnc;
+    R h, u, v, fnc;
+    L zbc;
+    R hlo;             // split precision: the depth's compensation term
     R dta_or_area;     // variant H: DT/AREA; variant F: AREA
     R sidex;           // variant F: the CFL length of the cell (v0 functors.cu:752-763)
 };
-template <class R>
-struct CellUpdateOut { R h, u, v, z, w; };
+template <class R, class L = R>
+struct CellUpdateOut { R h, u, v, w; L z; R hlo; };
 
 // accumulate slot j's contribution (functors.cu:732-742), in slot order
 template <class A>
@@ -721,9 +791,9 @@ __device__ __forceinline__ void wsum_add(typename A::real &wh, typename A::real 
 }
 
 template <class A, int VARIANT>
-__device__ __forceinline__ CellUpdateOut<typename A::real> update_cell(const CellUpdateIn<typename A::real> &c,
-                                                                      typename A::real wh, typename A::real wu,
-                                                                      typename A::real wv, const StepParams &p) {
+__device__ __forceinline__ CellUpdateOut<typename A::real, typename A::level>
+update_cell(const CellUpdateIn<typename A::real, typename A::level> &c, typename A::real wh, typename A::real wu,
+            typename A::real wv, const StepParams &p) {
     using R = typename A::real;
     const R HM1 = A::c(p.hm1), HM2 = A::c(p.hm2), DT = A::c(p.dt);
     R dta;
@@ -737,9 +807,23 @@ __device__ __forceinline__ CellUpdateOut<typename A::real> update_cell(const Cel
         dta = c.dta_or_area;
     }
     const R cap = A::c(VARIANT == 1 ? 5.0 : 15.0);
-    CellUpdateOut<R> o;
-    o.h = A::fmax(A::add(A::madd(-dta, wh, c.h, M_H2), A::c(K::QLUA)), HM1);
-    o.z = A::add(o.h, c.zbc);
+    CellUpdateOut<R, typename A::level> o;
+    o.hlo = R(0);
+    if constexpr (is_split<A>::value) {
+        // H + (-DTA*WH), Kahan-compensated: (h, hlo) carries the depth to ~2x fp32
+        // precision.  A cell at the dry threshold has no compensation (its hlo,
+        // if any, is the level offset of split_level, not part of the depth).
+        const R comp = c.h > HM1 ? c.hlo : R(0);
+        const R y = A::madd(-dta, wh, comp, M_H2);
+        const R t = c.h + y;
+        o.hlo = y - (t - c.h);
+        o.h = t;
+        if (!(o.h > HM1)) { o.h = HM1; o.hlo = R(0); }
+        o.z = split_level<A>(o.h, o.hlo, c.zbc);
+    } else {
+        o.h = A::fmax(A::add(A::madd(-dta, wh, c.h, M_H2), A::c(K::QLUA)), HM1);
+        o.z = A::ladd(A::lvl(o.h), c.zbc);
+    }
     if (o.h <= HM1) {
         o.u = R(0); o.v = R(0);
     } else if (o.h <= HM2) {

@@ -97,16 +97,21 @@ constexpr int UPDATE_THREADS = 128;
 // and mirror each other exactly (reciprocal neighbours, negated normal, same
 // length), then every other real slot on its own.  The zero-length fourth slot
 // of a triangle is no record; the cell update evaluates it.
-template <class R>
+template <class A>
 struct DevMesh {
+    using Policy = A;
+    using R = typename A::real;
+    using L = typename A::level;
     int C;                     // cells
     int per_day;               // steps per table interval (steps_per_day - 1)
     int ndays, nb, nhq;
     int npairs, nrecords;
     double hm1, hm2, jl, dt;
-    R *S[2];                   // [C][4] state {H, U, V, Z}; a step reads S[step & 1], writes the other
+    R *S[2];                   // [C][4] state {H, U, V, Z}, split precision {H, U, V, H_lo};
+                               // a step reads S[step & 1], writes the other
     R *W;
-    const R *zbc, *fnc, *dta;  // dta: DT/AREA (variant H) or AREA (variant F)
+    const L *zbc;
+    const R *fnc, *dta;        // dta: DT/AREA (variant H) or AREA (variant F)
     const R *sidex;            // variant F CFL length
     const int32_t *bcell;      // [C] row of the boundary tables, -1 = none
     const uint8_t *cmask;      // [C] bit j: slot j is a real slot
@@ -117,18 +122,20 @@ struct DevMesh {
     uint8_t *rmeta;            // code | own_first | has_nb of slot a (code changes on breach)
     const R *rgeo;             // [nrecords][4] {COSF, SINF, SIDE, 0} of slot a
     R *f0, *f1, *f2, *f3;      // [4C] fluxes of the last step, index 4*cell + j
-    const R *bqt, *bdqt, *bzt, *bdzt;   // [ndays*nb]
-    const R *btop;             // [nb]
+    const R *bqt, *bdqt;       // [ndays*nb]
+    const L *bzt, *bdzt;       // [ndays*nb]
+    const L *btop;             // [nb]
     const int32_t *bnhq1;      // [nb]
-    const R *bzw, *bqw;        // [nb*nhq]; one extra zero row at index nb
+    const L *bzw;              // [nb*nhq]; one extra zero row at index nb
+    const R *bqw;              // [nb*nhq]; one extra zero row at index nb
     uint32_t *err;
     const long long *step_ctr;
 };
 
 struct StepIndex { int par, kt, jt; };
 
-template <class R>
-__device__ __forceinline__ StepIndex step_index(const DevMesh<R> &m, int k) {
+template <class A>
+__device__ __forceinline__ StepIndex step_index(const DevMesh<A> &m, int k) {
     const long long step = *m.step_ctr + k;
     StepIndex si;
     si.par = (int)(step & 1);
@@ -158,16 +165,18 @@ __device__ __forceinline__ void st4(float *p, float x, float y, float z, float w
     *reinterpret_cast<float4 *>(p) = make_float4(x, y, z, w);
 }
 
-template <class R>
-__device__ __forceinline__ CellState<R> load_cell(const DevMesh<R> &m, int par, int c) {
-    const Vec4<R> v = ld4(m.S[par] + 4 * (size_t)c);
-    return {v.x, v.y, v.z, v.w, m.zbc[c]};
+template <class A>
+__device__ __forceinline__ CellStateA<A> load_cell(const DevMesh<A> &m, int par, int c) {
+    const Vec4<typename A::real> v = ld4(m.S[par] + 4 * (size_t)c);
+    const typename A::level zbc = m.zbc[c];
+    if constexpr (is_split<A>::value) return {v.x, v.y, v.z, split_level<A>(v.x, v.w, zbc), zbc};
+    else return {v.x, v.y, v.z, v.w, zbc};
 }
 
 // the slot's terms of the cell sums (functors.cu:733-741): F0 and SIDE for
 // WH = fma(SIDE, F0, WH), and the complete WU / WV increments
 template <class A>
-__device__ __forceinline__ void store_terms(const DevMesh<typename A::real> &m, int s, const typename A::real f[4],
+__device__ __forceinline__ void store_terms(const DevMesh<A> &m, int s, const typename A::real f[4],
                                             typename A::real side, typename A::real cs, typename A::real sn) {
     using R = typename A::real;
     const R fr1 = A::add(f[1], f[3]);
@@ -177,29 +186,30 @@ __device__ __forceinline__ void store_terms(const DevMesh<typename A::real> &m, 
     st4(m.slotw + 4 * (size_t)s, f[0], dwu, dwv, side);
 }
 
-template <class R>
-__device__ __forceinline__ void store_flux(const DevMesh<R> &m, int s, const R f[4]) {
+template <class A>
+__device__ __forceinline__ void store_flux(const DevMesh<A> &m, int s, const typename A::real f[4]) {
     m.f0[s] = f[0]; m.f1[s] = f[1]; m.f2[s] = f[2]; m.f3[s] = f[3];
 }
 
 // One slot on its own: flux_slot with its boundary tables (functors.cu:47-202).
 template <class A, int VARIANT>
-__device__ __forceinline__ void single_record(const DevMesh<typename A::real> &m, int r, const StepIndex &si,
+__device__ __forceinline__ void single_record(const DevMesh<A> &m, int r, const StepIndex &si,
                                               const StepParams &p, int write_flux) {
     using R = typename A::real;
     const int4 ix = m.rix[r];
     const int a = ix.x, b = ix.y, sa = ix.z;
     const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
-    SlotIn<R> in;
+    using L = typename A::level;
+    SlotInA<A> in;
     in.own = load_cell(m, si.par, a);
     const uint8_t meta = m.rmeta[r];
     in.code = (int8_t)(meta & META_CODE);
     in.own_first = meta & META_OWN_FIRST;
     in.has_nb = meta & META_HAS_NB;
-    in.nb = in.has_nb ? load_cell(m, si.par, b) : CellState<R>{R(0), R(0), R(0), R(0), R(0)};
+    in.nb = in.has_nb ? load_cell(m, si.par, b) : CellStateA<A>{R(0), R(0), R(0), L(0), L(0)};
     in.cosj = g.x; in.sinj = g.y; in.side = g.z;
     auto fetch = [&]() {
-        BoundaryIn<R> bi;
+        BoundaryInA<A> bi;
         const int row = m.bcell[a];
         if (row >= 0) {
             const size_t q = (size_t)si.jt * m.nb + row;
@@ -207,7 +217,7 @@ __device__ __forceinline__ void single_record(const DevMesh<typename A::real> &m
             bi.top = m.btop[row]; bi.nhq1 = m.bnhq1[row];
             bi.zw = m.bzw + (size_t)row * m.nhq; bi.qw = m.bqw + (size_t)row * m.nhq;
         } else {
-            bi.qt = bi.dqt = bi.zt = bi.dzt = bi.top = R(0); bi.nhq1 = 0;
+            bi.qt = bi.dqt = R(0); bi.zt = bi.dzt = bi.top = L(0); bi.nhq1 = 0;
             bi.zw = m.bzw + (size_t)m.nb * m.nhq; bi.qw = m.bqw + (size_t)m.nb * m.nhq;
         }
         bi.nhq = m.nhq;
@@ -231,12 +241,12 @@ __device__ __forceinline__ void single_record(const DevMesh<typename A::real> &m
 // The mirrored Osher of a pair computed on its own (when its inputs differ
 // from the direct route's in the normal velocity).
 template <class A>
-__device__ __forceinline__ void pair_mirror(const DevMesh<typename A::real> &m, int r, const StepIndex &si,
+__device__ __forceinline__ void pair_mirror(const DevMesh<A> &m, int r, const StepIndex &si,
                                             const StepParams &p, int write_flux) {
     using R = typename A::real;
     const int4 ix = m.rix[r];
     const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
-    const CellState<R> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
+    const CellStateA<A> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
     const R cs = g.x, sn = g.y;
     const R clA = A::sqrt(A::mul(A::c(9.81), A_.h));
     const OsherIn<R> oi = osher_inputs<A>(A_, B_, cs, sn, clA, true, p);
@@ -265,7 +275,7 @@ __device__ __forceinline__ bool same_bits(R a, R b) {
 // that differs; otherwise the pair goes to a per-CTA queue whose mirrored
 // Osher evaluations run together after the main pass.
 template <class A, int VARIANT, int THREADS, int MINB>
-__global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<typename A::real> m, int k, int write_flux) {
+__global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k, int write_flux) {
     using R = typename A::real;
     __shared__ int queue[THREADS];
     __shared__ int qn;
@@ -279,11 +289,11 @@ __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<typename A:
     if (r < m.npairs) {
         const int4 ix = m.rix[r];
         const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
-        const CellState<R> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
+        const CellStateA<A> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
         const R cs = g.x, sn = g.y;
         const R clA = A::sqrt(A::mul(A::c(9.81), A_.h));
-        auto nofetch = []() { return BoundaryIn<R>{}; };
-        SlotIn<R> ia, ib;
+        auto nofetch = []() { return BoundaryInA<A>{}; };
+        SlotInA<A> ia, ib;
         ia.own = A_; ia.nb = B_; ia.has_nb = true; ia.own_first = true; ia.code = CODE_ZERO;
         ia.cosj = cs; ia.sinj = sn; ia.side = g.z;
         ib.own = B_; ib.nb = A_; ib.has_nb = true; ib.own_first = false; ib.code = CODE_ZERO;
@@ -351,14 +361,19 @@ __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<typename A:
 // zero-length fourth slot of a triangle is evaluated here without pow
 // (flux_slot's ZERO_LEN), exactly when fluxes are written out.
 template <class A, int VARIANT, int UMINB>
-__global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<typename A::real> m, int k, int write_flux) {
+__global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<A> m, int k, int write_flux) {
     using R = typename A::real;
     cudaGridDependencySynchronize();
     cudaTriggerProgrammaticLaunchCompletion();
     const StepIndex si = step_index(m, k);
     const StepParams p{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
+    using L = typename A::level;
     for (int c = blockIdx.x * UPDATE_THREADS + threadIdx.x; c < m.C; c += gridDim.x * UPDATE_THREADS) {
-    const CellState<R> st = load_cell(m, si.par, c);
+    const Vec4<R> raw = ld4(m.S[si.par] + 4 * (size_t)c);
+    CellStateA<A> st;
+    st.h = raw.x; st.u = raw.y; st.v = raw.z; st.zbc = m.zbc[c];
+    if constexpr (is_split<A>::value) st.z = split_level<A>(raw.x, raw.w, st.zbc);
+    else st.z = raw.w;
     const unsigned mask = m.cmask[c];
     const R fnc = m.fnc[c], dta = m.dta[c], sidex = VARIANT == 1 ? m.sidex[c] : R(0);
     Vec4<R> t[4];
@@ -374,12 +389,12 @@ __global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<t
             wu = A::add(wu, t[j].y);
             wv = A::add(wv, t[j].z);
         } else {
-            SlotIn<R> in;
+            SlotInA<A> in;
             in.own = st;
-            in.nb = {R(0), R(0), R(0), R(0), R(0)};
+            in.nb = {R(0), R(0), R(0), L(0), L(0)};
             in.has_nb = false; in.own_first = false; in.code = CODE_ZERO;
             in.cosj = R(0); in.sinj = R(0); in.side = R(0);
-            auto nofetch = []() { return BoundaryIn<R>{}; };
+            auto nofetch = []() { return BoundaryInA<A>{}; };
             SlotOut<R> o;
             if (write_flux) {
                 flux_slot<A, VARIANT, decltype(nofetch), false>(in, A::sqrt(A::mul(A::c(9.81), st.h)), p, nofetch, o);
@@ -391,14 +406,16 @@ __global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<t
             wsum_add<A>(wh, wu, wv, o.f[0], o.f[1], o.f[2], o.f[3], R(0), R(0), R(0));
         }
     }
-    CellUpdateIn<R> ci;
+    CellUpdateIn<R, L> ci;
     ci.h = st.h; ci.u = st.u; ci.v = st.v; ci.zbc = st.zbc;
+    ci.hlo = is_split<A>::value ? raw.w : R(0);
     ci.fnc = fnc;
     ci.dta_or_area = dta;
     ci.sidex = sidex;
-    CellUpdateOut<R> o = update_cell<A, VARIANT>(ci, wh, wu, wv, p);
+    CellUpdateOut<R, L> o = update_cell<A, VARIANT>(ci, wh, wu, wv, p);
     const int np = si.par ^ 1;
-    st4(m.S[np] + 4 * (size_t)c, o.h, o.u, o.v, o.z);
+    if constexpr (is_split<A>::value) st4(m.S[np] + 4 * (size_t)c, o.h, o.u, o.v, o.hlo);
+    else st4(m.S[np] + 4 * (size_t)c, o.h, o.u, o.v, o.z);
     m.W[c] = o.w;
     if (!(isfinite((double)o.h) && isfinite((double)o.u) && isfinite((double)o.v))) atomicOr(m.err, ERRBIT_NONFINITE);
     }
@@ -406,31 +423,60 @@ __global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<t
 
 __global__ void tick_kernel(long long *ctr, int n) { *ctr += n; }
 
+// Split precision state <-> the reference's (H, Z) of one cell.  The depth is
+// kept as the fp32 pair (h, hlo) with h + hlo = H; a cell at or below the dry
+// threshold keeps in hlo the offset of its level instead (split_level).
+struct SplitCodec {
+    static __host__ __device__ inline void encode(double H, double Z, double zbc, float hm1f, float &h, float &hlo) {
+        h = (float)H;
+        hlo = h > hm1f ? (float)(H - (double)h) : (float)((Z - zbc) - (double)h);
+    }
+    static __host__ __device__ inline double depth(float h, float hlo, float hm1f, double hm1) {
+        return h > hm1f ? (double)h + (double)hlo : (h == hm1f ? hm1 : (double)h);
+    }
+    static __host__ __device__ inline double level(float h, float hlo, double zbc) {
+        return (double)h + ((double)hlo + zbc);
+    }
+};
+
 // reference-order staging <-> device-order state (perm[new] = old)
-template <class R>
-__global__ void stage_in_kernel(int C, const int32_t *__restrict__ perm, const double *__restrict__ stage,
-                                const long long *ctr, R *S0, R *S1) {
+template <class A>
+__global__ void stage_in_kernel(DevMesh<A> m, const int32_t *__restrict__ perm, const double *__restrict__ stage) {
+    using R = typename A::real;
+    const int C = m.C;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C) return;
     const int o = perm[i];
-    R *d = (((*ctr) & 1) ? S1 : S0) + 4 * (size_t)i;
-    d[0] = (R)stage[o];
+    R *d = m.S[(*m.step_ctr) & 1] + 4 * (size_t)i;
     d[1] = (R)stage[(size_t)C + o];
     d[2] = (R)stage[2 * (size_t)C + o];
-    d[3] = (R)stage[3 * (size_t)C + o];
+    if constexpr (is_split<A>::value) {
+        float h, hlo;
+        SplitCodec::encode(stage[o], stage[3 * (size_t)C + o], m.zbc[i], (float)m.hm1, h, hlo);
+        d[0] = h; d[3] = hlo;
+    } else {
+        d[0] = (R)stage[o];
+        d[3] = (R)stage[3 * (size_t)C + o];
+    }
 }
-template <class R>
-__global__ void stage_out_kernel(int C, const int32_t *__restrict__ perm, double *__restrict__ stage,
-                                 const long long *ctr, const R *S0, const R *S1, const R *W) {
+template <class A>
+__global__ void stage_out_kernel(DevMesh<A> m, const int32_t *__restrict__ perm, double *__restrict__ stage) {
+    using R = typename A::real;
+    const int C = m.C;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C) return;
     const int o = perm[i];
-    const R *d = (((*ctr) & 1) ? S1 : S0) + 4 * (size_t)i;
-    stage[o] = (double)d[0];
+    const R *d = m.S[(*m.step_ctr) & 1] + 4 * (size_t)i;
     stage[(size_t)C + o] = (double)d[1];
     stage[2 * (size_t)C + o] = (double)d[2];
-    stage[3 * (size_t)C + o] = (double)d[3];
-    stage[4 * (size_t)C + o] = (double)W[i];
+    if constexpr (is_split<A>::value) {
+        stage[o] = SplitCodec::depth(d[0], d[3], (float)m.hm1, m.hm1);
+        stage[3 * (size_t)C + o] = SplitCodec::level(d[0], d[3], m.zbc[i]);
+    } else {
+        stage[o] = (double)d[0];
+        stage[3 * (size_t)C + o] = (double)d[3];
+    }
+    stage[4 * (size_t)C + o] = (double)m.W[i];
 }
 
 // per-cell constants that the update needs, computed on the device with the
@@ -521,8 +567,9 @@ struct hb_handle {
     std::vector<int32_t> inv;        // inv[old] = new
     std::vector<double> klas_orig;   // [4C] reference order
     std::vector<void *> allocs;
-    hb::DevMesh<double> m64{};
-    hb::DevMesh<float> m32{};
+    hb::DevMesh<hb::F64Exact> m64{};
+    hb::DevMesh<hb::F32Fast> m32{};
+    hb::DevMesh<hb::F32Split> ms{};
     uint32_t *d_err = nullptr;
     long long *d_ctr = nullptr;
     int32_t *d_perm = nullptr;       // perm on the device
@@ -534,7 +581,14 @@ struct hb_handle {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_steps = 0;
     int launch_config = 0;           // index into LAUNCH_CONFIGS
-    bool fp32() const { return opt.precision == HB_FP32; }
+    // f(mesh) on the device mesh of this handle's precision
+    template <class F> int with_mesh(F &&f) {
+        switch (opt.precision) {
+        case HB_FP32: return f(m32);
+        case HB_SPLIT: return f(ms);
+        default: return f(m64);
+        }
+    }
     ~hb_handle() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (graph) cudaGraphDestroy(graph);
@@ -570,8 +624,10 @@ int dev_alloc(hb_handle *h, T **dst, size_t count) {
 
 #define TRY(x) do { int st_ = (x); if (st_ != HB_OK) return st_; } while (0)
 
-template <class R>
-int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
+template <class A>
+int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<A> &m) {
+    using R = typename A::real;
+    using L = typename A::level;
     const int C = h->C;
     const size_t S = 4 * (size_t)C;
     const auto &perm = h->perm;
@@ -579,6 +635,11 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
     auto cellv = [&](const double *src) {
         std::vector<R> v(C);
         for (int i = 0; i < C; i++) v[i] = (R)src[perm[i]];
+        return v;
+    };
+    auto cell_levels = [&](const double *src) {
+        std::vector<L> v(C);
+        for (int i = 0; i < C; i++) v[i] = (L)src[perm[i]];
         return v;
     };
     auto slotv = [&](const double *src) {
@@ -671,29 +732,29 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
     std::vector<int> rows;
     for (int i = 0; i < C; i++) if (needs_table[i]) { bcell[i] = (int32_t)rows.size(); rows.push_back(i); }
     const int NB = (int)rows.size(), ND = h->ndays, NHQ = std::max(h->nhq, 0);
-    std::vector<R> bqt((size_t)ND * NB), bdqt((size_t)ND * NB), bzt((size_t)ND * NB), bdzt((size_t)ND * NB);
-    std::vector<R> btop(NB), bzw((size_t)(NB + 1) * NHQ, R(0)), bqw((size_t)(NB + 1) * NHQ, R(0));
+    std::vector<R> bqt((size_t)ND * NB), bdqt((size_t)ND * NB), bqw((size_t)(NB + 1) * NHQ, R(0));
+    std::vector<L> bzt((size_t)ND * NB), bdzt((size_t)ND * NB), btop(NB), bzw((size_t)(NB + 1) * NHQ, L(0));
     std::vector<int32_t> bnhq1(NB);
     for (int r = 0; r < NB; r++) {
         const int old = perm[rows[r]];
         for (int d = 0; d < ND; d++) {
             const size_t t = (size_t)d * C + old;
             bqt[(size_t)d * NB + r] = (R)md->qt[t]; bdqt[(size_t)d * NB + r] = (R)md->dqt[t];
-            bzt[(size_t)d * NB + r] = (R)md->zt[t]; bdzt[(size_t)d * NB + r] = (R)md->dzt[t];
+            bzt[(size_t)d * NB + r] = (L)md->zt[t]; bdzt[(size_t)d * NB + r] = (L)md->dzt[t];
         }
-        btop[r] = (R)md->bfeat[old];
+        btop[r] = (L)md->bfeat[old];
         bnhq1[r] = md->nhq1[old];
         for (int q = 0; q < NHQ; q++) {
-            bzw[(size_t)r * NHQ + q] = (R)md->zw[(size_t)old * NHQ + q];
+            bzw[(size_t)r * NHQ + q] = (L)md->zw[(size_t)old * NHQ + q];
             bqw[(size_t)r * NHQ + q] = (R)md->qw[(size_t)old * NHQ + q];
         }
     }
     m.nb = NB;
-    const R *c;
     int32_t *ip;
     uint8_t *up;
     R *rp;
-    TRY(dev_upload(h, &rp, cellv(md->zbc))); m.zbc = rp;
+    L *lp;
+    TRY(dev_upload(h, &lp, cell_levels(md->zbc))); m.zbc = lp;
     TRY(dev_upload(h, &rp, cellv(md->fnc))); m.fnc = rp;
     R *area_d = nullptr, *side_d = nullptr;
     TRY(dev_upload(h, &area_d, cellv(md->area)));
@@ -714,11 +775,11 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
     TRY(dev_upload(h, &ip, bcell)); m.bcell = ip;
     TRY(dev_upload(h, &rp, bqt)); m.bqt = rp;
     TRY(dev_upload(h, &rp, bdqt)); m.bdqt = rp;
-    TRY(dev_upload(h, &rp, bzt)); m.bzt = rp;
-    TRY(dev_upload(h, &rp, bdzt)); m.bdzt = rp;
-    TRY(dev_upload(h, &rp, btop)); m.btop = rp;
+    TRY(dev_upload(h, &lp, bzt)); m.bzt = lp;
+    TRY(dev_upload(h, &lp, bdzt)); m.bdzt = lp;
+    TRY(dev_upload(h, &lp, btop)); m.btop = lp;
     TRY(dev_upload(h, &ip, bnhq1)); m.bnhq1 = ip;
-    TRY(dev_upload(h, &rp, bzw)); m.bzw = rp;
+    TRY(dev_upload(h, &lp, bzw)); m.bzw = lp;
     TRY(dev_upload(h, &rp, bqw)); m.bqw = rp;
     for (int b = 0; b < 2; b++) TRY(dev_alloc(h, &m.S[b], 4 * (size_t)C));
     TRY(dev_alloc(h, &m.slotw, 16 * (size_t)C));
@@ -729,7 +790,6 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
     TRY(dev_alloc(h, &dta, C));
     TRY(dev_alloc(h, &sidex, C));
     const int blocks = (C + 255) / 256;
-    using A = typename std::conditional<std::is_same<R, double>::value, hb::F64Exact, hb::F32Fast>::type;
     if (h->opt.variant == HB_VARIANT_F) hb::setup_cells_kernel<A, 1><<<blocks, 256>>>(C, h->dt, area_d, side_d, dta, sidex);
     else hb::setup_cells_kernel<A, 0><<<blocks, 256>>>(C, h->dt, area_d, side_d, dta, sidex);
     HB_CUDA_RET(cudaGetLastError());
@@ -738,12 +798,11 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<R> &m) {
     m.sidex = sidex;
     m.err = h->d_err;
     m.step_ctr = h->d_ctr;
-    (void)c;
     return HB_OK;
 }
 
 template <class A, int VARIANT>
-int launch_steps(hb_handle *h, hb::DevMesh<typename A::real> &m, int n, cudaStream_t st) {
+int launch_steps(hb_handle *h, hb::DevMesh<A> &m, int n, cudaStream_t st) {
     // Programmatic dependent launch: each kernel may start while its predecessor
     // drains and waits in cudaGridDependencySynchronize for its results.
     cudaLaunchAttribute attr[1];
@@ -789,8 +848,10 @@ int launch_steps(hb_handle *h, hb::DevMesh<typename A::real> &m, int n, cudaStre
 int enqueue_steps(hb_handle *h, int n, cudaStream_t st) {
     if (n <= 0) return HB_OK;
     const bool f = h->opt.variant == HB_VARIANT_F;
-    if (h->fp32()) return f ? launch_steps<hb::F32Fast, 1>(h, h->m32, n, st) : launch_steps<hb::F32Fast, 0>(h, h->m32, n, st);
-    return f ? launch_steps<hb::F64Exact, 1>(h, h->m64, n, st) : launch_steps<hb::F64Exact, 0>(h, h->m64, n, st);
+    return h->with_mesh([&](auto &m) {
+        using A = typename std::remove_reference<decltype(m)>::type::Policy;
+        return f ? launch_steps<A, 1>(h, m, n, st) : launch_steps<A, 0>(h, m, n, st);
+    });
 }
 
 int check_range(hb_handle *h, long long n) {
@@ -816,7 +877,7 @@ extern "C" int hb_create(const hb_mesh_desc *md, const hb_options *opt_in, hb_ha
     *out = nullptr;
     hb_options opt;
     if (opt_in) opt = *opt_in; else hb_options_default(&opt);
-    if (opt.precision != HB_FP64 && opt.precision != HB_FP32)
+    if (opt.precision != HB_FP64 && opt.precision != HB_FP32 && opt.precision != HB_SPLIT)
         return hb::set_error(HB_E_INVALID, "hb_create: precision %d not available on this path", opt.precision);
     if (md->cells <= 0 || md->ndays <= 0 || md->steps_per_day < 2 || md->nhq < 0)
         return hb::set_error(HB_E_INVALID, "hb_create: cells=%d ndays=%d steps_per_day=%d", md->cells, md->ndays,
@@ -859,7 +920,7 @@ extern "C" int hb_create(const hb_mesh_desc *md, const hb_options *opt_in, hb_ha
         delete h;
         return st;
     }
-    st = h->fp32() ? build_device_mesh<float>(h, md, h->m32) : build_device_mesh<double>(h, md, h->m64);
+    st = h->with_mesh([&](auto &m) { return build_device_mesh(h, md, m); });
     if (st != HB_OK) { delete h; return st; }
     *out = h;
     return HB_OK;
@@ -871,44 +932,43 @@ extern "C" int hb_destroy(hb_handle *h) {
 }
 
 namespace {
-template <class R>
-int set_state_t(hb_handle *h, hb::DevMesh<R> &m, const double *H, const double *U, const double *V, const double *Z,
+// State in and out go through the reference-order staging buffer and the
+// staging kernels, which hold each precision's conversion (SplitCodec).
+template <class A>
+int set_state_t(hb_handle *h, hb::DevMesh<A> &m, const double *H, const double *U, const double *V, const double *Z,
                 const double *W) {
+    using R = typename A::real;
     const int C = h->C;
-    const int par = (int)(h->steps_done & 1);
-    const double *src[5] = {H, U, V, Z, W};
+    const double *src[4] = {H, U, V, Z};
     for (int k = 0; k < 4; k++)
         if (!src[k]) return hb::set_error(HB_E_INVALID, "hb_set_state: missing array");
-    std::vector<R> buf(4 * (size_t)C);
-    for (int i = 0; i < C; i++)
-        for (int k = 0; k < 4; k++) buf[4 * (size_t)i + k] = (R)src[k][h->perm[i]];
-    HB_CUDA_RET(cudaMemcpy(m.S[par], buf.data(), buf.size() * sizeof(R), cudaMemcpyHostToDevice));
+    HB_CUDA_RET(cudaDeviceSynchronize());
+    for (int k = 0; k < 4; k++)
+        HB_CUDA_RET(cudaMemcpy(h->d_stage + (size_t)k * C, src[k], C * sizeof(double), cudaMemcpyHostToDevice));
+    hb::stage_in_kernel<A><<<(C + 255) / 256, 256>>>(m, h->d_perm, h->d_stage);
+    HB_CUDA_RET(cudaGetLastError());
     if (W) {
         std::vector<R> w(C);
         for (int i = 0; i < C; i++) w[i] = (R)W[h->perm[i]];
         HB_CUDA_RET(cudaMemcpy(m.W, w.data(), C * sizeof(R), cudaMemcpyHostToDevice));
     }
+    HB_CUDA_RET(cudaDeviceSynchronize());
     return HB_OK;
 }
-template <class R>
-int get_state_t(hb_handle *h, hb::DevMesh<R> &m, double *H, double *U, double *V, double *Z, double *W) {
+template <class A>
+int get_state_t(hb_handle *h, hb::DevMesh<A> &m, double *H, double *U, double *V, double *Z, double *W) {
     const int C = h->C;
-    const int par = (int)(h->steps_done & 1);
     double *dst[5] = {H, U, V, Z, W};
     HB_CUDA_RET(cudaDeviceSynchronize());
-    std::vector<R> buf(4 * (size_t)C);
-    HB_CUDA_RET(cudaMemcpy(buf.data(), m.S[par], buf.size() * sizeof(R), cudaMemcpyDeviceToHost));
-    for (int k = 0; k < 4; k++)
-        if (dst[k])
-            for (int i = 0; i < C; i++) dst[k][h->perm[i]] = (double)buf[4 * (size_t)i + k];
-    if (W) {
-        HB_CUDA_RET(cudaMemcpy(buf.data(), m.W, C * sizeof(R), cudaMemcpyDeviceToHost));
-        for (int i = 0; i < C; i++) W[h->perm[i]] = (double)buf[i];
-    }
+    hb::stage_out_kernel<A><<<(C + 255) / 256, 256>>>(m, h->d_perm, h->d_stage);
+    HB_CUDA_RET(cudaGetLastError());
+    for (int k = 0; k < 5; k++)
+        if (dst[k]) HB_CUDA_RET(cudaMemcpy(dst[k], h->d_stage + (size_t)k * C, C * sizeof(double), cudaMemcpyDeviceToHost));
     return HB_OK;
 }
-template <class R>
-int get_flux_t(hb_handle *h, hb::DevMesh<R> &m, double *F0, double *F1, double *F2, double *F3) {
+template <class A>
+int get_flux_t(hb_handle *h, hb::DevMesh<A> &m, double *F0, double *F1, double *F2, double *F3) {
+    using R = typename A::real;
     const int C = h->C;
     const size_t S = 4 * (size_t)C;
     std::vector<R> buf(S);
@@ -923,8 +983,8 @@ int get_flux_t(hb_handle *h, hb::DevMesh<R> &m, double *F0, double *F1, double *
     }
     return HB_OK;
 }
-template <class R>
-int get_klas_t(hb_handle *h, hb::DevMesh<R> &m, double *klas) {
+template <class A>
+int get_klas_t(hb_handle *h, hb::DevMesh<A> &m, double *klas) {
     const int C = h->C;
     const size_t S = 4 * (size_t)C;
     std::vector<uint8_t> meta(std::max(h->nslots, 1));
@@ -945,19 +1005,19 @@ int get_klas_t(hb_handle *h, hb::DevMesh<R> &m, double *klas) {
 
 extern "C" int hb_set_state(hb_handle *h, const double *H, const double *U, const double *V, const double *Z, const double *W) {
     if (!h) return hb::set_error(HB_E_INVALID, "null handle");
-    return h->fp32() ? set_state_t(h, h->m32, H, U, V, Z, W) : set_state_t(h, h->m64, H, U, V, Z, W);
+    return h->with_mesh([&](auto &m) { return set_state_t(h, m, H, U, V, Z, W); });
 }
 extern "C" int hb_get_state(hb_handle *h, double *H, double *U, double *V, double *Z, double *W) {
     if (!h) return hb::set_error(HB_E_INVALID, "null handle");
-    return h->fp32() ? get_state_t(h, h->m32, H, U, V, Z, W) : get_state_t(h, h->m64, H, U, V, Z, W);
+    return h->with_mesh([&](auto &m) { return get_state_t(h, m, H, U, V, Z, W); });
 }
 extern "C" int hb_get_flux(hb_handle *h, double *F0, double *F1, double *F2, double *F3) {
     if (!h) return hb::set_error(HB_E_INVALID, "null handle");
-    return h->fp32() ? get_flux_t(h, h->m32, F0, F1, F2, F3) : get_flux_t(h, h->m64, F0, F1, F2, F3);
+    return h->with_mesh([&](auto &m) { return get_flux_t(h, m, F0, F1, F2, F3); });
 }
 extern "C" int hb_get_klas(hb_handle *h, double *klas) {
     if (!h || !klas) return hb::set_error(HB_E_INVALID, "null argument");
-    return h->fp32() ? get_klas_t(h, h->m32, klas) : get_klas_t(h, h->m64, klas);
+    return h->with_mesh([&](auto &m) { return get_klas_t(h, m, klas); });
 }
 
 extern "C" int hb_step(hb_handle *h, int32_t nsteps, void *stream) {
@@ -969,18 +1029,18 @@ extern "C" int hb_step(hb_handle *h, int32_t nsteps, void *stream) {
 }
 
 namespace {
-template <class R>
-int step_host_t(hb_handle *h, hb::DevMesh<R> &m, double *H, double *U, double *V, double *Z, double *W, int n,
+template <class A>
+int step_host_t(hb_handle *h, hb::DevMesh<A> &m, double *H, double *U, double *V, double *Z, double *W, int n,
                 cudaStream_t st) {
     const int C = h->C;
     const size_t b = (size_t)C * sizeof(double);
     double *io[5] = {H, U, V, Z, W};
     for (int k = 0; k < 4; k++) HB_CUDA_RET(cudaMemcpyAsync(h->d_stage + (size_t)k * C, io[k], b, cudaMemcpyHostToDevice, st));
     const int blocks = (C + 255) / 256;
-    hb::stage_in_kernel<R><<<blocks, 256, 0, st>>>(C, h->d_perm, h->d_stage, h->d_ctr, m.S[0], m.S[1]);
+    hb::stage_in_kernel<A><<<blocks, 256, 0, st>>>(m, h->d_perm, h->d_stage);
     HB_CUDA_RET(cudaGetLastError());
     TRY(enqueue_steps(h, n, st));
-    hb::stage_out_kernel<R><<<blocks, 256, 0, st>>>(C, h->d_perm, h->d_stage, h->d_ctr, m.S[0], m.S[1], m.W);
+    hb::stage_out_kernel<A><<<blocks, 256, 0, st>>>(m, h->d_perm, h->d_stage);
     HB_CUDA_RET(cudaGetLastError());
     for (int k = 0; k < 5; k++)
         if (io[k]) HB_CUDA_RET(cudaMemcpyAsync(io[k], h->d_stage + (size_t)k * C, b, cudaMemcpyDeviceToHost, st));
@@ -993,7 +1053,7 @@ extern "C" int hb_step_host(hb_handle *h, double *H, double *U, double *V, doubl
     if (!h || !H || !U || !V || !Z || nsteps < 0) return hb::set_error(HB_E_INVALID, "hb_step_host: bad argument");
     TRY(check_range(h, nsteps));
     cudaStream_t st = (cudaStream_t)stream;
-    int r = h->fp32() ? step_host_t(h, h->m32, H, U, V, Z, W, nsteps, st) : step_host_t(h, h->m64, H, U, V, Z, W, nsteps, st);
+    int r = h->with_mesh([&](auto &m) { return step_host_t(h, m, H, U, V, Z, W, nsteps, st); });
     if (r == HB_OK) h->steps_done += nsteps;
     return r;
 }
@@ -1028,10 +1088,11 @@ extern "C" int hb_set_position(hb_handle *h, int64_t steps_done) {
     HB_CUDA_RET(cudaDeviceSynchronize());
     // keep the state in place: it sits in buffer (steps_done & 1)
     if ((steps_done & 1) != (h->steps_done & 1)) {
-        const size_t bytes = (size_t)h->C * (h->fp32() ? sizeof(float) : sizeof(double));
         const int from = (int)(h->steps_done & 1), to = from ^ 1;
-        if (h->fp32()) HB_CUDA_RET(cudaMemcpy(h->m32.S[to], h->m32.S[from], 4 * bytes, cudaMemcpyDeviceToDevice));
-        else HB_CUDA_RET(cudaMemcpy(h->m64.S[to], h->m64.S[from], 4 * bytes, cudaMemcpyDeviceToDevice));
+        TRY(h->with_mesh([&](auto &m) -> int {
+            HB_CUDA_RET(cudaMemcpy(m.S[to], m.S[from], 4 * (size_t)h->C * sizeof(*m.S[0]), cudaMemcpyDeviceToDevice));
+            return HB_OK;
+        }));
     }
     long long v = steps_done;
     HB_CUDA_RET(cudaMemcpy(h->d_ctr, &v, sizeof v, cudaMemcpyHostToDevice));
@@ -1071,15 +1132,16 @@ extern "C" int hb_graph_launch(hb_handle *h, void *stream) {
 extern "C" int hb_device_state(hb_handle *h, void **H, void **U, void **V, void **Z, void **W, int32_t *stride) {
     if (!h) return hb::set_error(HB_E_INVALID, "null handle");
     const int par = (int)(h->steps_done & 1);
-    if (h->fp32()) {
-        float *b = h->m32.S[par];
-        if (H) *H = b; if (U) *U = b + 1; if (V) *V = b + 2; if (Z) *Z = b + 3;
-        if (W) *W = h->m32.W;
-    } else {
-        double *b = h->m64.S[par];
-        if (H) *H = b; if (U) *U = b + 1; if (V) *V = b + 2; if (Z) *Z = b + 3;
-        if (W) *W = h->m64.W;
-    }
+    h->with_mesh([&](auto &m) {
+        auto *b = m.S[par];
+        if (H) *H = b;
+        if (U) *U = b + 1;
+        if (V) *V = b + 2;
+        // split precision keeps no level: its fourth entry is the depth's low part
+        if (Z) *Z = h->opt.precision == HB_SPLIT ? nullptr : (void *)(b + 3);
+        if (W) *W = m.W;
+        return HB_OK;
+    });
     if (stride) *stride = 4;
     return HB_OK;
 }

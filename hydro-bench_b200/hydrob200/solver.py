@@ -37,14 +37,15 @@ class Deck:
 
     def __init__(self, root: str):
         self._h = C.c_void_p()
-        check(lib().hb_deck_load(root.encode(), C.byref(self._h)))
+        self._lib = lib()   # held for __del__, which may run after module teardown
+        check(self._lib.hb_deck_load(root.encode(), C.byref(self._h)))
         self.root = root
         self.mesh = _lib.MeshDesc()
         check(lib().hb_deck_mesh(self._h, C.byref(self.mesh)))
 
     def __del__(self):
         if getattr(self, "_h", None) and self._h.value:
-            lib().hb_deck_free(self._h)
+            self._lib.hb_deck_free(self._h)
             self._h = C.c_void_p()
 
     @property

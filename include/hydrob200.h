@@ -37,6 +37,12 @@ typedef enum {
 } hb_status;
 
 typedef enum { HB_VARIANT_H = 0, HB_VARIANT_F = 1 } hb_variant;
+/* HB_FP64: the reference's fp64 kernels, bit for bit.  HB_FP32: the fp32 tree
+ * (cuda_native_impl/fp32_src).  HB_SPLIT: no reference counterpart; fluxes,
+ * velocities and depths in fp32, while water levels, beds and boundary levels
+ * stay fp64, every depth formed as level minus bed is taken in fp64, and each
+ * cell's depth update is Kahan-compensated.  Its device state is the fp32
+ * quadruple {H, U, V, H_lo} (no Z; hb_get_state rebuilds Z in fp64). */
 typedef enum { HB_FP64 = 0, HB_FP32 = 1, HB_SPLIT = 2 } hb_precision;
 
 /* Host description of a mesh and its boundary tables, reference layout.
