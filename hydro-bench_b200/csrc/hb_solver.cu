@@ -1,19 +1,23 @@
-// hb_solver.cu -- the handle-based path: the mesh lives on the device in a
-// bandwidth-reduced cell order, and one kernel launch per step computes every
-// slot's flux and the cell update together.
+// hb_solver.cu -- the handle-based path.  The mesh lives on the device in a
+// bandwidth-reduced cell order; a step is two kernels chained by programmatic
+// dependent launch:
+//   flux_kernel    one thread per flux record: an interior edge whose two slots
+//                  mirror each other (one Osher evaluation serves both), or a
+//                  single slot (CalculateFluxKernel, functors.cu:47-202);
+//   update_kernel  one thread per cell: the slot sums in slot order j = 0..3
+//                  and the new state (UpdateCellKernel, functors.cu:717-784).
+// The state is double-buffered: a step reads buffer (step & 1) and writes the
+// other, which is what the reference's two-kernel sequence amounts to.  The
+// per-slot flux arrays are written only by the last step of a launch
+// sequence, plus every step for the slots whose boundary code leaves some
+// fluxes unwritten (those keep their old values, functors.cu:525-565).
 //
-// Step kernel layout: four consecutive lanes of a warp own the four slots of
-// one cell (slot j on lane 4*c + j).  Each lane computes its slot's flux
-// (CalculateFluxKernel, functors.cu:47-202), the four lanes exchange their
-// fluxes with warp shuffles and sum them in slot order j = 0..3 (the order of
-// UpdateCellKernel, functors.cu:732-742), and lane j = 0 writes the cell's new
-// state (functors.cu:744-783).  The state is double-buffered: a step reads
-// buffer (step & 1) and writes the other, which is what the reference's
-// two-kernel sequence amounts to.  The per-slot flux arrays are written only
-// by the last step of a launch sequence, plus every step for the slots whose
-// boundary code leaves some fluxes unwritten (those keep their old values,
-// functors.cu:525-565).
+// A handle may hold a batch of independent scenarios (hb_create_batch).  Their
+// cells and records are concatenated, each scenario renumbered on its own, and
+// per-CTA segment tables give every CTA one scenario and a record or cell
+// range, so one launch pair steps the whole batch.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -92,6 +96,13 @@ constexpr int N_LAUNCH_CONFIGS = sizeof(LAUNCH_CONFIGS) / sizeof(LAUNCH_CONFIGS[
 constexpr int DEFAULT_LAUNCH_CONFIG = 0;
 constexpr int UPDATE_THREADS = 128;
 
+// Constants of one scenario of a batch (the only entry for a single mesh).
+struct ScnParams {
+    double hm1, hm2, jl, dt;
+    int per_day, ndays;        // steps per table interval; intervals in the tables
+    int cell0, cells;          // the scenario's cells in the device order
+};
+
 // Device mesh.  Cells are in reverse Cuthill-McKee order.  The flux work is a
 // list of records: first the interior edges whose two slots both have code 0
 // and mirror each other exactly (reciprocal neighbours, negated normal, same
@@ -130,20 +141,25 @@ struct DevMesh {
     const R *bqw;              // [nb*nhq]; one extra zero row at index nb
     uint32_t *err;
     const long long *step_ctr;
+    // batches: per-CTA segment tables, one scenario per CTA
+    int nscen;
+    const ScnParams *scn;      // [nscen]
+    const int4 *fseg;          // flux CTAs {scenario, first record, records, 1 = mirror pairs}
+    const int4 *useg;          // update CTAs {scenario, first cell, cells, 0}
 };
 
 struct StepIndex { int par, kt, jt; };
 
 template <class A>
-__device__ __forceinline__ StepIndex step_index(const DevMesh<A> &m, int k) {
+__device__ __forceinline__ StepIndex step_index(const DevMesh<A> &m, int k, int per_day, int ndays) {
     const long long step = *m.step_ctr + k;
     StepIndex si;
     si.par = (int)(step & 1);
-    si.jt = (int)(step / m.per_day);
-    si.kt = 1 + (int)(step % m.per_day);
-    if (si.jt >= m.ndays) {   // beyond the boundary tables: never read past them
-        if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(m.err, ERRBIT_TABLE_RANGE);
-        si.jt = m.ndays - 1;
+    si.jt = (int)(step / per_day);
+    si.kt = 1 + (int)(step % per_day);
+    if (si.jt >= ndays) {   // beyond the boundary tables: never read past them
+        if (threadIdx.x == 0) atomicOr(m.err, ERRBIT_TABLE_RANGE);
+        si.jt = ndays - 1;
     }
     return si;
 }
@@ -266,109 +282,131 @@ __device__ __forceinline__ bool same_bits(R a, R b) {
     else return __float_as_int((float)a) == __float_as_int((float)b);
 }
 
-// Flux of every record of one step.  A pair evaluates both slots' branch
-// chains (functors.cu:98-150) and, when both reach Osher, runs it once: the
-// direct route at a and the mirrored route at b have the same cells, normal
-// and inputs except two rotations that the reference build rounds
-// differently.  When those agree bit for bit the two Osher evaluations are
-// identical, and the b side's FLUX2 is re-summed with its own tangent if only
-// that differs; otherwise the pair goes to a per-CTA queue whose mirrored
-// Osher evaluations run together after the main pass.
-template <class A, int VARIANT, int THREADS, int MINB>
-__global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k, int write_flux) {
+// One mirror-pair record.  It evaluates both slots' branch chains
+// (functors.cu:98-150) and, when both reach Osher, runs it once: the direct
+// route at a and the mirrored route at b have the same cells, normal and
+// inputs except two rotations that the reference build rounds differently.
+// When those agree bit for bit the two Osher evaluations are identical, and
+// the b side's FLUX2 is re-summed with its own tangent if only that differs;
+// otherwise the pair goes to the CTA's queue, whose mirrored Osher
+// evaluations run together after the main pass (pair_mirror).
+template <class A, int VARIANT>
+__device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const StepIndex &si, const StepParams &p,
+                                            int write_flux, int *queue, int *qn) {
     using R = typename A::real;
+    const int4 ix = m.rix[r];
+    const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
+    const CellStateA<A> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
+    const R cs = g.x, sn = g.y;
+    const R clA = A::sqrt(A::mul(A::c(9.81), A_.h));
+    auto nofetch = []() { return BoundaryInA<A>{}; };
+    SlotInA<A> ia, ib;
+    ia.own = A_; ia.nb = B_; ia.has_nb = true; ia.own_first = true; ia.code = CODE_ZERO;
+    ia.cosj = cs; ia.sinj = sn; ia.side = g.z;
+    ib.own = B_; ib.nb = A_; ib.has_nb = true; ib.own_first = false; ib.code = CODE_ZERO;
+    ib.cosj = -cs; ib.sinj = -sn; ib.side = ia.side;
+    // each side's branch chain; a side whose fluxes are final is written at once
+    int ra_, rb_;
+    {
+        SlotOut<R> oa;
+        ra_ = flux_chain<A, VARIANT>(ia, clA, p, nofetch, oa);   // 0 or 1 (direct)
+        if (!ra_) {
+            if (write_flux) store_flux(m, ix.z, oa.f);
+            store_terms<A>(m, ix.z, oa.f, g.z, cs, sn);
+        }
+    }
+    {
+        SlotOut<R> ob;
+        rb_ = flux_chain<A, VARIANT>(ib, R(0), p, nofetch, ob);  // 0 or 2 (mirrored)
+        if (!rb_) {
+            if (write_flux) store_flux(m, ix.w, ob.f);
+            store_terms<A>(m, ix.w, ob.f, g.z, -cs, -sn);
+        }
+    }
+    if (ra_ | rb_) {
+        // the two routes' inputs differ only in QL2, UR and so QR1 (osher_inputs)
+        OsherIn<R> oi = osher_inputs<A>(A_, B_, cs, sn, clA, ra_ == 0, p);
+        const R ql2_d = oi.ql[2], ur_d = oi.ur, qr1_d = oi.qr[1];
+        const R ql2_m = ra_ ? A::dot(A_.v, cs, -A_.u, sn, M_QL2M) : ql2_d;
+        const R ur_m = ra_ ? A::dot(B_.u, cs, B_.v, sn, M_UR1) : ur_d;
+        R qr1_m = A::mul(ur_m, oi.ratio);
+        if (oi.hcR <= A::c(p.hm2) || oi.qr[0] <= A::c(p.hm2)) qr1_m = A::copysign(A::c(K::VMIN), ur_m);
+        R fo[4];
+        OsherTrace<R> tr;
+        osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo, &tr);
+        if (ra_) {
+            R f[4];
+            f[0] = fo[0];
+            f[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, ur_d);
+            f[2] = fo[2];
+            f[3] = fo[3];
+            if (write_flux) store_flux(m, ix.z, f);
+            store_terms<A>(m, ix.z, f, g.z, cs, sn);
+        }
+        if (rb_) {
+            if (!ra_ || same_bits(qr1_d, qr1_m)) {
+                R f[4];
+                f[0] = -fo[0];
+                f[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, ur_m);
+                f[2] = (!ra_ || same_bits(ql2_d, ql2_m)) ? fo[2] : osher_f2<A>(tr, ql2_m, oi.qr[2]);
+                f[3] = mirror_f3<A>(fo[3], A_.zbc, B_.zbc);
+                if (write_flux) store_flux(m, ix.w, f);
+                store_terms<A>(m, ix.w, f, g.z, -cs, -sn);
+            } else {
+                queue[atomicAdd(qn, 1)] = r;
+            }
+        }
+    }
+}
+
+// Flux of every record of one step.  Single mesh (SEG = false): records
+// [0, npairs) are mirror pairs and the rest single slots, one per thread.
+// Batch (SEG = true): CTA b takes the scenario and record range of fseg[b].
+template <class A, int VARIANT, int THREADS, int MINB, bool SEG>
+__global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k, int write_flux) {
     __shared__ int queue[THREADS];
     __shared__ int qn;
     if (threadIdx.x == 0) qn = 0;
-    cudaGridDependencySynchronize();
-    cudaTriggerProgrammaticLaunchCompletion();
-    const StepIndex si = step_index(m, k);
-    const StepParams p{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
+    int r;
+    bool valid, pair;
+    StepIndex si;
+    StepParams p;
+    if constexpr (SEG) {
+        const int4 d = m.fseg[blockIdx.x];   // constant tables: read before the dependency wait
+        const ScnParams sp = m.scn[d.x];
+        cudaGridDependencySynchronize();
+        cudaTriggerProgrammaticLaunchCompletion();
+        si = step_index(m, k, sp.per_day, sp.ndays);
+        p = StepParams{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
+        r = d.y + (int)threadIdx.x;
+        valid = (int)threadIdx.x < d.z;
+        pair = d.w != 0;
+    } else {
+        cudaGridDependencySynchronize();
+        cudaTriggerProgrammaticLaunchCompletion();
+        si = step_index(m, k, m.per_day, m.ndays);
+        p = StepParams{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
+        r = blockIdx.x * THREADS + threadIdx.x;
+        valid = r < m.nrecords;
+        pair = r < m.npairs;
+    }
     __syncthreads();
-    const int r = blockIdx.x * THREADS + threadIdx.x;
-    if (r < m.npairs) {
-        const int4 ix = m.rix[r];
-        const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
-        const CellStateA<A> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
-        const R cs = g.x, sn = g.y;
-        const R clA = A::sqrt(A::mul(A::c(9.81), A_.h));
-        auto nofetch = []() { return BoundaryInA<A>{}; };
-        SlotInA<A> ia, ib;
-        ia.own = A_; ia.nb = B_; ia.has_nb = true; ia.own_first = true; ia.code = CODE_ZERO;
-        ia.cosj = cs; ia.sinj = sn; ia.side = g.z;
-        ib.own = B_; ib.nb = A_; ib.has_nb = true; ib.own_first = false; ib.code = CODE_ZERO;
-        ib.cosj = -cs; ib.sinj = -sn; ib.side = ia.side;
-        // each side's branch chain; a side whose fluxes are final is written at once
-        int ra_, rb_;
-        {
-            SlotOut<R> oa;
-            ra_ = flux_chain<A, VARIANT>(ia, clA, p, nofetch, oa);   // 0 or 1 (direct)
-            if (!ra_) {
-                if (write_flux) store_flux(m, ix.z, oa.f);
-                store_terms<A>(m, ix.z, oa.f, g.z, cs, sn);
-            }
-        }
-        {
-            SlotOut<R> ob;
-            rb_ = flux_chain<A, VARIANT>(ib, R(0), p, nofetch, ob);  // 0 or 2 (mirrored)
-            if (!rb_) {
-                if (write_flux) store_flux(m, ix.w, ob.f);
-                store_terms<A>(m, ix.w, ob.f, g.z, -cs, -sn);
-            }
-        }
-        if (ra_ | rb_) {
-            // the two routes' inputs differ only in QL2, UR and so QR1 (osher_inputs)
-            OsherIn<R> oi = osher_inputs<A>(A_, B_, cs, sn, clA, ra_ == 0, p);
-            const R ql2_d = oi.ql[2], ur_d = oi.ur, qr1_d = oi.qr[1];
-            const R ql2_m = ra_ ? A::dot(A_.v, cs, -A_.u, sn, M_QL2M) : ql2_d;
-            const R ur_m = ra_ ? A::dot(B_.u, cs, B_.v, sn, M_UR1) : ur_d;
-            R qr1_m = A::mul(ur_m, oi.ratio);
-            if (oi.hcR <= A::c(p.hm2) || oi.qr[0] <= A::c(p.hm2)) qr1_m = A::copysign(A::c(K::VMIN), ur_m);
-            R fo[4];
-            OsherTrace<R> tr;
-            osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo, &tr);
-            if (ra_) {
-                R f[4];
-                f[0] = fo[0];
-                f[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, ur_d);
-                f[2] = fo[2];
-                f[3] = fo[3];
-                if (write_flux) store_flux(m, ix.z, f);
-                store_terms<A>(m, ix.z, f, g.z, cs, sn);
-            }
-            if (rb_) {
-                if (!ra_ || same_bits(qr1_d, qr1_m)) {
-                    R f[4];
-                    f[0] = -fo[0];
-                    f[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, ur_m);
-                    f[2] = (!ra_ || same_bits(ql2_d, ql2_m)) ? fo[2] : osher_f2<A>(tr, ql2_m, oi.qr[2]);
-                    f[3] = mirror_f3<A>(fo[3], A_.zbc, B_.zbc);
-                    if (write_flux) store_flux(m, ix.w, f);
-                    store_terms<A>(m, ix.w, f, g.z, -cs, -sn);
-                } else {
-                    queue[atomicAdd(&qn, 1)] = r;
-                }
-            }
-        }
-    } else if (r < m.nrecords) {
-        single_record<A, VARIANT>(m, r, si, p, write_flux);
+    if (valid) {
+        if (pair) pair_record<A, VARIANT>(m, r, si, p, write_flux, queue, &qn);
+        else single_record<A, VARIANT>(m, r, si, p, write_flux);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < qn; i += THREADS) pair_mirror<A>(m, queue[i], si, p, write_flux);
 }
 
-// Sums and update of every cell (UpdateCellKernel, functors.cu:717-784).  The
+// Sums and update of one cell (UpdateCellKernel, functors.cu:717-784).  The
 // zero-length fourth slot of a triangle is evaluated here without pow
 // (flux_slot's ZERO_LEN), exactly when fluxes are written out.
-template <class A, int VARIANT, int UMINB>
-__global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<A> m, int k, int write_flux) {
+template <class A, int VARIANT>
+__device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const StepIndex &si, const StepParams &p,
+                                           int write_flux) {
     using R = typename A::real;
-    cudaGridDependencySynchronize();
-    cudaTriggerProgrammaticLaunchCompletion();
-    const StepIndex si = step_index(m, k);
-    const StepParams p{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
     using L = typename A::level;
-    for (int c = blockIdx.x * UPDATE_THREADS + threadIdx.x; c < m.C; c += gridDim.x * UPDATE_THREADS) {
     const Vec4<R> raw = ld4(m.S[si.par] + 4 * (size_t)c);
     CellStateA<A> st;
     st.h = raw.x; st.u = raw.y; st.v = raw.z; st.zbc = m.zbc[c];
@@ -418,6 +456,27 @@ __global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<A
     else st4(m.S[np] + 4 * (size_t)c, o.h, o.u, o.v, o.z);
     m.W[c] = o.w;
     if (!(isfinite((double)o.h) && isfinite((double)o.u) && isfinite((double)o.v))) atomicOr(m.err, ERRBIT_NONFINITE);
+}
+
+// Every cell of one step.  Single mesh: a grid-stride loop over the cells.
+// Batch: CTA b takes the scenario and cell range of useg[b].
+template <class A, int VARIANT, int UMINB, bool SEG>
+__global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<A> m, int k, int write_flux) {
+    if constexpr (SEG) {
+        const int4 d = m.useg[blockIdx.x];
+        const ScnParams sp = m.scn[d.x];
+        cudaGridDependencySynchronize();
+        cudaTriggerProgrammaticLaunchCompletion();
+        const StepIndex si = step_index(m, k, sp.per_day, sp.ndays);
+        const StepParams p{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
+        if ((int)threadIdx.x < d.z) update_one<A, VARIANT>(m, d.y + (int)threadIdx.x, si, p, write_flux);
+    } else {
+        cudaGridDependencySynchronize();
+        cudaTriggerProgrammaticLaunchCompletion();
+        const StepIndex si = step_index(m, k, m.per_day, m.ndays);
+        const StepParams p{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
+        for (int c = blockIdx.x * UPDATE_THREADS + threadIdx.x; c < m.C; c += gridDim.x * UPDATE_THREADS)
+            update_one<A, VARIANT>(m, c, si, p, write_flux);
     }
 }
 
@@ -439,20 +498,21 @@ struct SplitCodec {
     }
 };
 
-// reference-order staging <-> device-order state (perm[new] = old)
+// Reference-order staging <-> device-order state of one scenario: cells
+// [cell0, cell0 + C) of the device state, perm[new] = old within the scenario.
 template <class A>
-__global__ void stage_in_kernel(DevMesh<A> m, const int32_t *__restrict__ perm, const double *__restrict__ stage) {
+__global__ void stage_in_kernel(DevMesh<A> m, int cell0, int C, double hm1, const int32_t *__restrict__ perm,
+                                const double *__restrict__ stage) {
     using R = typename A::real;
-    const int C = m.C;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C) return;
     const int o = perm[i];
-    R *d = m.S[(*m.step_ctr) & 1] + 4 * (size_t)i;
+    R *d = m.S[(*m.step_ctr) & 1] + 4 * ((size_t)cell0 + i);
     d[1] = (R)stage[(size_t)C + o];
     d[2] = (R)stage[2 * (size_t)C + o];
     if constexpr (is_split<A>::value) {
         float h, hlo;
-        SplitCodec::encode(stage[o], stage[3 * (size_t)C + o], m.zbc[i], (float)m.hm1, h, hlo);
+        SplitCodec::encode(stage[o], stage[3 * (size_t)C + o], m.zbc[cell0 + i], (float)hm1, h, hlo);
         d[0] = h; d[3] = hlo;
     } else {
         d[0] = (R)stage[o];
@@ -460,23 +520,23 @@ __global__ void stage_in_kernel(DevMesh<A> m, const int32_t *__restrict__ perm, 
     }
 }
 template <class A>
-__global__ void stage_out_kernel(DevMesh<A> m, const int32_t *__restrict__ perm, double *__restrict__ stage) {
+__global__ void stage_out_kernel(DevMesh<A> m, int cell0, int C, double hm1, const int32_t *__restrict__ perm,
+                                 double *__restrict__ stage) {
     using R = typename A::real;
-    const int C = m.C;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C) return;
     const int o = perm[i];
-    const R *d = m.S[(*m.step_ctr) & 1] + 4 * (size_t)i;
+    const R *d = m.S[(*m.step_ctr) & 1] + 4 * ((size_t)cell0 + i);
     stage[(size_t)C + o] = (double)d[1];
     stage[2 * (size_t)C + o] = (double)d[2];
     if constexpr (is_split<A>::value) {
-        stage[o] = SplitCodec::depth(d[0], d[3], (float)m.hm1, m.hm1);
-        stage[3 * (size_t)C + o] = SplitCodec::level(d[0], d[3], m.zbc[i]);
+        stage[o] = SplitCodec::depth(d[0], d[3], (float)hm1, hm1);
+        stage[3 * (size_t)C + o] = SplitCodec::level(d[0], d[3], m.zbc[cell0 + i]);
     } else {
         stage[o] = (double)d[0];
         stage[3 * (size_t)C + o] = (double)d[3];
     }
-    stage[4 * (size_t)C + o] = (double)m.W[i];
+    stage[4 * (size_t)C + o] = (double)m.W[cell0 + i];
 }
 
 // per-cell constants that the update needs, computed on the device with the
@@ -559,28 +619,49 @@ std::vector<int32_t> rcm_order(int C, const std::vector<int32_t> &nbr4) {
 // ---------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------
+namespace hb {
+// One scenario of a handle, on the host.
+struct Scenario {
+    int cells = 0, cell0 = 0;           // its cells: device indices [cell0, cell0 + cells)
+    int rec0 = 0, npairs = 0, nrecords = 0;   // its records [rec0, rec0 + nrecords), pairs first
+    int ndays = 0, steps_per_day = 0, per_day = 0, nhq = 0;
+    double dt = 0, hm1 = 0, hm2 = 0, jl = 0;
+    std::vector<int32_t> perm;          // perm[new] = old, within the scenario
+    std::vector<int32_t> inv;           // inv[old] = new
+    std::vector<double> klas_orig;      // [4 cells] reference order
+    std::vector<int32_t> slot_index;    // [4 cells] device slot -> record, -1 = zero-length slot
+    long long step_limit() const { return (long long)ndays * per_day; }
+};
+}  // namespace hb
+
 struct hb_handle {
     hb_options opt;
-    int C = 0, ndays = 0, nhq = 0, steps_per_day = 0, per_day = 0;
-    double dt = 0, hm1 = 0, hm2 = 0, jl = 0;
-    std::vector<int32_t> perm;       // perm[new] = old
-    std::vector<int32_t> inv;        // inv[old] = new
-    std::vector<double> klas_orig;   // [4C] reference order
+    int C = 0;                       // cells of every scenario
+    int max_cells = 0;               // cells of the largest scenario
+    std::vector<hb::Scenario> scn;
     std::vector<void *> allocs;
     hb::DevMesh<hb::F64Exact> m64{};
     hb::DevMesh<hb::F32Fast> m32{};
     hb::DevMesh<hb::F32Split> ms{};
     uint32_t *d_err = nullptr;
     long long *d_ctr = nullptr;
-    int32_t *d_perm = nullptr;       // perm on the device
-    std::vector<int32_t> slot_index; // [4C] device-order slot -> compact real slot, -1 = zero-length slot
-    int nslots = 0;
-    double *d_stage = nullptr;       // [5C] reference-order staging for hb_step_host
+    int32_t *d_perm = nullptr;       // scenario permutations, concatenated
+    double *d_stage = nullptr;       // [5 max_cells] reference-order staging
+    int4 *d_fseg[3] = {nullptr, nullptr, nullptr};   // flux segment tables for 64/128/256 threads
+    int nfseg[3] = {0, 0, 0};
+    int4 *d_useg = nullptr;
+    int nuseg = 0;
     long long steps_done = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int graph_steps = 0;
     int launch_config = 0;           // index into LAUNCH_CONFIGS
+    bool segmented() const { return scn.size() > 1; }
+    long long step_limit() const {
+        long long l = LLONG_MAX;
+        for (const auto &s : scn) l = std::min(l, s.step_limit());
+        return l;
+    }
     // f(mesh) on the device mesh of this handle's precision
     template <class F> int with_mesh(F &&f) {
         switch (opt.precision) {
@@ -589,9 +670,15 @@ struct hb_handle {
         default: return f(m64);
         }
     }
-    ~hb_handle() {
+    void drop_graph() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (graph) cudaGraphDestroy(graph);
+        graph_exec = nullptr;
+        graph = nullptr;
+        graph_steps = 0;
+    }
+    ~hb_handle() {
+        drop_graph();
         for (void *p : allocs) cudaFree(p);
     }
 };
@@ -624,35 +711,67 @@ int dev_alloc(hb_handle *h, T **dst, size_t count) {
 
 #define TRY(x) do { int st_ = (x); if (st_ != HB_OK) return st_; } while (0)
 
+// Host image of the device mesh of every scenario, concatenated.
 template <class A>
-int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<A> &m) {
+struct HostMesh {
     using R = typename A::real;
     using L = typename A::level;
-    const int C = h->C;
+    std::vector<L> zbc;
+    std::vector<R> fnc, area, side4;
+    std::vector<uint8_t> cmask;
+    std::vector<int4> rix;
+    std::vector<uint8_t> rmeta;
+    std::vector<R> rgeo;
+    std::vector<int32_t> bcell;               // global table row, -1 = none
+    // one entry per table row: the row's values for each interval of its scenario
+    std::vector<std::vector<R>> qt, dqt;
+    std::vector<std::vector<L>> zt, dzt;
+    std::vector<L> top;
+    std::vector<int32_t> nhq1;
+    std::vector<std::vector<L>> zw;
+    std::vector<std::vector<R>> qw;
+};
+
+// Validates one scenario's mesh and appends it (renumbered) to hm.
+template <class A>
+int append_scenario(const hb_mesh_desc *md, bool renumber, hb::Scenario &sc, HostMesh<A> &hm) {
+    using R = typename A::real;
+    using L = typename A::level;
+    if (md->cells <= 0 || md->ndays <= 0 || md->steps_per_day < 2 || md->nhq < 0)
+        return hb::set_error(HB_E_INVALID, "mesh: cells=%d ndays=%d steps_per_day=%d", md->cells, md->ndays,
+                             md->steps_per_day);
+    const double *need[] = {md->nac, md->klas, md->side, md->cosf, md->sinf, md->zbc, md->area, md->fnc,
+                            md->bfeat, md->qt, md->dqt, md->zt, md->dzt};
+    for (const double *p : need) if (!p) return hb::set_error(HB_E_INVALID, "mesh: missing array");
+    if (md->nhq > 0 && (!md->zw || !md->qw || !md->nhq1)) return hb::set_error(HB_E_INVALID, "mesh: missing rating tables");
+    const int C = md->cells;
     const size_t S = 4 * (size_t)C;
-    const auto &perm = h->perm;
-    const auto &inv = h->inv;
-    auto cellv = [&](const double *src) {
-        std::vector<R> v(C);
-        for (int i = 0; i < C; i++) v[i] = (R)src[perm[i]];
-        return v;
-    };
-    auto cell_levels = [&](const double *src) {
-        std::vector<L> v(C);
-        for (int i = 0; i < C; i++) v[i] = (L)src[perm[i]];
-        return v;
-    };
-    auto slotv = [&](const double *src) {
-        std::vector<R> v(S);
-        for (int i = 0; i < C; i++)
-            for (int j = 0; j < 4; j++) v[4 * (size_t)i + j] = (R)src[4 * (size_t)perm[i] + j];
-        return v;
-    };
-    m.C = C;
-    m.per_day = h->per_day;
-    m.ndays = h->ndays;
-    m.nhq = h->nhq;
-    m.hm1 = h->hm1; m.hm2 = h->hm2; m.jl = h->jl; m.dt = h->dt;
+    sc.cells = C;
+    sc.cell0 = (int)hm.zbc.size();
+    sc.ndays = md->ndays; sc.nhq = md->nhq;
+    sc.steps_per_day = md->steps_per_day; sc.per_day = md->steps_per_day - 1;
+    sc.dt = md->dt; sc.hm1 = md->hm1; sc.hm2 = md->hm2; sc.jl = md->jl;
+    // neighbour lists in input order, for the renumbering
+    std::vector<int32_t> nbr_old(S, -1);
+    for (size_t s = 0; s < S; s++) {
+        const int nc = (int)(md->nac[s] - 1.0);
+        if (nc != -1 && (nc < 0 || nc >= C)) return hb::set_error(HB_E_BADMESH, "NAC[%zu] = %g out of range", s, md->nac[s]);
+        nbr_old[s] = nc;
+    }
+    if (renumber) sc.perm = hb::rcm_order(C, nbr_old);
+    else { sc.perm.resize(C); std::iota(sc.perm.begin(), sc.perm.end(), 0); }
+    sc.inv.assign(C, -1);
+    for (int i = 0; i < C; i++) sc.inv[sc.perm[i]] = i;
+    sc.klas_orig.assign(md->klas, md->klas + S);
+    const auto &perm = sc.perm;
+    const auto &inv = sc.inv;
+    const int c0 = sc.cell0;
+    for (int i = 0; i < C; i++) {
+        hm.zbc.push_back((L)md->zbc[perm[i]]);
+        hm.fnc.push_back((R)md->fnc[perm[i]]);
+        hm.area.push_back((R)md->area[perm[i]]);
+        for (int j = 0; j < 4; j++) hm.side4.push_back((R)md->side[4 * (size_t)perm[i] + j]);
+    }
     // real slots: everything except a zero-length slot without neighbour and code 0
     std::vector<int32_t> nbr4(S, -1);
     std::vector<uint8_t> meta4(S, 0);
@@ -662,12 +781,10 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<A> &m) {
         const int old = perm[i];
         for (int j = 0; j < 4; j++) {
             const size_t so = 4 * (size_t)old + j, sn = 4 * (size_t)i + j;
-            const int nc_old = (int)(md->nac[so] - 1.0);
-            int8_t code = hb::klas_code(md->klas[so]);
+            const int nc_old = nbr_old[so];
+            const int8_t code = hb::klas_code(md->klas[so]);
             uint8_t mt = (uint8_t)code;
             if (nc_old != -1) {
-                if (nc_old < 0 || nc_old >= C)
-                    return hb::set_error(HB_E_BADMESH, "NAC of cell %d slot %d = %g out of range", old + 1, j, md->nac[so]);
                 nbr4[sn] = inv[nc_old];
                 mt |= hb::META_HAS_NB;
                 if (old < nc_old) mt |= hb::META_OWN_FIRST;
@@ -680,16 +797,23 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<A> &m) {
                 needs_table[i] = 1;
         }
     }
-    // records: exact mirror pairs first, then every other real slot
-    std::vector<uint8_t> cmask(C, 0);
-    for (int i = 0; i < C; i++)
+    for (int i = 0; i < C; i++) {
+        uint8_t cm = 0;
         for (int j = 0; j < 4; j++)
-            if (real4[4 * (size_t)i + j]) cmask[i] |= (uint8_t)(1u << j);
+            if (real4[4 * (size_t)i + j]) cm |= (uint8_t)(1u << j);
+        hm.cmask.push_back(cm);
+    }
+    // records: exact mirror pairs first, then every other real slot
+    sc.rec0 = (int)hm.rix.size();
     std::vector<char> paired(S, 0);
-    std::vector<int32_t> ra, rb, rsa, rsb;
-    std::vector<uint8_t> rmeta;
-    std::vector<R> rcos, rsin, rside;
     auto slot_of = [&](int i, int j) { return 4 * (size_t)perm[i] + j; };   // reference slot of device slot
+    auto push = [&](int a, int b, size_t sa, long long sb, uint8_t mt, size_t so) {
+        hm.rix.push_back(make_int4(c0 + a, b < 0 ? -1 : c0 + b, (int)(4 * (size_t)c0 + sa),
+                                   sb < 0 ? -1 : (int)(4 * (size_t)c0 + sb)));
+        hm.rmeta.push_back(mt);
+        hm.rgeo.push_back((R)md->cosf[so]); hm.rgeo.push_back((R)md->sinf[so]);
+        hm.rgeo.push_back((R)md->side[so]); hm.rgeo.push_back(R(0));
+    };
     for (int i = 0; i < C; i++) {
         for (int j = 0; j < 4; j++) {
             const size_t sn = 4 * (size_t)i + j;
@@ -707,80 +831,135 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<A> &m) {
                 md->sinf[ob] != -md->sinf[oa] || md->side[ob] != md->side[oa])
                 continue;
             paired[sn] = paired[sb] = 1;
-            ra.push_back(i); rb.push_back(nb); rsa.push_back((int32_t)sn); rsb.push_back((int32_t)sb);
-            rmeta.push_back(meta4[sn]);
-            rcos.push_back((R)md->cosf[oa]); rsin.push_back((R)md->sinf[oa]); rside.push_back((R)md->side[oa]);
+            push(i, nb, sn, (long long)sb, meta4[sn], oa);
         }
     }
-    m.npairs = (int)ra.size();
-    h->slot_index.assign(S, -1);
+    sc.npairs = (int)hm.rix.size() - sc.rec0;
+    sc.slot_index.assign(S, -1);
     for (int i = 0; i < C; i++) {
         for (int j = 0; j < 4; j++) {
             const size_t sn = 4 * (size_t)i + j;
             if (!real4[sn] || paired[sn]) continue;
-            h->slot_index[sn] = (int32_t)ra.size();
-            const size_t so = slot_of(i, j);
-            ra.push_back(i); rb.push_back(nbr4[sn]); rsa.push_back((int32_t)sn); rsb.push_back(-1);
-            rmeta.push_back(meta4[sn]);
-            rcos.push_back((R)md->cosf[so]); rsin.push_back((R)md->sinf[so]); rside.push_back((R)md->side[so]);
+            sc.slot_index[sn] = (int32_t)hm.rix.size();
+            push(i, nbr4[sn], sn, -1, meta4[sn], slot_of(i, j));
         }
     }
-    m.nrecords = (int)ra.size();
-    h->nslots = m.nrecords;
-    // compact boundary tables
-    std::vector<int32_t> bcell(C, -1);
-    std::vector<int> rows;
-    for (int i = 0; i < C; i++) if (needs_table[i]) { bcell[i] = (int32_t)rows.size(); rows.push_back(i); }
-    const int NB = (int)rows.size(), ND = h->ndays, NHQ = std::max(h->nhq, 0);
-    std::vector<R> bqt((size_t)ND * NB), bdqt((size_t)ND * NB), bqw((size_t)(NB + 1) * NHQ, R(0));
-    std::vector<L> bzt((size_t)ND * NB), bdzt((size_t)ND * NB), btop(NB), bzw((size_t)(NB + 1) * NHQ, L(0));
-    std::vector<int32_t> bnhq1(NB);
-    for (int r = 0; r < NB; r++) {
-        const int old = perm[rows[r]];
-        for (int d = 0; d < ND; d++) {
+    sc.nrecords = (int)hm.rix.size() - sc.rec0;
+    // boundary table rows of the cells that need them
+    const int NHQ = std::max(md->nhq, 0);
+    for (int i = 0; i < C; i++) {
+        if (!needs_table[i]) { hm.bcell.push_back(-1); continue; }
+        hm.bcell.push_back((int32_t)hm.top.size());
+        const int old = perm[i];
+        std::vector<R> q(md->ndays), dq(md->ndays), w(NHQ);
+        std::vector<L> z(md->ndays), dz(md->ndays), zw(NHQ);
+        for (int d = 0; d < md->ndays; d++) {
             const size_t t = (size_t)d * C + old;
-            bqt[(size_t)d * NB + r] = (R)md->qt[t]; bdqt[(size_t)d * NB + r] = (R)md->dqt[t];
-            bzt[(size_t)d * NB + r] = (L)md->zt[t]; bdzt[(size_t)d * NB + r] = (L)md->dzt[t];
+            q[d] = (R)md->qt[t]; dq[d] = (R)md->dqt[t]; z[d] = (L)md->zt[t]; dz[d] = (L)md->dzt[t];
         }
-        btop[r] = (L)md->bfeat[old];
-        bnhq1[r] = md->nhq1[old];
-        for (int q = 0; q < NHQ; q++) {
-            bzw[(size_t)r * NHQ + q] = (L)md->zw[(size_t)old * NHQ + q];
-            bqw[(size_t)r * NHQ + q] = (R)md->qw[(size_t)old * NHQ + q];
+        for (int k = 0; k < NHQ; k++) {
+            zw[k] = (L)md->zw[(size_t)old * NHQ + k];
+            w[k] = (R)md->qw[(size_t)old * NHQ + k];
+        }
+        hm.qt.push_back(q); hm.dqt.push_back(dq); hm.zt.push_back(z); hm.dzt.push_back(dz);
+        hm.top.push_back((L)md->bfeat[old]);
+        hm.nhq1.push_back(NHQ > 0 ? md->nhq1[old] : 0);
+        hm.zw.push_back(zw); hm.qw.push_back(w);
+    }
+    return HB_OK;
+}
+
+// Segment tables: CTAs of `threads` records (flux) or UPDATE_THREADS cells
+// (update), none straddling two scenarios or the pair/single boundary.
+std::vector<int4> flux_segments(const std::vector<hb::Scenario> &scn, int threads) {
+    std::vector<int4> seg;
+    for (int s = 0; s < (int)scn.size(); s++) {
+        const auto &sc = scn[s];
+        for (int b = 0; b < sc.npairs; b += threads)
+            seg.push_back(make_int4(s, sc.rec0 + b, std::min(threads, sc.npairs - b), 1));
+        const int ns = sc.nrecords - sc.npairs;
+        for (int b = 0; b < ns; b += threads)
+            seg.push_back(make_int4(s, sc.rec0 + sc.npairs + b, std::min(threads, ns - b), 0));
+    }
+    return seg;
+}
+std::vector<int4> update_segments(const std::vector<hb::Scenario> &scn) {
+    std::vector<int4> seg;
+    for (int s = 0; s < (int)scn.size(); s++)
+        for (int b = 0; b < scn[s].cells; b += hb::UPDATE_THREADS)
+            seg.push_back(make_int4(s, scn[s].cell0 + b, std::min(hb::UPDATE_THREADS, scn[s].cells - b), 0));
+    return seg;
+}
+
+int thread_slot(int threads) { return threads == 64 ? 0 : threads == 128 ? 1 : 2; }
+
+template <class A>
+int build_device_mesh(hb_handle *h, const hb_mesh_desc *mds, int n, hb::DevMesh<A> &m) {
+    using R = typename A::real;
+    using L = typename A::level;
+    HostMesh<A> hm;
+    h->scn.resize(n);
+    for (int s = 0; s < n; s++) {
+        const int st = append_scenario<A>(&mds[s], h->opt.renumber != 0, h->scn[s], hm);
+        if (st != HB_OK) return n > 1 ? hb::set_error(st, "scenario %d: %s", s, hb_last_error_string()) : st;
+    }
+    const int C = (int)hm.zbc.size();
+    h->C = C;
+    h->max_cells = 0;
+    for (const auto &sc : h->scn) h->max_cells = std::max(h->max_cells, sc.cells);
+    const hb::Scenario &s0 = h->scn[0];
+    m.C = C;
+    m.per_day = s0.per_day; m.ndays = s0.ndays;
+    m.hm1 = s0.hm1; m.hm2 = s0.hm2; m.jl = s0.jl; m.dt = s0.dt;
+    m.npairs = s0.npairs;                 // a single mesh's records: [0, npairs) pairs
+    m.nrecords = (int)hm.rix.size();
+    // boundary tables: [day][row] over the longest scenario; a scenario's rows
+    // repeat its last interval beyond its own tables (never read: step_index clamps)
+    const int NB = (int)hm.top.size();
+    int ND = 1, NHQ = 0;
+    for (const auto &sc : h->scn) { ND = std::max(ND, sc.ndays); NHQ = std::max(NHQ, sc.nhq); }
+    std::vector<R> bqt((size_t)ND * NB), bdqt((size_t)ND * NB), bqw((size_t)(NB + 1) * NHQ, R(0));
+    std::vector<L> bzt((size_t)ND * NB), bdzt((size_t)ND * NB), bzw((size_t)(NB + 1) * NHQ, L(0));
+    for (int r = 0; r < NB; r++) {
+        const int nd = (int)hm.qt[r].size();
+        for (int d = 0; d < ND; d++) {
+            const int dd = std::min(d, nd - 1);
+            bqt[(size_t)d * NB + r] = hm.qt[r][dd]; bdqt[(size_t)d * NB + r] = hm.dqt[r][dd];
+            bzt[(size_t)d * NB + r] = hm.zt[r][dd]; bdzt[(size_t)d * NB + r] = hm.dzt[r][dd];
+        }
+        for (size_t k = 0; k < hm.zw[r].size(); k++) {
+            bzw[(size_t)r * NHQ + k] = hm.zw[r][k];
+            bqw[(size_t)r * NHQ + k] = hm.qw[r][k];
         }
     }
     m.nb = NB;
+    m.nhq = NHQ;
     int32_t *ip;
     uint8_t *up;
     R *rp;
     L *lp;
-    TRY(dev_upload(h, &lp, cell_levels(md->zbc))); m.zbc = lp;
-    TRY(dev_upload(h, &rp, cellv(md->fnc))); m.fnc = rp;
+    TRY(dev_upload(h, &lp, hm.zbc)); m.zbc = lp;
+    TRY(dev_upload(h, &rp, hm.fnc)); m.fnc = rp;
     R *area_d = nullptr, *side_d = nullptr;
-    TRY(dev_upload(h, &area_d, cellv(md->area)));
-    TRY(dev_upload(h, &side_d, slotv(md->side)));   // [4C], for the per-cell setup only
-    TRY(dev_upload(h, &up, cmask)); m.cmask = up;
+    TRY(dev_upload(h, &area_d, hm.area));
+    TRY(dev_upload(h, &side_d, hm.side4));   // [4C], for the per-cell setup only
+    TRY(dev_upload(h, &up, hm.cmask)); m.cmask = up;
     {
-        std::vector<int4> rix(ra.size());
-        std::vector<R> rgeo(4 * ra.size(), R(0));
-        for (size_t r = 0; r < ra.size(); r++) {
-            rix[r] = make_int4(ra[r], rb[r], rsa[r], rsb[r]);
-            rgeo[4 * r] = rcos[r]; rgeo[4 * r + 1] = rsin[r]; rgeo[4 * r + 2] = rside[r];
-        }
-        int4 *ixp; R *gp;
-        TRY(dev_upload(h, &ixp, rix)); m.rix = ixp;
-        TRY(dev_upload(h, &gp, rgeo)); m.rgeo = gp;
+        int4 *ixp;
+        TRY(dev_upload(h, &ixp, hm.rix)); m.rix = ixp;
+        TRY(dev_upload(h, &rp, hm.rgeo)); m.rgeo = rp;
     }
-    TRY(dev_upload(h, &up, rmeta)); m.rmeta = up;
-    TRY(dev_upload(h, &ip, bcell)); m.bcell = ip;
+    TRY(dev_upload(h, &up, hm.rmeta)); m.rmeta = up;
+    TRY(dev_upload(h, &ip, hm.bcell)); m.bcell = ip;
     TRY(dev_upload(h, &rp, bqt)); m.bqt = rp;
     TRY(dev_upload(h, &rp, bdqt)); m.bdqt = rp;
     TRY(dev_upload(h, &lp, bzt)); m.bzt = lp;
     TRY(dev_upload(h, &lp, bdzt)); m.bdzt = lp;
-    TRY(dev_upload(h, &lp, btop)); m.btop = lp;
-    TRY(dev_upload(h, &ip, bnhq1)); m.bnhq1 = ip;
+    TRY(dev_upload(h, &lp, hm.top)); m.btop = lp;
+    TRY(dev_upload(h, &ip, hm.nhq1)); m.bnhq1 = ip;
     TRY(dev_upload(h, &lp, bzw)); m.bzw = lp;
     TRY(dev_upload(h, &rp, bqw)); m.bqw = rp;
+    const size_t S = 4 * (size_t)C;
     for (int b = 0; b < 2; b++) TRY(dev_alloc(h, &m.S[b], 4 * (size_t)C));
     TRY(dev_alloc(h, &m.slotw, 16 * (size_t)C));
     TRY(dev_alloc(h, &m.W, C));
@@ -789,37 +968,68 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *md, hb::DevMesh<A> &m) {
     R *dta = nullptr, *sidex = nullptr;
     TRY(dev_alloc(h, &dta, C));
     TRY(dev_alloc(h, &sidex, C));
-    const int blocks = (C + 255) / 256;
-    if (h->opt.variant == HB_VARIANT_F) hb::setup_cells_kernel<A, 1><<<blocks, 256>>>(C, h->dt, area_d, side_d, dta, sidex);
-    else hb::setup_cells_kernel<A, 0><<<blocks, 256>>>(C, h->dt, area_d, side_d, dta, sidex);
-    HB_CUDA_RET(cudaGetLastError());
+    for (const auto &sc : h->scn) {
+        const int blocks = (sc.cells + 255) / 256;
+        const size_t c0 = sc.cell0;
+        if (h->opt.variant == HB_VARIANT_F)
+            hb::setup_cells_kernel<A, 1><<<blocks, 256>>>(sc.cells, sc.dt, area_d + c0, side_d + 4 * c0, dta + c0, sidex + c0);
+        else
+            hb::setup_cells_kernel<A, 0><<<blocks, 256>>>(sc.cells, sc.dt, area_d + c0, side_d + 4 * c0, dta + c0, sidex + c0);
+        HB_CUDA_RET(cudaGetLastError());
+    }
     HB_CUDA_RET(cudaDeviceSynchronize());
     m.dta = dta;
     m.sidex = sidex;
     m.err = h->d_err;
     m.step_ctr = h->d_ctr;
+    // scenario table and segment tables
+    std::vector<hb::ScnParams> sp;
+    for (const auto &sc : h->scn)
+        sp.push_back(hb::ScnParams{sc.hm1, sc.hm2, sc.jl, sc.dt, sc.per_day, sc.ndays, sc.cell0, sc.cells});
+    hb::ScnParams *spd;
+    TRY(dev_upload(h, &spd, sp)); m.scn = spd;
+    m.nscen = n;
+    const int tsizes[3] = {64, 128, 256};
+    for (int t = 0; t < 3; t++) {
+        const std::vector<int4> seg = flux_segments(h->scn, tsizes[t]);
+        h->nfseg[t] = (int)seg.size();
+        TRY(dev_upload(h, &h->d_fseg[t], seg));
+    }
+    {
+        const std::vector<int4> seg = update_segments(h->scn);
+        h->nuseg = (int)seg.size();
+        TRY(dev_upload(h, &h->d_useg, seg));
+    }
+    m.fseg = h->d_fseg[1];
+    m.useg = h->d_useg;
+    // scenario permutations on the device, for the staging kernels
+    std::vector<int32_t> perms;
+    for (const auto &sc : h->scn) perms.insert(perms.end(), sc.perm.begin(), sc.perm.end());
+    TRY(dev_upload(h, &h->d_perm, perms));
+    TRY(dev_alloc(h, &h->d_stage, 5 * (size_t)h->max_cells));
     return HB_OK;
 }
 
-template <class A, int VARIANT>
-int launch_steps(hb_handle *h, hb::DevMesh<A> &m, int n, cudaStream_t st) {
+template <class A, int VARIANT, bool SEG>
+int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     // Programmatic dependent launch: each kernel may start while its predecessor
     // drains and waits in cudaGridDependencySynchronize for its results.
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cudaLaunchConfig_t cfg_u{};
-    int nsm = 0, per_sm = 0;
-    HB_CUDA_RET(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->opt.device));
-    (void)per_sm;
-    cfg_u.gridDim = dim3((unsigned)std::max(1, (h->C + hb::UPDATE_THREADS - 1) / hb::UPDATE_THREADS));
+    cfg_u.gridDim = SEG ? dim3((unsigned)std::max(1, h->nuseg))
+                        : dim3((unsigned)std::max(1, (h->C + hb::UPDATE_THREADS - 1) / hb::UPDATE_THREADS));
     cfg_u.blockDim = dim3(hb::UPDATE_THREADS);
     cfg_u.stream = st;
     cfg_u.attrs = attr;
     cfg_u.numAttrs = 1;
     auto go = [&](auto flux, int threads, auto update) -> int {
         cudaLaunchConfig_t cfg_f = cfg_u;
-        cfg_f.gridDim = dim3((unsigned)std::max(1, (m.nrecords + threads - 1) / threads));
+        const int ts = thread_slot(threads);
+        m.fseg = h->d_fseg[ts];
+        cfg_f.gridDim = SEG ? dim3((unsigned)std::max(1, h->nfseg[ts]))
+                            : dim3((unsigned)std::max(1, (m.nrecords + threads - 1) / threads));
         cfg_f.blockDim = dim3(threads);
         for (int k = 0; k < n; k++) {
             HB_CUDA_RET(cudaLaunchKernelEx(&cfg_f, flux, m, k, (int)(k == n - 1)));
@@ -830,14 +1040,14 @@ int launch_steps(hb_handle *h, hb::DevMesh<A> &m, int n, cudaStream_t st) {
     int rc;
     using namespace hb;
     switch (h->launch_config) {
-    case 0: rc = go(flux_kernel<A, VARIANT, 128, 6>, 128, update_kernel<A, VARIANT, 6>); break;
-    case 1: rc = go(flux_kernel<A, VARIANT, 128, 6>, 128, update_kernel<A, VARIANT, 8>); break;
-    case 2: rc = go(flux_kernel<A, VARIANT, 128, 8>, 128, update_kernel<A, VARIANT, 8>); break;
-    case 3: rc = go(flux_kernel<A, VARIANT, 256, 3>, 256, update_kernel<A, VARIANT, 6>); break;
-    case 4: rc = go(flux_kernel<A, VARIANT, 256, 4>, 256, update_kernel<A, VARIANT, 8>); break;
-    case 5: rc = go(flux_kernel<A, VARIANT, 128, 4>, 128, update_kernel<A, VARIANT, 6>); break;
-    case 6: rc = go(flux_kernel<A, VARIANT, 256, 2>, 256, update_kernel<A, VARIANT, 6>); break;
-    default: rc = go(flux_kernel<A, VARIANT, 64, 12>, 64, update_kernel<A, VARIANT, 8>); break;
+    case 0: rc = go(flux_kernel<A, VARIANT, 128, 6, SEG>, 128, update_kernel<A, VARIANT, 6, SEG>); break;
+    case 1: rc = go(flux_kernel<A, VARIANT, 128, 6, SEG>, 128, update_kernel<A, VARIANT, 8, SEG>); break;
+    case 2: rc = go(flux_kernel<A, VARIANT, 128, 8, SEG>, 128, update_kernel<A, VARIANT, 8, SEG>); break;
+    case 3: rc = go(flux_kernel<A, VARIANT, 256, 3, SEG>, 256, update_kernel<A, VARIANT, 6, SEG>); break;
+    case 4: rc = go(flux_kernel<A, VARIANT, 256, 4, SEG>, 256, update_kernel<A, VARIANT, 8, SEG>); break;
+    case 5: rc = go(flux_kernel<A, VARIANT, 128, 4, SEG>, 128, update_kernel<A, VARIANT, 6, SEG>); break;
+    case 6: rc = go(flux_kernel<A, VARIANT, 256, 2, SEG>, 256, update_kernel<A, VARIANT, 6, SEG>); break;
+    default: rc = go(flux_kernel<A, VARIANT, 64, 12, SEG>, 64, update_kernel<A, VARIANT, 8, SEG>); break;
     }
     if (rc != HB_OK) return rc;
     hb::tick_kernel<<<1, 1, 0, st>>>(h->d_ctr, n);
@@ -848,17 +1058,26 @@ int launch_steps(hb_handle *h, hb::DevMesh<A> &m, int n, cudaStream_t st) {
 int enqueue_steps(hb_handle *h, int n, cudaStream_t st) {
     if (n <= 0) return HB_OK;
     const bool f = h->opt.variant == HB_VARIANT_F;
+    const bool seg = h->segmented();
     return h->with_mesh([&](auto &m) {
         using A = typename std::remove_reference<decltype(m)>::type::Policy;
-        return f ? launch_steps<A, 1>(h, m, n, st) : launch_steps<A, 0>(h, m, n, st);
+        if (seg) return f ? launch_steps_t<A, 1, true>(h, m, n, st) : launch_steps_t<A, 0, true>(h, m, n, st);
+        return f ? launch_steps_t<A, 1, false>(h, m, n, st) : launch_steps_t<A, 0, false>(h, m, n, st);
     });
 }
 
 int check_range(hb_handle *h, long long n) {
-    const long long limit = (long long)h->ndays * h->per_day;
+    const long long limit = h->step_limit();
     if (h->steps_done + n > limit)
-        return hb::set_error(HB_E_INVALID, "step %lld..%lld beyond the boundary tables (%d intervals of %d steps)",
-                             h->steps_done, h->steps_done + n, h->ndays, h->per_day);
+        return hb::set_error(HB_E_INVALID, "step %lld..%lld beyond the boundary tables (%lld steps)", h->steps_done,
+                             h->steps_done + n, limit);
+    return HB_OK;
+}
+
+int check_scenario(hb_handle *h, int s) {
+    if (!h) return hb::set_error(HB_E_INVALID, "null handle");
+    if (s < 0 || s >= (int)h->scn.size())
+        return hb::set_error(HB_E_INVALID, "scenario %d outside 0..%d", s, (int)h->scn.size() - 1);
     return HB_OK;
 }
 
@@ -872,58 +1091,36 @@ extern "C" int hb_tile_configs(int32_t *threads, int32_t *min_blocks, int32_t ca
     return hb::N_LAUNCH_CONFIGS;
 }
 
-extern "C" int hb_create(const hb_mesh_desc *md, const hb_options *opt_in, hb_handle **out) {
-    if (!md || !out) return hb::set_error(HB_E_INVALID, "hb_create: null argument");
+extern "C" int hb_create_batch(const hb_mesh_desc *meshes, int32_t n, const hb_options *opt_in, hb_handle **out) {
+    if (!meshes || !out || n <= 0) return hb::set_error(HB_E_INVALID, "hb_create_batch: bad argument");
     *out = nullptr;
     hb_options opt;
     if (opt_in) opt = *opt_in; else hb_options_default(&opt);
     if (opt.precision != HB_FP64 && opt.precision != HB_FP32 && opt.precision != HB_SPLIT)
         return hb::set_error(HB_E_INVALID, "hb_create: precision %d not available on this path", opt.precision);
-    if (md->cells <= 0 || md->ndays <= 0 || md->steps_per_day < 2 || md->nhq < 0)
-        return hb::set_error(HB_E_INVALID, "hb_create: cells=%d ndays=%d steps_per_day=%d", md->cells, md->ndays,
-                             md->steps_per_day);
-    if (md->cells > (1 << 29)) return hb::set_error(HB_E_TOO_LARGE, "hb_create: %d cells", md->cells);
-    const double *need[] = {md->nac, md->klas, md->side, md->cosf, md->sinf, md->zbc, md->area, md->fnc,
-                            md->bfeat, md->qt, md->dqt, md->zt, md->dzt};
-    for (const double *p : need) if (!p) return hb::set_error(HB_E_INVALID, "hb_create: missing mesh array");
-    if (md->nhq > 0 && (!md->zw || !md->qw || !md->nhq1)) return hb::set_error(HB_E_INVALID, "hb_create: missing rating tables");
+    if (opt.tile_config < 0 || opt.tile_config > hb::N_LAUNCH_CONFIGS)
+        return hb::set_error(HB_E_INVALID, "hb_create: tile_config %d outside 0..%d", opt.tile_config, hb::N_LAUNCH_CONFIGS);
+    long long total = 0;
+    for (int s = 0; s < n; s++) total += std::max(meshes[s].cells, 0);
+    if (total > (1 << 29)) return hb::set_error(HB_E_TOO_LARGE, "hb_create: %lld cells", total);
     HB_CUDA_RET(cudaSetDevice(opt.device));
     auto h = new hb_handle();
     h->opt = opt;
-    h->C = md->cells; h->ndays = md->ndays; h->nhq = md->nhq;
-    h->steps_per_day = md->steps_per_day; h->per_day = md->steps_per_day - 1;
-    h->dt = md->dt; h->hm1 = md->hm1; h->hm2 = md->hm2; h->jl = md->jl;
-    if (opt.tile_config < 0 || opt.tile_config > hb::N_LAUNCH_CONFIGS) {
-        delete h;
-        return hb::set_error(HB_E_INVALID, "hb_create: tile_config %d outside 0..%d", opt.tile_config, hb::N_LAUNCH_CONFIGS);
-    }
     h->launch_config = opt.tile_config == 0 ? hb::DEFAULT_LAUNCH_CONFIG : opt.tile_config - 1;
-    const int C = h->C;
-    // neighbour lists in input order, for the renumbering
-    std::vector<int32_t> nbr_old(4 * (size_t)C, -1);
-    for (size_t s = 0; s < 4 * (size_t)C; s++) {
-        int nc = (int)(md->nac[s] - 1.0);
-        if (nc != -1 && (nc < 0 || nc >= C)) {
-            delete h;
-            return hb::set_error(HB_E_BADMESH, "NAC[%zu] = %g out of range", s, md->nac[s]);
-        }
-        nbr_old[s] = nc;
-    }
-    if (opt.renumber) h->perm = hb::rcm_order(C, nbr_old);
-    else { h->perm.resize(C); std::iota(h->perm.begin(), h->perm.end(), 0); }
-    h->inv.assign(C, -1);
-    for (int i = 0; i < C; i++) h->inv[h->perm[i]] = i;
-    h->klas_orig.assign(md->klas, md->klas + 4 * (size_t)C);
     int st;
-    if ((st = dev_alloc(h, &h->d_err, 1)) != HB_OK || (st = dev_alloc(h, &h->d_ctr, 1)) != HB_OK ||
-        (st = dev_upload(h, &h->d_perm, h->perm)) != HB_OK || (st = dev_alloc(h, &h->d_stage, 5 * (size_t)C)) != HB_OK) {
+    if ((st = dev_alloc(h, &h->d_err, 1)) != HB_OK || (st = dev_alloc(h, &h->d_ctr, 1)) != HB_OK) {
         delete h;
         return st;
     }
-    st = h->with_mesh([&](auto &m) { return build_device_mesh(h, md, m); });
+    st = h->with_mesh([&](auto &m) { return build_device_mesh(h, meshes, n, m); });
     if (st != HB_OK) { delete h; return st; }
     *out = h;
     return HB_OK;
+}
+
+extern "C" int hb_create(const hb_mesh_desc *md, const hb_options *opt_in, hb_handle **out) {
+    if (!md || !out) return hb::set_error(HB_E_INVALID, "hb_create: null argument");
+    return hb_create_batch(md, 1, opt_in, out);
 }
 
 extern "C" int hb_destroy(hb_handle *h) {
@@ -931,45 +1128,61 @@ extern "C" int hb_destroy(hb_handle *h) {
     return HB_OK;
 }
 
+extern "C" int hb_batch_size(hb_handle *h, int32_t *n) {
+    if (!h || !n) return hb::set_error(HB_E_INVALID, "null argument");
+    *n = (int32_t)h->scn.size();
+    return HB_OK;
+}
+
+extern "C" int hb_scenario_cells(hb_handle *h, int32_t s, int32_t *cells, int32_t *first) {
+    TRY(check_scenario(h, s));
+    if (cells) *cells = h->scn[s].cells;
+    if (first) *first = h->scn[s].cell0;
+    return HB_OK;
+}
+
 namespace {
 // State in and out go through the reference-order staging buffer and the
 // staging kernels, which hold each precision's conversion (SplitCodec).
 template <class A>
-int set_state_t(hb_handle *h, hb::DevMesh<A> &m, const double *H, const double *U, const double *V, const double *Z,
-                const double *W) {
+int set_state_t(hb_handle *h, int s, hb::DevMesh<A> &m, const double *H, const double *U, const double *V,
+                const double *Z, const double *W) {
     using R = typename A::real;
-    const int C = h->C;
+    const hb::Scenario &sc = h->scn[s];
+    const int C = sc.cells;
     const double *src[4] = {H, U, V, Z};
     for (int k = 0; k < 4; k++)
         if (!src[k]) return hb::set_error(HB_E_INVALID, "hb_set_state: missing array");
     HB_CUDA_RET(cudaDeviceSynchronize());
     for (int k = 0; k < 4; k++)
         HB_CUDA_RET(cudaMemcpy(h->d_stage + (size_t)k * C, src[k], C * sizeof(double), cudaMemcpyHostToDevice));
-    hb::stage_in_kernel<A><<<(C + 255) / 256, 256>>>(m, h->d_perm, h->d_stage);
+    hb::stage_in_kernel<A><<<(C + 255) / 256, 256>>>(m, sc.cell0, C, sc.hm1, h->d_perm + sc.cell0, h->d_stage);
     HB_CUDA_RET(cudaGetLastError());
     if (W) {
         std::vector<R> w(C);
-        for (int i = 0; i < C; i++) w[i] = (R)W[h->perm[i]];
-        HB_CUDA_RET(cudaMemcpy(m.W, w.data(), C * sizeof(R), cudaMemcpyHostToDevice));
+        for (int i = 0; i < C; i++) w[i] = (R)W[sc.perm[i]];
+        HB_CUDA_RET(cudaMemcpy(m.W + sc.cell0, w.data(), C * sizeof(R), cudaMemcpyHostToDevice));
     }
     HB_CUDA_RET(cudaDeviceSynchronize());
     return HB_OK;
 }
 template <class A>
-int get_state_t(hb_handle *h, hb::DevMesh<A> &m, double *H, double *U, double *V, double *Z, double *W) {
-    const int C = h->C;
+int get_state_t(hb_handle *h, int s, hb::DevMesh<A> &m, double *H, double *U, double *V, double *Z, double *W) {
+    const hb::Scenario &sc = h->scn[s];
+    const int C = sc.cells;
     double *dst[5] = {H, U, V, Z, W};
     HB_CUDA_RET(cudaDeviceSynchronize());
-    hb::stage_out_kernel<A><<<(C + 255) / 256, 256>>>(m, h->d_perm, h->d_stage);
+    hb::stage_out_kernel<A><<<(C + 255) / 256, 256>>>(m, sc.cell0, C, sc.hm1, h->d_perm + sc.cell0, h->d_stage);
     HB_CUDA_RET(cudaGetLastError());
     for (int k = 0; k < 5; k++)
         if (dst[k]) HB_CUDA_RET(cudaMemcpy(dst[k], h->d_stage + (size_t)k * C, C * sizeof(double), cudaMemcpyDeviceToHost));
     return HB_OK;
 }
 template <class A>
-int get_flux_t(hb_handle *h, hb::DevMesh<A> &m, double *F0, double *F1, double *F2, double *F3) {
+int get_flux_t(hb_handle *h, int s, hb::DevMesh<A> &m, double *F0, double *F1, double *F2, double *F3) {
     using R = typename A::real;
-    const int C = h->C;
+    const hb::Scenario &sc = h->scn[s];
+    const int C = sc.cells;
     const size_t S = 4 * (size_t)C;
     std::vector<R> buf(S);
     double *dst[4] = {F0, F1, F2, F3};
@@ -977,25 +1190,25 @@ int get_flux_t(hb_handle *h, hb::DevMesh<A> &m, double *F0, double *F1, double *
     HB_CUDA_RET(cudaDeviceSynchronize());
     for (int k = 0; k < 4; k++) {
         if (!dst[k]) continue;
-        HB_CUDA_RET(cudaMemcpy(buf.data(), src[k], S * sizeof(R), cudaMemcpyDeviceToHost));
+        HB_CUDA_RET(cudaMemcpy(buf.data(), src[k] + 4 * (size_t)sc.cell0, S * sizeof(R), cudaMemcpyDeviceToHost));
         for (int i = 0; i < C; i++)
-            for (int j = 0; j < 4; j++) dst[k][4 * (size_t)h->perm[i] + j] = (double)buf[4 * (size_t)i + j];
+            for (int j = 0; j < 4; j++) dst[k][4 * (size_t)sc.perm[i] + j] = (double)buf[4 * (size_t)i + j];
     }
     return HB_OK;
 }
 template <class A>
-int get_klas_t(hb_handle *h, hb::DevMesh<A> &m, double *klas) {
-    const int C = h->C;
-    const size_t S = 4 * (size_t)C;
-    std::vector<uint8_t> meta(std::max(h->nslots, 1));
+int get_klas_t(hb_handle *h, int s, hb::DevMesh<A> &m, double *klas) {
+    const hb::Scenario &sc = h->scn[s];
+    const int C = sc.cells;
+    std::vector<uint8_t> meta(std::max(sc.nrecords, 1));
     HB_CUDA_RET(cudaDeviceSynchronize());
-    HB_CUDA_RET(cudaMemcpy(meta.data(), m.rmeta, h->nslots, cudaMemcpyDeviceToHost));
+    HB_CUDA_RET(cudaMemcpy(meta.data(), m.rmeta + sc.rec0, sc.nrecords, cudaMemcpyDeviceToHost));
     for (int i = 0; i < C; i++)
         for (int j = 0; j < 4; j++) {
-            const size_t so = 4 * (size_t)h->perm[i] + j;
-            const int ci = h->slot_index[4 * (size_t)i + j];
-            const int code = ci < 0 ? hb::CODE_ZERO : (meta[ci] & hb::META_CODE);
-            double k = h->klas_orig[so];
+            const size_t so = 4 * (size_t)sc.perm[i] + j;
+            const int ci = sc.slot_index[4 * (size_t)i + j];
+            const int code = ci < 0 ? hb::CODE_ZERO : (meta[ci - sc.rec0] & hb::META_CODE);
+            double k = sc.klas_orig[so];
             if (hb::klas_code(k) == hb::CODE_K7 && code == hb::CODE_ZERO) k = 0.0;   // breached (functors.cu:242)
             klas[so] = k;
         }
@@ -1003,21 +1216,35 @@ int get_klas_t(hb_handle *h, hb::DevMesh<A> &m, double *klas) {
 }
 }  // namespace
 
+extern "C" int hb_set_state_at(hb_handle *h, int32_t s, const double *H, const double *U, const double *V,
+                               const double *Z, const double *W) {
+    TRY(check_scenario(h, s));
+    return h->with_mesh([&](auto &m) { return set_state_t(h, s, m, H, U, V, Z, W); });
+}
+extern "C" int hb_get_state_at(hb_handle *h, int32_t s, double *H, double *U, double *V, double *Z, double *W) {
+    TRY(check_scenario(h, s));
+    return h->with_mesh([&](auto &m) { return get_state_t(h, s, m, H, U, V, Z, W); });
+}
+extern "C" int hb_get_flux_at(hb_handle *h, int32_t s, double *F0, double *F1, double *F2, double *F3) {
+    TRY(check_scenario(h, s));
+    return h->with_mesh([&](auto &m) { return get_flux_t(h, s, m, F0, F1, F2, F3); });
+}
+extern "C" int hb_get_klas_at(hb_handle *h, int32_t s, double *klas) {
+    TRY(check_scenario(h, s));
+    if (!klas) return hb::set_error(HB_E_INVALID, "null argument");
+    return h->with_mesh([&](auto &m) { return get_klas_t(h, s, m, klas); });
+}
 extern "C" int hb_set_state(hb_handle *h, const double *H, const double *U, const double *V, const double *Z, const double *W) {
-    if (!h) return hb::set_error(HB_E_INVALID, "null handle");
-    return h->with_mesh([&](auto &m) { return set_state_t(h, m, H, U, V, Z, W); });
+    return hb_set_state_at(h, 0, H, U, V, Z, W);
 }
 extern "C" int hb_get_state(hb_handle *h, double *H, double *U, double *V, double *Z, double *W) {
-    if (!h) return hb::set_error(HB_E_INVALID, "null handle");
-    return h->with_mesh([&](auto &m) { return get_state_t(h, m, H, U, V, Z, W); });
+    return hb_get_state_at(h, 0, H, U, V, Z, W);
 }
 extern "C" int hb_get_flux(hb_handle *h, double *F0, double *F1, double *F2, double *F3) {
-    if (!h) return hb::set_error(HB_E_INVALID, "null handle");
-    return h->with_mesh([&](auto &m) { return get_flux_t(h, m, F0, F1, F2, F3); });
+    return hb_get_flux_at(h, 0, F0, F1, F2, F3);
 }
 extern "C" int hb_get_klas(hb_handle *h, double *klas) {
-    if (!h || !klas) return hb::set_error(HB_E_INVALID, "null argument");
-    return h->with_mesh([&](auto &m) { return get_klas_t(h, m, klas); });
+    return hb_get_klas_at(h, 0, klas);
 }
 
 extern "C" int hb_step(hb_handle *h, int32_t nsteps, void *stream) {
@@ -1032,15 +1259,16 @@ namespace {
 template <class A>
 int step_host_t(hb_handle *h, hb::DevMesh<A> &m, double *H, double *U, double *V, double *Z, double *W, int n,
                 cudaStream_t st) {
-    const int C = h->C;
+    const hb::Scenario &sc = h->scn[0];
+    const int C = sc.cells;
     const size_t b = (size_t)C * sizeof(double);
     double *io[5] = {H, U, V, Z, W};
     for (int k = 0; k < 4; k++) HB_CUDA_RET(cudaMemcpyAsync(h->d_stage + (size_t)k * C, io[k], b, cudaMemcpyHostToDevice, st));
     const int blocks = (C + 255) / 256;
-    hb::stage_in_kernel<A><<<blocks, 256, 0, st>>>(m, h->d_perm, h->d_stage);
+    hb::stage_in_kernel<A><<<blocks, 256, 0, st>>>(m, 0, C, sc.hm1, h->d_perm, h->d_stage);
     HB_CUDA_RET(cudaGetLastError());
     TRY(enqueue_steps(h, n, st));
-    hb::stage_out_kernel<A><<<blocks, 256, 0, st>>>(m, h->d_perm, h->d_stage);
+    hb::stage_out_kernel<A><<<blocks, 256, 0, st>>>(m, 0, C, sc.hm1, h->d_perm, h->d_stage);
     HB_CUDA_RET(cudaGetLastError());
     for (int k = 0; k < 5; k++)
         if (io[k]) HB_CUDA_RET(cudaMemcpyAsync(io[k], h->d_stage + (size_t)k * C, b, cudaMemcpyDeviceToHost, st));
@@ -1051,6 +1279,7 @@ int step_host_t(hb_handle *h, hb::DevMesh<A> &m, double *H, double *U, double *V
 extern "C" int hb_step_host(hb_handle *h, double *H, double *U, double *V, double *Z, double *W, int32_t nsteps,
                             void *stream) {
     if (!h || !H || !U || !V || !Z || nsteps < 0) return hb::set_error(HB_E_INVALID, "hb_step_host: bad argument");
+    if (h->segmented()) return hb::set_error(HB_E_INVALID, "hb_step_host: not available on a batch handle");
     TRY(check_range(h, nsteps));
     cudaStream_t st = (cudaStream_t)stream;
     int r = h->with_mesh([&](auto &m) { return step_host_t(h, m, H, U, V, Z, W, nsteps, st); });
@@ -1077,9 +1306,10 @@ extern "C" int hb_device_errors(hb_handle *h, uint32_t *bits) {
 
 extern "C" int hb_position(hb_handle *h, int64_t *steps_done, int32_t *kt, int32_t *jt) {
     if (!h) return hb::set_error(HB_E_INVALID, "null handle");
+    const int per_day = h->scn[0].per_day;
     if (steps_done) *steps_done = h->steps_done;
-    if (kt) *kt = 1 + (int)(h->steps_done % h->per_day);
-    if (jt) *jt = (int)(h->steps_done / h->per_day);
+    if (kt) *kt = 1 + (int)(h->steps_done % per_day);
+    if (jt) *jt = (int)(h->steps_done / per_day);
     return HB_OK;
 }
 
@@ -1106,8 +1336,7 @@ extern "C" int hb_capture_graph(hb_handle *h, int32_t nsteps, void *stream) {
     cudaStream_t cap = st;
     bool own = false;
     if (!st) { HB_CUDA_RET(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)); own = true; }
-    if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
-    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    h->drop_graph();
     HB_CUDA_RET(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
     int st2 = enqueue_steps(h, nsteps, cap);
     cudaGraph_t g = nullptr;
@@ -1147,7 +1376,102 @@ extern "C" int hb_device_state(hb_handle *h, void **H, void **U, void **V, void 
 }
 
 extern "C" int hb_get_permutation(hb_handle *h, int32_t *perm) {
-    if (!h || !perm) return hb::set_error(HB_E_INVALID, "null argument");
-    memcpy(perm, h->perm.data(), h->perm.size() * sizeof(int32_t));
+    return hb_get_permutation_at(h, 0, perm);
+}
+
+extern "C" int hb_get_permutation_at(hb_handle *h, int32_t s, int32_t *perm) {
+    TRY(check_scenario(h, s));
+    if (!perm) return hb::set_error(HB_E_INVALID, "null argument");
+    memcpy(perm, h->scn[s].perm.data(), h->scn[s].perm.size() * sizeof(int32_t));
+    return HB_OK;
+}
+
+extern "C" int hb_set_tile_config(hb_handle *h, int32_t tile_config) {
+    if (!h) return hb::set_error(HB_E_INVALID, "null handle");
+    if (tile_config < 0 || tile_config > hb::N_LAUNCH_CONFIGS)
+        return hb::set_error(HB_E_INVALID, "tile_config %d outside 0..%d", tile_config, hb::N_LAUNCH_CONFIGS);
+    const int c = tile_config == 0 ? hb::DEFAULT_LAUNCH_CONFIG : tile_config - 1;
+    if (c != h->launch_config) h->drop_graph();
+    h->launch_config = c;
+    return HB_OK;
+}
+
+extern "C" int hb_get_tile_config(hb_handle *h, int32_t *tile_config) {
+    if (!h || !tile_config) return hb::set_error(HB_E_INVALID, "null argument");
+    *tile_config = h->launch_config + 1;
+    return HB_OK;
+}
+
+// The autotuner: every launch shape runs `steps` steps from the current state
+// (after one untimed step), timed with CUDA events on `stream`; the state,
+// fluxes, boundary codes, error bits and step counter are restored after each
+// trial and at the end, so the handle continues as if nothing had run.  The
+// fastest shape becomes the handle's (a captured graph is dropped).
+extern "C" int hb_autotune(hb_handle *h, int32_t steps, void *stream, float *ms_per_step, int32_t capacity,
+                           int32_t *best) {
+    if (!h || steps <= 0) return hb::set_error(HB_E_INVALID, "hb_autotune: bad argument");
+    TRY(check_range(h, (long long)steps + 1));
+    cudaStream_t st = (cudaStream_t)stream;
+    HB_CUDA_RET(cudaDeviceSynchronize());
+    // snapshot of everything a step writes
+    struct Piece { void *p; size_t bytes; };
+    std::vector<Piece> pieces;
+    h->with_mesh([&](auto &m) {
+        using R = typename std::remove_reference<decltype(m)>::type::R;
+        const size_t C = (size_t)h->C;
+        pieces = {{m.S[0], 4 * C * sizeof(R)}, {m.S[1], 4 * C * sizeof(R)}, {m.W, C * sizeof(R)},
+                  {m.f0, 4 * C * sizeof(R)}, {m.f1, 4 * C * sizeof(R)}, {m.f2, 4 * C * sizeof(R)},
+                  {m.f3, 4 * C * sizeof(R)}, {m.rmeta, (size_t)std::max(m.nrecords, 1)},
+                  {h->d_err, sizeof(uint32_t)}, {h->d_ctr, sizeof(long long)}};
+        return HB_OK;
+    });
+    size_t total = 0;
+    for (auto &p : pieces) total += (p.bytes + 255) & ~(size_t)255;
+    char *snap = nullptr;
+    {
+        cudaError_t e = cudaMalloc(&snap, total);
+        if (e != cudaSuccess) return hb::set_error(HB_E_NOMEM, "hb_autotune: cudaMalloc(%zu): %s", total, cudaGetErrorString(e));
+    }
+    auto copy_all = [&](bool save) -> int {
+        size_t off = 0;
+        for (auto &p : pieces) {
+            if (save) HB_CUDA_RET(cudaMemcpyAsync(snap + off, p.p, p.bytes, cudaMemcpyDeviceToDevice, st));
+            else HB_CUDA_RET(cudaMemcpyAsync(p.p, snap + off, p.bytes, cudaMemcpyDeviceToDevice, st));
+            off += (p.bytes + 255) & ~(size_t)255;
+        }
+        return HB_OK;
+    };
+    const int saved_config = h->launch_config;
+    int rc = copy_all(true);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (rc == HB_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        rc = hb::set_error(HB_E_CUDA, "hb_autotune: cudaEventCreate failed");
+    int best_c = saved_config;
+    float best_ms = 0.f;
+    for (int c = 0; rc == HB_OK && c < hb::N_LAUNCH_CONFIGS; c++) {
+        h->launch_config = c;
+        if ((rc = copy_all(false)) != HB_OK) break;
+        if ((rc = enqueue_steps(h, 1, st)) != HB_OK) break;
+        if (cudaEventRecord(e0, st) != cudaSuccess) { rc = hb::set_error(HB_E_CUDA, "cudaEventRecord"); break; }
+        if ((rc = enqueue_steps(h, steps, st)) != HB_OK) break;
+        if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = hb::set_error(HB_E_CUDA, "hb_autotune: event wait failed");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= (float)steps;
+        if (ms_per_step && c < capacity) ms_per_step[c] = ms;
+        if (c == 0 || ms < best_ms) { best_ms = ms; best_c = c; }
+    }
+    if (rc == HB_OK) rc = copy_all(false);
+    cudaStreamSynchronize(st);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(snap);
+    if (rc != HB_OK) { h->launch_config = saved_config; return rc; }
+    if (best_c != saved_config) h->drop_graph();
+    h->launch_config = best_c;
+    if (best) *best = best_c + 1;
     return HB_OK;
 }

@@ -81,6 +81,17 @@ def lib():
         "hb_tile_configs": (C.c_int, [_ip, _ip, C.c_int32]),
         "hb_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(Options), C.POINTER(vp)]),
         "hb_destroy": (C.c_int, [vp]),
+        "hb_create_batch": (C.c_int, [C.POINTER(MeshDesc), C.c_int32, C.POINTER(Options), C.POINTER(vp)]),
+        "hb_batch_size": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+        "hb_scenario_cells": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+        "hb_set_state_at": (C.c_int, [vp, C.c_int32, _dp, _dp, _dp, _dp, _dp]),
+        "hb_get_state_at": (C.c_int, [vp, C.c_int32, _dp, _dp, _dp, _dp, _dp]),
+        "hb_get_flux_at": (C.c_int, [vp, C.c_int32, _dp, _dp, _dp, _dp]),
+        "hb_get_klas_at": (C.c_int, [vp, C.c_int32, _dp]),
+        "hb_get_permutation_at": (C.c_int, [vp, C.c_int32, _ip]),
+        "hb_set_tile_config": (C.c_int, [vp, C.c_int32]),
+        "hb_get_tile_config": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+        "hb_autotune": (C.c_int, [vp, C.c_int32, vp, C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_int32)]),
         "hb_set_state": (C.c_int, [vp, _dp, _dp, _dp, _dp, _dp]),
         "hb_get_state": (C.c_int, [vp, _dp, _dp, _dp, _dp, _dp]),
         "hb_get_flux": (C.c_int, [vp, _dp, _dp, _dp, _dp]),
@@ -129,4 +140,7 @@ EXPORTED = ["hb_options_default", "hb_tile_configs", "hb_create", "hb_destroy", 
             "hb_graph_launch", "hb_device_state", "hb_get_permutation", "hb_device_errors", "hb_last_error",
             "hb_last_error_string", "hb_status_string", "hb_deck_load", "hb_deck_mesh", "hb_deck_state",
             "hb_deck_free", "hb_ref_calculate_flux", "hb_ref_update_cell", "hb_ref_calculate_flux_f32",
-            "hb_ref_update_cell_f32", "hb_ref_take_device_errors", "hb_ref_step_static"]
+            "hb_ref_update_cell_f32", "hb_ref_take_device_errors", "hb_ref_step_static",
+            "hb_create_batch", "hb_batch_size", "hb_scenario_cells", "hb_set_state_at", "hb_get_state_at",
+            "hb_get_flux_at", "hb_get_klas_at", "hb_get_permutation_at", "hb_set_tile_config", "hb_get_tile_config",
+            "hb_autotune"]

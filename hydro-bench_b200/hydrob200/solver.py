@@ -9,7 +9,7 @@ interval and the interval ("day") index of ``cuda_native_impl/benchmark.cu:87-96
 from __future__ import annotations
 
 import ctypes as C
-from typing import Dict, Optional
+from typing import Dict, Optional, Sequence
 
 import numpy as np
 
@@ -167,6 +167,25 @@ class Solver:
     def graph_launch(self, stream=None) -> None:
         check(lib().hb_graph_launch(self._h, _stream_handle(stream)))
 
+    @property
+    def tile_config(self) -> int:
+        v = C.c_int32()
+        check(lib().hb_get_tile_config(self._h, C.byref(v)))
+        return v.value
+
+    @tile_config.setter
+    def tile_config(self, cfg: int) -> None:
+        check(lib().hb_set_tile_config(self._h, int(cfg)))
+
+    def autotune(self, steps: int = 20, stream=None):
+        """hb_autotune: times every launch shape on this handle's mesh(es) and
+        keeps the fastest; returns (best tile_config, ms per step by config)."""
+        n = lib().hb_tile_configs(None, None, 0)
+        ms = (C.c_float * n)()
+        best = C.c_int32()
+        check(lib().hb_autotune(self._h, int(steps), _stream_handle(stream), ms, n, C.byref(best)))
+        return best.value, {i + 1: float(ms[i]) for i in range(n)}
+
     def permutation(self) -> np.ndarray:
         p = np.empty(self.cells, dtype=np.int32)
         check(lib().hb_get_permutation(self._h, p.ctypes.data_as(_lib._ip)))
@@ -188,6 +207,71 @@ class Solver:
 
         return {k: torch.as_tensor(_CAI(p.value, self.cells, stride.value if k != "W" else 1), device="cuda")
                 for k, p in zip("HUVZW", ptrs)}
+
+
+class Batch(Solver):
+    """A batch of independent scenarios stepped together (``hb_create_batch``).
+
+    Every launch covers all scenarios; per-scenario state, fluxes and boundary
+    codes are read and written with the ``*_at`` calls (``scenario`` index).
+    ``step``, ``sync``, ``capture_graph`` and ``graph_launch`` advance all.
+    """
+
+    def __init__(self, decks: Sequence[Deck], variant="H", precision="fp64", device: int = 0,
+                 renumber: bool = True, init_state: bool = True, tile_config: int = 0):
+        self.decks = list(decks)   # keeps the host arrays alive
+        opt = _lib.Options()
+        lib().hb_options_default(C.byref(opt))
+        opt.variant = _VARIANTS[variant]
+        opt.precision = _PRECISIONS[precision]
+        opt.device = device
+        opt.renumber = 1 if renumber else 0
+        opt.tile_config = int(tile_config)
+        self.variant = opt.variant
+        self.precision = opt.precision
+        meshes = (_lib.MeshDesc * len(self.decks))(*[d.mesh for d in self.decks])
+        self._h = C.c_void_p()
+        check(lib().hb_create_batch(meshes, len(self.decks), C.byref(opt), C.byref(self._h)))
+        self.sizes = [d.cells for d in self.decks]
+        self.cells = sum(self.sizes)
+        if init_state:
+            for i, d in enumerate(self.decks):
+                st = d.state()
+                self.set_state(st["H"], st["U"], st["V"], st["Z"], st["W"], scenario=i)
+
+    def __len__(self):
+        return len(self.decks)
+
+    def set_state(self, H, U, V, Z, W=None, scenario: int = 0):
+        n = self.sizes[scenario]
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (H, U, V, Z)]
+        w = np.ascontiguousarray(W, dtype=np.float64) if W is not None else None
+        for a in arrs:
+            if a.shape != (n,):
+                raise ValueError(f"state arrays of scenario {scenario} must have shape ({n},)")
+        check(lib().hb_set_state_at(self._h, scenario, *[_as_dp(a) for a in arrs],
+                                    _as_dp(w) if w is not None else None))
+
+    def get_state(self, scenario: int = 0) -> Dict[str, np.ndarray]:
+        out = {k: np.empty(self.sizes[scenario]) for k in "HUVZW"}
+        check(lib().hb_get_state_at(self._h, scenario, *[_as_dp(out[k]) for k in "HUVZW"]))
+        return out
+
+    def flux(self, scenario: int = 0) -> Dict[str, np.ndarray]:
+        n = 4 * self.sizes[scenario]
+        out = {k: np.empty(n) for k in ("FLUX0", "FLUX1", "FLUX2", "FLUX3")}
+        check(lib().hb_get_flux_at(self._h, scenario, *[_as_dp(out[k]) for k in ("FLUX0", "FLUX1", "FLUX2", "FLUX3")]))
+        return out
+
+    def klas(self, scenario: int = 0) -> np.ndarray:
+        out = np.empty(4 * self.sizes[scenario])
+        check(lib().hb_get_klas_at(self._h, scenario, _as_dp(out)))
+        return out
+
+    def permutation(self, scenario: int = 0) -> np.ndarray:
+        p = np.empty(self.sizes[scenario], dtype=np.int32)
+        check(lib().hb_get_permutation_at(self._h, scenario, p.ctypes.data_as(_lib._ip)))
+        return p
 
 
 class RefLayoutMesh:

@@ -87,6 +87,36 @@ void hb_options_default(hb_options *opt);
 int hb_create(const hb_mesh_desc *mesh, const hb_options *opt, hb_handle **out);
 int hb_destroy(hb_handle *h);
 
+/* A batch of n independent scenarios (meshes of any sizes, their own DT, HM1,
+ * HM2, JL and boundary tables) stepped together: every kernel launch covers
+ * all of them, each CTA taking one scenario's records or cells from a segment
+ * table.  No reference counterpart; the reference runs one mesh per process.
+ * The calls below without _at address scenario 0; hb_step, hb_sync,
+ * hb_capture_graph and hb_graph_launch advance every scenario, and
+ * hb_position reports scenario 0's (kt, jt).  hb_step_host is single-mesh only. */
+int hb_create_batch(const hb_mesh_desc *meshes, int32_t n, const hb_options *opt, hb_handle **out);
+int hb_batch_size(hb_handle *h, int32_t *n);
+/* Cells of scenario s and the device index of its first cell. */
+int hb_scenario_cells(hb_handle *h, int32_t s, int32_t *cells, int32_t *first);
+int hb_set_state_at(hb_handle *h, int32_t s, const double *H, const double *U, const double *V, const double *Z,
+                    const double *W);
+int hb_get_state_at(hb_handle *h, int32_t s, double *H, double *U, double *V, double *Z, double *W);
+int hb_get_flux_at(hb_handle *h, int32_t s, double *F0, double *F1, double *F2, double *F3);
+int hb_get_klas_at(hb_handle *h, int32_t s, double *klas);
+int hb_get_permutation_at(hb_handle *h, int32_t s, int32_t *perm);
+
+/* Launch shape of a handle (index + 1 into hb_tile_configs; 0 = default).
+ * Changing it drops a captured graph. */
+int hb_set_tile_config(hb_handle *h, int32_t tile_config);
+int hb_get_tile_config(hb_handle *h, int32_t *tile_config);
+/* Autotuner: times every launch shape over `steps` steps of this handle's own
+ * mesh(es) from the current state (CUDA events on `stream`), restores the
+ * state, fluxes, boundary codes, error bits and step counter afterwards, and
+ * keeps the fastest shape (*best, as a tile_config).  ms_per_step[i] (i <
+ * capacity) receives shape i+1's time.  Drops a captured graph if the shape
+ * changes.  Needs steps + 1 steps of boundary tables beyond the position. */
+int hb_autotune(hb_handle *h, int32_t steps, void *stream, float *ms_per_step, int32_t capacity, int32_t *best);
+
 /* State in reference order, fp64 host arrays of [CELL]. W may be NULL. */
 int hb_set_state(hb_handle *h, const double *H, const double *U, const double *V, const double *Z, const double *W);
 int hb_get_state(hb_handle *h, double *H, double *U, double *V, double *Z, double *W);
