@@ -408,22 +408,47 @@ __device__ __forceinline__ void table_lookup(typename A::real x, typename A::lev
     }
 }
 
+// Arithmetic of the iterated boundary conditions (KLAS 10 depth, KLAS 1 / 3
+// Riemann invariant).  Their stopping tests (|change| <= tol) turn a rounding
+// difference into a different iteration count and so into a flux difference
+// of the order of the tolerance; split precision therefore runs them in fp64
+// (a few boundary edges per mesh).  The other policies use their own.
+template <class A> struct iter_policy { using type = A; };
+template <> struct iter_policy<F32Split> { using type = F64Exact; };
+template <class A> using iter_real = typename iter_policy<A>::type::real;
+
 // Riemann-invariant iteration of KLAS 1 / 3 (functors.cu:355-367, :379-391)
 template <class A>
-__device__ __forceinline__ typename A::real invariant_iter(typename A::real ql1, typename A::real h,
-                                                           typename A::real hb1, double tol, int mfial, int mfiar) {
-    using R = typename A::real;
-    R fial = A::madd(A::c(6.264), A::sqrt(h), ql1, mfial);
-    R ur0 = ql1, urb = ur0;
-    R shb = A::sqrt(hb1);
+__device__ __forceinline__ iter_real<A> invariant_iter(iter_real<A> ql1, iter_real<A> h, iter_real<A> hb1, double tol,
+                                                       int mfial, int mfiar) {
+    using I = typename iter_policy<A>::type;
+    using T = iter_real<A>;
+    T fial = I::madd(I::c(6.264), I::sqrt(h), ql1, mfial);
+    T ur0 = ql1, urb = ur0;
+    T shb = I::sqrt(hb1);
     for (int k = 1; k <= 30; k++) {
-        R fiar = A::madd(A::c(-6.264), shb, urb, mfiar);
-        R dsum = A::add(fial, fiar), ddif = A::sub(fial, fiar);
-        urb = A::divk(A::div(A::mul(A::mul(dsum, ddif), ddif), hb1), 313.92);
-        if (A::fabs(A::sub(urb, ur0)) <= A::c(tol)) break;
+        T fiar = I::madd(I::c(-6.264), shb, urb, mfiar);
+        T dsum = I::add(fial, fiar), ddif = I::sub(fial, fiar);
+        urb = I::divk(I::div(I::mul(I::mul(dsum, ddif), ddif), hb1), 313.92);
+        if (I::fabs(I::sub(urb, ur0)) <= I::c(tol)) break;
         ur0 = urb;
     }
     return urb;
+}
+
+// Depth at a given-discharge boundary, KLAS 10 (functors.cu:212-224)
+template <class A>
+__device__ __forceinline__ iter_real<A> inflow_depth(iter_real<A> fil, iter_real<A> f0, iter_real<A> h) {
+    using I = typename iter_policy<A>::type;
+    using T = iter_real<A>;
+    T hb0 = h, hb = T(0);
+    for (int k = 1; k <= 20; k++) {
+        T w = I::sub(fil, I::div(f0, hb0));
+        hb = I::divk(I::mul(w, w), 39.24);
+        if (I::fabs(I::sub(hb0, hb)) <= I::c(0.005)) break;
+        hb0 = I::add(I::mul(hb0, I::c(0.5)), I::mul(hb, I::c(0.5)));
+    }
+    return hb;
 }
 
 template <class A, int VARIANT, class TableFetch>
@@ -432,6 +457,8 @@ __device__ __forceinline__ void bounda(const SlotInA<A> &in, const StepParams &p
                                        typename A::real vc, const TableFetch &fetch, SlotOut<typename A::real> &o) {
     using R = typename A::real;
     using L = typename A::level;
+    using I = typename iter_policy<A>::type;
+    using T = iter_real<A>;
     const R h = in.own.h;
     const R hm2 = A::c(p.hm2);
     R cl = A::sqrt(A::mul(A::c(9.81), h));
@@ -452,18 +479,13 @@ __device__ __forceinline__ void bounda(const SlotInA<A> &in, const StepParams &p
         BoundaryInA<A> b = fetch();
         R f0 = -A::madd(b.dqt, A::c((double)p.kt), b.qt, M_K10);
         f0 = A::div(f0, in.side);
-        R qb2 = A::mul(f0, f0);
-        R hb0 = h, hb = R(0);
-        for (int k = 1; k <= 20; k++) {
-            R w = A::sub(fil, A::div(f0, hb0));
-            hb = A::divk(A::mul(w, w), 39.24);
-            if (A::fabs(A::sub(hb0, hb)) <= A::c(0.005)) break;
-            hb0 = A::add(A::mul(hb0, A::c(0.5)), A::mul(hb, A::c(0.5)));
-        }
+        const T f0t = (T)f0;
+        const T qb2 = I::mul(f0t, f0t);
+        const T hb = inflow_depth<A>((T)fil, f0t, (T)h);
         o.f[0] = f0;
-        o.f[1] = hb <= R(1) ? R(0) : A::div(qb2, hb);
+        o.f[1] = hb <= T(1) ? R(0) : (R)I::div(qb2, hb);
         o.f[2] = R(0);
-        o.f[3] = A::mul(A::mul(A::c(4.905), hb), hb);
+        o.f[3] = (R)I::mul(I::mul(I::c(4.905), hb), hb);
         o.mask = 0xF;
         break;
     }
@@ -474,18 +496,19 @@ __device__ __forceinline__ void bounda(const SlotInA<A> &in, const StepParams &p
         L zq = L(0);   // the reference leaves ZQH1 unset when the cell has no table (NHQ1 = 0)
         table_lookup<A>(q3, zq, b.qw, b.zw, b.nhq1);
         R dzq = A::depth(zq, in.own.z);
-        R hb1 = A::fmax(A::depth(zq, in.own.zbc), hm2);
+        const T hb1 = I::fmax((T)A::lsub(zq, in.own.zbc), I::c(p.hm2));
         R qw1 = b.nhq > 1 ? b.qw[1] : R(0);   // QW_row[1] (functors.cu:347)
         ql[1] = A::fmax(ql[1], R(0));
-        if (q3 <= qw1 || hb1 <= hm2 || dzq >= A::c(0.1)) {
+        if (q3 <= qw1 || hb1 <= I::c(p.hm2) || dzq >= A::c(0.1)) {
             o.f[0] = A::mul(h, ql[1]);
             o.f[1] = A::mul(o.f[0], ql[1]);
             o.f[3] = A::mul(A::mul(A::c(4.905), h), h);
         } else {
-            R urb = invariant_iter<A>(ql[1], h, hb1, 0.001, M_FIAL3, M_FIAR3);
-            o.f[0] = A::mul(hb1, urb);
-            o.f[1] = A::mul(o.f[0], urb);
-            o.f[3] = A::mul(A::mul(A::c(4.905), hb1), hb1);
+            const T urb = invariant_iter<A>((T)ql[1], (T)h, hb1, 0.001, M_FIAL3, M_FIAR3);
+            const T f0 = I::mul(hb1, urb);
+            o.f[0] = (R)f0;
+            o.f[1] = (R)I::mul(f0, urb);
+            o.f[3] = (R)I::mul(I::mul(I::c(4.905), hb1), hb1);
         }
         o.mask = 0xF;
         break;
@@ -493,12 +516,12 @@ __device__ __forceinline__ void bounda(const SlotInA<A> &in, const StepParams &p
     case CODE_K1: {
         BoundaryInA<A> b = fetch();
         int mult = VARIANT == 1 ? p.kt : p.jt;
-        R hb1 = A::depth(A::lmadd(b.dzt, A::lc((double)mult), b.zt, M_K1), in.own.zbc);
-        hb1 = A::fmax(hb1, hm2);
-        R urb = invariant_iter<A>(ql[1], h, hb1, 0.0001, M_FIAL1, M_FIAR1);
-        o.f[0] = A::mul(hb1, urb);
-        o.f[1] = A::mul(o.f[0], urb);
-        o.f[3] = A::mul(A::mul(A::c(4.905), hb1), hb1);
+        const T hb1 = I::fmax((T)A::lsub(A::lmadd(b.dzt, A::lc((double)mult), b.zt, M_K1), in.own.zbc), I::c(p.hm2));
+        const T urb = invariant_iter<A>((T)ql[1], (T)h, hb1, 0.0001, M_FIAL1, M_FIAR1);
+        const T f0 = I::mul(hb1, urb);
+        o.f[0] = (R)f0;
+        o.f[1] = (R)I::mul(f0, urb);
+        o.f[3] = (R)I::mul(I::mul(I::c(4.905), hb1), hb1);
         o.mask = 0xF;
         break;
     }

@@ -615,13 +615,10 @@ def config_24k(seed: int = 20240603, steps: int = 1000, n_field: Optional[np.nda
     return channel_deck("C24K", 24_020, 20_000.0, 4_000.0, seed, steps=steps, mdt=60, n_field=n_field)
 
 
-def config_ensemble(n: int = 64, seed: int = 20240604, steps: int = 1000, cmin: int = 5_000,
-                    cmax: int = 200_000, dt: float = 0.5) -> List[Deck]:
-    """The batched ensemble: ``n`` independent channel scenarios, each from its
-    own seed.  Cells are log-uniform in [cmin, cmax]; Manning n ~ U(0.015, 0.04);
-    a Gaussian inflow hydrograph peaking at Q ~ U(50, 500) m^3/s at t = 250 s
-    (sigma 100 s); dt = 0.5 s.  Each domain is 5:1 with the cell area of the
-    207,234-cell configuration (40 km x 8 km), bumps of 1 m."""
+def ensemble_specs(n: int = 64, seed: int = 20240604, steps: int = 1000, cmin: int = 5_000,
+                   cmax: int = 200_000, dt: float = 0.5) -> List[dict]:
+    """Parameters of the batched ensemble's scenarios (see config_ensemble),
+    one dict of channel_deck arguments per scenario."""
     rng = np.random.default_rng(seed)
     cell_area = 40_000.0 * 8_000.0 / 207_234
     out = []
@@ -631,8 +628,21 @@ def config_ensemble(n: int = 64, seed: int = 20240604, steps: int = 1000, cmin: 
         q_peak = float(rng.uniform(50.0, 500.0))
         ly = math.sqrt(c * cell_area / 5.0)
         lx = 5.0 * ly
-        out.append(channel_deck(f"E{i:02d}_{c}", c, lx, ly, seed * 1000 + i, bump_amp=1.0,
-                                bump_width=max(150.0, 0.015 * lx), hydrograph=(q_peak, 250.0, 100.0),
-                                n_manning=n_man, dt=dt, steps=steps, mdt=60))
+        out.append(dict(name=f"E{i:02d}_{c}", ncells=c, lx=lx, ly=ly, seed=seed * 1000 + i, bump_amp=1.0,
+                        bump_width=max(150.0, 0.015 * lx), hydrograph=(q_peak, 250.0, 100.0),
+                        n_manning=n_man, dt=dt, steps=steps, mdt=60))
     return out
 
+
+def ensemble_deck(spec: dict) -> Deck:
+    return channel_deck(**spec)
+
+
+def config_ensemble(n: int = 64, seed: int = 20240604, steps: int = 1000, cmin: int = 5_000,
+                    cmax: int = 200_000, dt: float = 0.5) -> List[Deck]:
+    """The batched ensemble: ``n`` independent channel scenarios, each from its
+    own seed.  Cells are log-uniform in [cmin, cmax]; Manning n ~ U(0.015, 0.04);
+    a Gaussian inflow hydrograph peaking at Q ~ U(50, 500) m^3/s at t = 250 s
+    (sigma 100 s); dt = 0.5 s.  Each domain is 5:1 with the cell area of the
+    207,234-cell configuration (40 km x 8 km), bumps of 1 m."""
+    return [ensemble_deck(sp) for sp in ensemble_specs(n, seed, steps, cmin, cmax, dt)]
