@@ -77,6 +77,8 @@ extern "C" void hb_options_default(hb_options *o) {
     o->device = 0;
     o->renumber = 1;
     o->tile_config = 0;
+    o->layout = HB_LAYOUT_EDGE;
+    o->tile_cells = 0;
 }
 
 namespace hb {
@@ -86,15 +88,26 @@ namespace hb {
 // ---------------------------------------------------------------------------
 enum : uint8_t { META_CODE = 0x0F, META_OWN_FIRST = 0x10, META_HAS_NB = 0x20 };
 
-// Launch shapes of the flux kernel (threads per CTA, CTAs per SM asked of the
-// compiler through __launch_bounds__, which caps registers per thread).
-// (The cell kernel has 128 threads per CTA and asks for update_min_blocks.)
-struct LaunchConfig { int threads, min_blocks, update_min_blocks; };
-constexpr LaunchConfig LAUNCH_CONFIGS[] = {{128, 6, 6}, {128, 6, 8}, {128, 8, 8}, {256, 3, 6}, {256, 4, 8},
-                                           {128, 4, 6}, {256, 2, 6}, {64, 12, 8}};
+// Launch shapes.  Edge layout: the flux kernel's threads per CTA and CTAs per
+// SM asked of the compiler through __launch_bounds__ (which caps registers
+// per thread), and the cell kernel's CTAs per SM (it has UPDATE_THREADS
+// threads).  Tile layout: the tile kernel's threads per CTA and CTAs per SM.
+enum Layout : int { LAYOUT_EDGE = HB_LAYOUT_EDGE, LAYOUT_TILE = HB_LAYOUT_TILE };
+struct LaunchConfig { int layout, threads, min_blocks, update_min_blocks; };
+constexpr LaunchConfig LAUNCH_CONFIGS[] = {
+    {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 8}, {LAYOUT_EDGE, 128, 8, 8}, {LAYOUT_EDGE, 256, 3, 6},
+    {LAYOUT_EDGE, 256, 4, 8}, {LAYOUT_EDGE, 128, 4, 6}, {LAYOUT_EDGE, 256, 2, 6}, {LAYOUT_EDGE, 64, 12, 8},
+    {LAYOUT_TILE, 256, 3, 0}, {LAYOUT_TILE, 256, 2, 0}, {LAYOUT_TILE, 128, 6, 0}, {LAYOUT_TILE, 128, 4, 0},
+    {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0}};
 constexpr int N_LAUNCH_CONFIGS = sizeof(LAUNCH_CONFIGS) / sizeof(LAUNCH_CONFIGS[0]);
-constexpr int DEFAULT_LAUNCH_CONFIG = 0;
+constexpr int DEFAULT_EDGE_CONFIG = 0;
+constexpr int DEFAULT_TILE_CONFIG = 8;
 constexpr int UPDATE_THREADS = 128;
+
+// One tile of the tile layout: a compact group of cells, contiguous in the
+// device order, with its records (mirror pairs inside the tile, then every
+// other real slot of its cells).
+struct TileDesc { int scn, cell0, cells, rec0, npairs, nsingles; };
 
 // Constants of one scenario of a batch (the only entry for a single mesh).
 struct ScnParams {
@@ -146,6 +159,9 @@ struct DevMesh {
     const ScnParams *scn;      // [nscen]
     const int4 *fseg;          // flux CTAs {scenario, first record, records, 1 = mirror pairs}
     const int4 *useg;          // update CTAs {scenario, first cell, cells, 0}
+    // tile layout
+    const TileDesc *tiles;     // [ntiles]
+    int ntiles, max_tile_cells, max_tile_pairs;
 };
 
 struct StepIndex { int par, kt, jt; };
@@ -189,17 +205,24 @@ __device__ __forceinline__ CellStateA<A> load_cell(const DevMesh<A> &m, int par,
     else return {v.x, v.y, v.z, v.w, zbc};
 }
 
+// Where a step keeps the slots' terms of the cell sums between the flux and
+// the update: slot s at p + 4 * (s - slot0).  Global memory (m.slotw, slot0 =
+// 0) between the two kernels of the edge layout; shared memory (slot0 = the
+// tile's first slot) inside the tile kernel.
+template <class R>
+struct Terms { R *p; int slot0; };
+
 // the slot's terms of the cell sums (functors.cu:733-741): F0 and SIDE for
 // WH = fma(SIDE, F0, WH), and the complete WU / WV increments
 template <class A>
-__device__ __forceinline__ void store_terms(const DevMesh<A> &m, int s, const typename A::real f[4],
+__device__ __forceinline__ void store_terms(const Terms<typename A::real> &t, int s, const typename A::real f[4],
                                             typename A::real side, typename A::real cs, typename A::real sn) {
     using R = typename A::real;
     const R fr1 = A::add(f[1], f[3]);
     const R slcos = A::mul(side, cs), slsin = A::mul(side, sn);
     const R dwu = A::dot(slcos, fr1, -slsin, f[2], M_WU);
     const R dwv = A::dot(slsin, fr1, slcos, f[2], M_WV);
-    st4(m.slotw + 4 * (size_t)s, f[0], dwu, dwv, side);
+    st4(t.p + 4 * (size_t)(s - t.slot0), f[0], dwu, dwv, side);
 }
 
 template <class A>
@@ -210,7 +233,7 @@ __device__ __forceinline__ void store_flux(const DevMesh<A> &m, int s, const typ
 // One slot on its own: flux_slot with its boundary tables (functors.cu:47-202).
 template <class A, int VARIANT>
 __device__ __forceinline__ void single_record(const DevMesh<A> &m, int r, const StepIndex &si,
-                                              const StepParams &p, int write_flux) {
+                                              const StepParams &p, int write_flux, const Terms<typename A::real> &tout) {
     using R = typename A::real;
     const int4 ix = m.rix[r];
     const int a = ix.x, b = ix.y, sa = ix.z;
@@ -249,7 +272,7 @@ __device__ __forceinline__ void single_record(const DevMesh<A> &m, int r, const 
         if (!(o.mask & 8)) o.f[3] = m.f3[sa];
     }
     if (write_flux || o.mask != 0xF) store_flux(m, sa, o.f);
-    store_terms<A>(m, sa, o.f, in.side, in.cosj, in.sinj);
+    store_terms<A>(tout, sa, o.f, in.side, in.cosj, in.sinj);
     if (o.klas_to_zero) m.rmeta[r] = (uint8_t)((meta & ~META_CODE) | CODE_ZERO);
     if (o.undefined) atomicOr(m.err, ERRBIT_UNDEFINED);
 }
@@ -258,7 +281,7 @@ __device__ __forceinline__ void single_record(const DevMesh<A> &m, int r, const 
 // from the direct route's in the normal velocity).
 template <class A>
 __device__ __forceinline__ void pair_mirror(const DevMesh<A> &m, int r, const StepIndex &si,
-                                            const StepParams &p, int write_flux) {
+                                            const StepParams &p, int write_flux, const Terms<typename A::real> &tout) {
     using R = typename A::real;
     const int4 ix = m.rix[r];
     const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
@@ -273,7 +296,7 @@ __device__ __forceinline__ void pair_mirror(const DevMesh<A> &m, int r, const St
     fb[2] = fo[2];
     fb[3] = mirror_f3<A>(fo[3], A_.zbc, B_.zbc);
     if (write_flux) store_flux(m, ix.w, fb);
-    store_terms<A>(m, ix.w, fb, g.z, -cs, -sn);
+    store_terms<A>(tout, ix.w, fb, g.z, -cs, -sn);
 }
 
 template <class R>
@@ -292,7 +315,7 @@ __device__ __forceinline__ bool same_bits(R a, R b) {
 // evaluations run together after the main pass (pair_mirror).
 template <class A, int VARIANT>
 __device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const StepIndex &si, const StepParams &p,
-                                            int write_flux, int *queue, int *qn) {
+                                            int write_flux, const Terms<typename A::real> &tout, int *queue, int *qn) {
     using R = typename A::real;
     const int4 ix = m.rix[r];
     const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
@@ -312,7 +335,7 @@ __device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const St
         ra_ = flux_chain<A, VARIANT>(ia, clA, p, nofetch, oa);   // 0 or 1 (direct)
         if (!ra_) {
             if (write_flux) store_flux(m, ix.z, oa.f);
-            store_terms<A>(m, ix.z, oa.f, g.z, cs, sn);
+            store_terms<A>(tout, ix.z, oa.f, g.z, cs, sn);
         }
     }
     {
@@ -320,7 +343,7 @@ __device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const St
         rb_ = flux_chain<A, VARIANT>(ib, R(0), p, nofetch, ob);  // 0 or 2 (mirrored)
         if (!rb_) {
             if (write_flux) store_flux(m, ix.w, ob.f);
-            store_terms<A>(m, ix.w, ob.f, g.z, -cs, -sn);
+            store_terms<A>(tout, ix.w, ob.f, g.z, -cs, -sn);
         }
     }
     if (ra_ | rb_) {
@@ -341,7 +364,7 @@ __device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const St
             f[2] = fo[2];
             f[3] = fo[3];
             if (write_flux) store_flux(m, ix.z, f);
-            store_terms<A>(m, ix.z, f, g.z, cs, sn);
+            store_terms<A>(tout, ix.z, f, g.z, cs, sn);
         }
         if (rb_) {
             if (!ra_ || same_bits(qr1_d, qr1_m)) {
@@ -351,7 +374,7 @@ __device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const St
                 f[2] = (!ra_ || same_bits(ql2_d, ql2_m)) ? fo[2] : osher_f2<A>(tr, ql2_m, oi.qr[2]);
                 f[3] = mirror_f3<A>(fo[3], A_.zbc, B_.zbc);
                 if (write_flux) store_flux(m, ix.w, f);
-                store_terms<A>(m, ix.w, f, g.z, -cs, -sn);
+                store_terms<A>(tout, ix.w, f, g.z, -cs, -sn);
             } else {
                 queue[atomicAdd(qn, 1)] = r;
             }
@@ -391,12 +414,13 @@ __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k
         pair = r < m.npairs;
     }
     __syncthreads();
+    const Terms<typename A::real> tout{m.slotw, 0};
     if (valid) {
-        if (pair) pair_record<A, VARIANT>(m, r, si, p, write_flux, queue, &qn);
-        else single_record<A, VARIANT>(m, r, si, p, write_flux);
+        if (pair) pair_record<A, VARIANT>(m, r, si, p, write_flux, tout, queue, &qn);
+        else single_record<A, VARIANT>(m, r, si, p, write_flux, tout);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < qn; i += THREADS) pair_mirror<A>(m, queue[i], si, p, write_flux);
+    for (int i = threadIdx.x; i < qn; i += THREADS) pair_mirror<A>(m, queue[i], si, p, write_flux, tout);
 }
 
 // Sums and update of one cell (UpdateCellKernel, functors.cu:717-784).  The
@@ -404,7 +428,7 @@ __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k
 // (flux_slot's ZERO_LEN), exactly when fluxes are written out.
 template <class A, int VARIANT>
 __device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const StepIndex &si, const StepParams &p,
-                                           int write_flux) {
+                                           int write_flux, const typename A::real *terms) {
     using R = typename A::real;
     using L = typename A::level;
     const Vec4<R> raw = ld4(m.S[si.par] + 4 * (size_t)c);
@@ -416,7 +440,7 @@ __device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const Ste
     const R fnc = m.fnc[c], dta = m.dta[c], sidex = VARIANT == 1 ? m.sidex[c] : R(0);
     Vec4<R> t[4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) t[j] = ld4(m.slotw + 16 * (size_t)c + 4 * j);
+    for (int j = 0; j < 4; j++) t[j] = ld4(terms + 4 * j);
     R wh = R(0), wu = R(0), wv = R(0);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -469,15 +493,50 @@ __global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<A
         cudaTriggerProgrammaticLaunchCompletion();
         const StepIndex si = step_index(m, k, sp.per_day, sp.ndays);
         const StepParams p{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
-        if ((int)threadIdx.x < d.z) update_one<A, VARIANT>(m, d.y + (int)threadIdx.x, si, p, write_flux);
+        const int c = d.y + (int)threadIdx.x;
+        if ((int)threadIdx.x < d.z) update_one<A, VARIANT>(m, c, si, p, write_flux, m.slotw + 16 * (size_t)c);
     } else {
         cudaGridDependencySynchronize();
         cudaTriggerProgrammaticLaunchCompletion();
         const StepIndex si = step_index(m, k, m.per_day, m.ndays);
         const StepParams p{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
         for (int c = blockIdx.x * UPDATE_THREADS + threadIdx.x; c < m.C; c += gridDim.x * UPDATE_THREADS)
-            update_one<A, VARIANT>(m, c, si, p, write_flux);
+            update_one<A, VARIANT>(m, c, si, p, write_flux, m.slotw + 16 * (size_t)c);
     }
+}
+
+// The whole step of one tile (tile layout): every record of the tile writes
+// its slots' terms into shared memory, then each cell of the tile sums its
+// four slots in order and is updated.  Slots of edges that leave the tile are
+// single records, computed by each tile for its own slot as the reference
+// computes every slot; the state of the neighbour across is read from global
+// memory, where the previous step (the previous launch) left it.
+template <class A, int VARIANT, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) tile_kernel(DevMesh<A> m, int k, int write_flux) {
+    using R = typename A::real;
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    R *terms = reinterpret_cast<R *>(tile_smem);                                       // [max cells][4 slots][4]
+    int *queue = reinterpret_cast<int *>(tile_smem + 16 * sizeof(R) * (size_t)m.max_tile_cells);
+    __shared__ int qn;
+    const TileDesc td = m.tiles[blockIdx.x];   // constant tables: read before the dependency wait
+    const ScnParams sp = m.scn[td.scn];
+    if (threadIdx.x == 0) qn = 0;
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
+    const StepIndex si = step_index(m, k, sp.per_day, sp.ndays);
+    const StepParams p{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
+    const Terms<R> tout{terms, 4 * td.cell0};
+    __syncthreads();
+    const int nrec = td.npairs + td.nsingles;
+    for (int i = threadIdx.x; i < nrec; i += THREADS) {
+        if (i < td.npairs) pair_record<A, VARIANT>(m, td.rec0 + i, si, p, write_flux, tout, queue, &qn);
+        else single_record<A, VARIANT>(m, td.rec0 + i, si, p, write_flux, tout);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < qn; i += THREADS) pair_mirror<A>(m, queue[i], si, p, write_flux, tout);
+    __syncthreads();
+    for (int c = threadIdx.x; c < td.cells; c += THREADS)
+        update_one<A, VARIANT>(m, td.cell0 + c, si, p, write_flux, terms + 16 * c);
 }
 
 __global__ void tick_kernel(long long *ctr, int n) { *ctr += n; }
@@ -614,6 +673,84 @@ std::vector<int32_t> rcm_order(int C, const std::vector<int32_t> &nbr4) {
     return order;   // order[new] = old
 }
 
+// Tile partition of the tile layout (integer-only; changes no arithmetic).
+// Breadth-first balls of up to T cells are grown from the first unassigned
+// cell of the reverse Cuthill-McKee order, so consecutive tiles are
+// neighbours; then every tile under T/2 cells is merged into the adjacent
+// tile it shares most edges with, as long as the sum stays within 5T/4.
+// Returns order[new] = old with each tile contiguous, and the tile starts
+// (starts.back() == C).
+void tile_partition(int C, const std::vector<int32_t> &nbr4, int T, std::vector<int32_t> &order,
+                    std::vector<int32_t> &starts) {
+    const std::vector<int32_t> seeds = rcm_order(C, nbr4);
+    std::vector<int32_t> tile(C, -1);
+    std::vector<std::vector<int32_t>> cells;
+    for (int seed : seeds) {
+        if (tile[seed] >= 0) continue;
+        const int t = (int)cells.size();
+        cells.emplace_back();
+        auto &mem = cells.back();
+        mem.push_back(seed);
+        tile[seed] = t;
+        for (size_t head = 0; head < mem.size() && (int)mem.size() < T; head++) {
+            const int x = mem[head];
+            for (int j = 0; j < 4 && (int)mem.size() < T; j++) {
+                const int y = nbr4[4 * (size_t)x + j];
+                if (y >= 0 && tile[y] < 0) { tile[y] = t; mem.push_back(y); }
+            }
+        }
+    }
+    const int nt = (int)cells.size();
+    std::vector<int> parent(nt);
+    std::iota(parent.begin(), parent.end(), 0);
+    auto find = [&](int x) { while (parent[x] != x) x = parent[x] = parent[parent[x]]; return x; };
+    std::vector<int> size(nt);
+    for (int t = 0; t < nt; t++) size[t] = (int)cells[t].size();
+    const int cap = T + T / 4;
+    for (int pass = 0; pass < 3; pass++) {
+        std::vector<int> by_size;
+        for (int t = 0; t < nt; t++) if (find(t) == t && size[t] < T / 2) by_size.push_back(t);
+        std::stable_sort(by_size.begin(), by_size.end(), [&](int a, int b) { return size[a] < size[b]; });
+        bool merged = false;
+        for (int t : by_size) {
+            if (find(t) != t || size[t] >= T / 2) continue;
+            std::vector<std::pair<int, int>> shared;   // (neighbour root, shared slots)
+            for (int x : cells[t])
+                for (int j = 0; j < 4; j++) {
+                    const int y = nbr4[4 * (size_t)x + j];
+                    if (y < 0) continue;
+                    const int r = find(tile[y]);
+                    if (r == t) continue;
+                    bool found = false;
+                    for (auto &e : shared) if (e.first == r) { e.second++; found = true; break; }
+                    if (!found) shared.push_back({r, 1});
+                }
+            int best = -1, best_n = 0;
+            for (auto &e : shared)
+                if (size[e.first] + size[t] <= cap && (e.second > best_n || (e.second == best_n && e.first < best)))
+                    best = e.first, best_n = e.second;
+            if (best < 0) continue;
+            // the earlier tile keeps its place in the order
+            const int keep = std::min(best, t), gone = std::max(best, t);
+            cells[keep].insert(cells[keep].end(), cells[gone].begin(), cells[gone].end());
+            cells[gone].clear();
+            size[keep] += size[gone];
+            size[gone] = 0;
+            parent[gone] = keep;
+            merged = true;
+        }
+        if (!merged) break;
+    }
+    order.clear();
+    starts.clear();
+    for (int t = 0; t < nt; t++) {
+        if (find(t) != t) continue;
+        starts.push_back((int32_t)order.size());
+        order.insert(order.end(), cells[t].begin(), cells[t].end());
+    }
+    starts.push_back((int32_t)order.size());
+}
+
 }  // namespace hb
 
 // ---------------------------------------------------------------------------
@@ -630,6 +767,7 @@ struct Scenario {
     std::vector<int32_t> inv;           // inv[old] = new
     std::vector<double> klas_orig;      // [4 cells] reference order
     std::vector<int32_t> slot_index;    // [4 cells] device slot -> record, -1 = zero-length slot
+    std::vector<TileDesc> tiles;        // the whole scenario is one tile in the edge layout
     long long step_limit() const { return (long long)ndays * per_day; }
 };
 }  // namespace hb
@@ -734,7 +872,7 @@ struct HostMesh {
 
 // Validates one scenario's mesh and appends it (renumbered) to hm.
 template <class A>
-int append_scenario(const hb_mesh_desc *md, bool renumber, hb::Scenario &sc, HostMesh<A> &hm) {
+int append_scenario(const hb_mesh_desc *md, int scn, const hb_options &opt, hb::Scenario &sc, HostMesh<A> &hm) {
     using R = typename A::real;
     using L = typename A::level;
     if (md->cells <= 0 || md->ndays <= 0 || md->steps_per_day < 2 || md->nhq < 0)
@@ -758,8 +896,17 @@ int append_scenario(const hb_mesh_desc *md, bool renumber, hb::Scenario &sc, Hos
         if (nc != -1 && (nc < 0 || nc >= C)) return hb::set_error(HB_E_BADMESH, "NAC[%zu] = %g out of range", s, md->nac[s]);
         nbr_old[s] = nc;
     }
-    if (renumber) sc.perm = hb::rcm_order(C, nbr_old);
-    else { sc.perm.resize(C); std::iota(sc.perm.begin(), sc.perm.end(), 0); }
+    std::vector<int32_t> starts;
+    if (opt.layout == HB_LAYOUT_TILE) {
+        hb::tile_partition(C, nbr_old, opt.tile_cells > 0 ? opt.tile_cells : 256, sc.perm, starts);
+    } else {
+        if (opt.renumber) sc.perm = hb::rcm_order(C, nbr_old);
+        else { sc.perm.resize(C); std::iota(sc.perm.begin(), sc.perm.end(), 0); }
+        starts = {0, C};
+    }
+    std::vector<int32_t> tile_of(C);
+    for (size_t t = 0; t + 1 < starts.size(); t++)
+        for (int i = starts[t]; i < starts[t + 1]; i++) tile_of[i] = (int32_t)t;
     sc.inv.assign(C, -1);
     for (int i = 0; i < C; i++) sc.inv[sc.perm[i]] = i;
     sc.klas_orig.assign(md->klas, md->klas + S);
@@ -803,7 +950,8 @@ int append_scenario(const hb_mesh_desc *md, bool renumber, hb::Scenario &sc, Hos
             if (real4[4 * (size_t)i + j]) cm |= (uint8_t)(1u << j);
         hm.cmask.push_back(cm);
     }
-    // records: exact mirror pairs first, then every other real slot
+    // records, tile by tile: exact mirror pairs inside the tile first, then
+    // every other real slot of the tile's cells
     sc.rec0 = (int)hm.rix.size();
     std::vector<char> paired(S, 0);
     auto slot_of = [&](int i, int j) { return 4 * (size_t)perm[i] + j; };   // reference slot of device slot
@@ -814,35 +962,44 @@ int append_scenario(const hb_mesh_desc *md, bool renumber, hb::Scenario &sc, Hos
         hm.rgeo.push_back((R)md->cosf[so]); hm.rgeo.push_back((R)md->sinf[so]);
         hm.rgeo.push_back((R)md->side[so]); hm.rgeo.push_back(R(0));
     };
-    for (int i = 0; i < C; i++) {
-        for (int j = 0; j < 4; j++) {
-            const size_t sn = 4 * (size_t)i + j;
-            if (!real4[sn] || paired[sn] || (meta4[sn] & hb::META_CODE) != hb::CODE_ZERO || nbr4[sn] < 0) continue;
-            if (!(meta4[sn] & hb::META_OWN_FIRST)) continue;      // the pair is listed from its lower-numbered side
-            const int nb = nbr4[sn];
-            int jb = -1;
-            for (int q = 0; q < 4; q++)
-                if (nbr4[4 * (size_t)nb + q] == i && !paired[4 * (size_t)nb + q]) { jb = q; break; }
-            if (jb < 0) continue;
-            const size_t sb = 4 * (size_t)nb + jb;
-            const size_t oa = slot_of(i, j), ob = slot_of(nb, jb);
-            // the two slots must see one edge: code 0 both, negated normal, same length
-            if ((meta4[sb] & hb::META_CODE) != hb::CODE_ZERO || !real4[sb] || md->cosf[ob] != -md->cosf[oa] ||
-                md->sinf[ob] != -md->sinf[oa] || md->side[ob] != md->side[oa])
-                continue;
-            paired[sn] = paired[sb] = 1;
-            push(i, nb, sn, (long long)sb, meta4[sn], oa);
-        }
-    }
-    sc.npairs = (int)hm.rix.size() - sc.rec0;
     sc.slot_index.assign(S, -1);
-    for (int i = 0; i < C; i++) {
-        for (int j = 0; j < 4; j++) {
-            const size_t sn = 4 * (size_t)i + j;
-            if (!real4[sn] || paired[sn]) continue;
-            sc.slot_index[sn] = (int32_t)hm.rix.size();
-            push(i, nbr4[sn], sn, -1, meta4[sn], slot_of(i, j));
+    sc.npairs = 0;
+    sc.tiles.clear();
+    for (size_t t = 0; t + 1 < starts.size(); t++) {
+        hb::TileDesc td{scn, c0 + starts[t], starts[t + 1] - starts[t], (int)hm.rix.size(), 0, 0};
+        for (int i = starts[t]; i < starts[t + 1]; i++) {
+            for (int j = 0; j < 4; j++) {
+                const size_t sn = 4 * (size_t)i + j;
+                if (!real4[sn] || paired[sn] || (meta4[sn] & hb::META_CODE) != hb::CODE_ZERO || nbr4[sn] < 0) continue;
+                if (!(meta4[sn] & hb::META_OWN_FIRST)) continue;      // the pair is listed from its lower-numbered side
+                const int nb = nbr4[sn];
+                if (tile_of[nb] != (int32_t)t) continue;
+                int jb = -1;
+                for (int q = 0; q < 4; q++)
+                    if (nbr4[4 * (size_t)nb + q] == i && !paired[4 * (size_t)nb + q]) { jb = q; break; }
+                if (jb < 0) continue;
+                const size_t sb = 4 * (size_t)nb + jb;
+                const size_t oa = slot_of(i, j), ob = slot_of(nb, jb);
+                // the two slots must see one edge: code 0 both, negated normal, same length
+                if ((meta4[sb] & hb::META_CODE) != hb::CODE_ZERO || !real4[sb] || md->cosf[ob] != -md->cosf[oa] ||
+                    md->sinf[ob] != -md->sinf[oa] || md->side[ob] != md->side[oa])
+                    continue;
+                paired[sn] = paired[sb] = 1;
+                push(i, nb, sn, (long long)sb, meta4[sn], oa);
+                td.npairs++;
+            }
         }
+        for (int i = starts[t]; i < starts[t + 1]; i++) {
+            for (int j = 0; j < 4; j++) {
+                const size_t sn = 4 * (size_t)i + j;
+                if (!real4[sn] || paired[sn]) continue;
+                sc.slot_index[sn] = (int32_t)hm.rix.size();
+                push(i, nbr4[sn], sn, -1, meta4[sn], slot_of(i, j));
+                td.nsingles++;
+            }
+        }
+        sc.npairs += td.npairs;
+        sc.tiles.push_back(td);
     }
     sc.nrecords = (int)hm.rix.size() - sc.rec0;
     // boundary table rows of the cells that need them
@@ -873,14 +1030,13 @@ int append_scenario(const hb_mesh_desc *md, bool renumber, hb::Scenario &sc, Hos
 // (update), none straddling two scenarios or the pair/single boundary.
 std::vector<int4> flux_segments(const std::vector<hb::Scenario> &scn, int threads) {
     std::vector<int4> seg;
-    for (int s = 0; s < (int)scn.size(); s++) {
-        const auto &sc = scn[s];
-        for (int b = 0; b < sc.npairs; b += threads)
-            seg.push_back(make_int4(s, sc.rec0 + b, std::min(threads, sc.npairs - b), 1));
-        const int ns = sc.nrecords - sc.npairs;
-        for (int b = 0; b < ns; b += threads)
-            seg.push_back(make_int4(s, sc.rec0 + sc.npairs + b, std::min(threads, ns - b), 0));
-    }
+    for (int s = 0; s < (int)scn.size(); s++)
+        for (const hb::TileDesc &td : scn[s].tiles) {
+            for (int b = 0; b < td.npairs; b += threads)
+                seg.push_back(make_int4(s, td.rec0 + b, std::min(threads, td.npairs - b), 1));
+            for (int b = 0; b < td.nsingles; b += threads)
+                seg.push_back(make_int4(s, td.rec0 + td.npairs + b, std::min(threads, td.nsingles - b), 0));
+        }
     return seg;
 }
 std::vector<int4> update_segments(const std::vector<hb::Scenario> &scn) {
@@ -900,7 +1056,7 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *mds, int n, hb::DevMesh<
     HostMesh<A> hm;
     h->scn.resize(n);
     for (int s = 0; s < n; s++) {
-        const int st = append_scenario<A>(&mds[s], h->opt.renumber != 0, h->scn[s], hm);
+        const int st = append_scenario<A>(&mds[s], s, h->opt, h->scn[s], hm);
         if (st != HB_OK) return n > 1 ? hb::set_error(st, "scenario %d: %s", s, hb_last_error_string()) : st;
     }
     const int C = (int)hm.zbc.size();
@@ -1002,6 +1158,21 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *mds, int n, hb::DevMesh<
     }
     m.fseg = h->d_fseg[1];
     m.useg = h->d_useg;
+    {
+        std::vector<hb::TileDesc> tiles;
+        m.max_tile_cells = 1;
+        m.max_tile_pairs = 1;
+        for (const auto &sc : h->scn)
+            for (const auto &td : sc.tiles) {
+                tiles.push_back(td);
+                m.max_tile_cells = std::max(m.max_tile_cells, td.cells);
+                m.max_tile_pairs = std::max(m.max_tile_pairs, td.npairs);
+            }
+        m.ntiles = (int)tiles.size();
+        hb::TileDesc *tp;
+        TRY(dev_upload(h, &tp, tiles));
+        m.tiles = tp;
+    }
     // scenario permutations on the device, for the staging kernels
     std::vector<int32_t> perms;
     for (const auto &sc : h->scn) perms.insert(perms.end(), sc.perm.begin(), sc.perm.end());
@@ -1047,7 +1218,8 @@ int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     case 4: rc = go(flux_kernel<A, VARIANT, 256, 4, SEG>, 256, update_kernel<A, VARIANT, 8, SEG>); break;
     case 5: rc = go(flux_kernel<A, VARIANT, 128, 4, SEG>, 128, update_kernel<A, VARIANT, 6, SEG>); break;
     case 6: rc = go(flux_kernel<A, VARIANT, 256, 2, SEG>, 256, update_kernel<A, VARIANT, 6, SEG>); break;
-    default: rc = go(flux_kernel<A, VARIANT, 64, 12, SEG>, 64, update_kernel<A, VARIANT, 8, SEG>); break;
+    case 7: rc = go(flux_kernel<A, VARIANT, 64, 12, SEG>, 64, update_kernel<A, VARIANT, 8, SEG>); break;
+    default: return hb::set_error(HB_E_INVALID, "launch shape %d is not an edge-layout shape", h->launch_config + 1);
     }
     if (rc != HB_OK) return rc;
     hb::tick_kernel<<<1, 1, 0, st>>>(h->d_ctr, n);
@@ -1055,15 +1227,84 @@ int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     return HB_OK;
 }
 
+size_t tile_smem_bytes(int max_cells, int max_pairs, size_t real_size) {
+    return 16 * real_size * (size_t)max_cells + sizeof(int) * (size_t)max_pairs;
+}
+
+// Calls f(kernel, threads) with the tile kernel of a tile-layout launch shape.
+template <class A, int VARIANT, class F>
+int with_tile_kernel(int config, F &&f) {
+    using namespace hb;
+    switch (config) {
+    case 8: return f(tile_kernel<A, VARIANT, 256, 3>, 256);
+    case 9: return f(tile_kernel<A, VARIANT, 256, 2>, 256);
+    case 10: return f(tile_kernel<A, VARIANT, 128, 6>, 128);
+    case 11: return f(tile_kernel<A, VARIANT, 128, 4>, 128);
+    case 12: return f(tile_kernel<A, VARIANT, 512, 1>, 512);
+    default: return f(tile_kernel<A, VARIANT, 256, 4>, 256);
+    }
+}
+
+template <class A, int VARIANT>
+int launch_tiles_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)std::max(1, m.ntiles));
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.dynamicSmemBytes = tile_smem_bytes(m.max_tile_cells, m.max_tile_pairs, sizeof(typename A::real));
+    const int rc = with_tile_kernel<A, VARIANT>(h->launch_config, [&](auto kernel, int threads) -> int {
+        cfg.blockDim = dim3(threads);
+        for (int k = 0; k < n; k++) HB_CUDA_RET(cudaLaunchKernelEx(&cfg, kernel, m, k, (int)(k == n - 1)));
+        return HB_OK;
+    });
+    if (rc != HB_OK) return rc;
+    hb::tick_kernel<<<1, 1, 0, st>>>(h->d_ctr, n);
+    HB_CUDA_RET(cudaGetLastError());
+    return HB_OK;
+}
+
+// Lets every tile kernel of the handle's policy use the shared memory its
+// largest tile needs (beyond the 48 KB default).
+template <class A, int VARIANT>
+int set_tile_smem(const hb::DevMesh<A> &m) {
+    const size_t bytes = tile_smem_bytes(m.max_tile_cells, m.max_tile_pairs, sizeof(typename A::real));
+    for (int c = 0; c < hb::N_LAUNCH_CONFIGS; c++) {
+        if (hb::LAUNCH_CONFIGS[c].layout != hb::LAYOUT_TILE) continue;
+        const int rc = with_tile_kernel<A, VARIANT>(c, [&](auto kernel, int) -> int {
+            HB_CUDA_RET(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+            return HB_OK;
+        });
+        if (rc != HB_OK) return rc;
+    }
+    return HB_OK;
+}
+
 int enqueue_steps(hb_handle *h, int n, cudaStream_t st) {
     if (n <= 0) return HB_OK;
     const bool f = h->opt.variant == HB_VARIANT_F;
     const bool seg = h->segmented();
+    const bool tiles = h->opt.layout == HB_LAYOUT_TILE;
     return h->with_mesh([&](auto &m) {
         using A = typename std::remove_reference<decltype(m)>::type::Policy;
+        if (tiles) return f ? launch_tiles_t<A, 1>(h, m, n, st) : launch_tiles_t<A, 0>(h, m, n, st);
         if (seg) return f ? launch_steps_t<A, 1, true>(h, m, n, st) : launch_steps_t<A, 0, true>(h, m, n, st);
         return f ? launch_steps_t<A, 1, false>(h, m, n, st) : launch_steps_t<A, 0, false>(h, m, n, st);
     });
+}
+
+int default_config(int layout) {
+    return layout == HB_LAYOUT_TILE ? hb::DEFAULT_TILE_CONFIG : hb::DEFAULT_EDGE_CONFIG;
+}
+
+// launch shape index of tile_config (0 = the layout's default), or -1
+int config_for(int layout, int tile_config) {
+    if (tile_config == 0) return default_config(layout);
+    if (tile_config < 0 || tile_config > hb::N_LAUNCH_CONFIGS) return -1;
+    return hb::LAUNCH_CONFIGS[tile_config - 1].layout == layout ? tile_config - 1 : -1;
 }
 
 int check_range(hb_handle *h, long long n) {
@@ -1083,6 +1324,15 @@ int check_scenario(hb_handle *h, int s) {
 
 }  // namespace
 
+extern "C" int hb_launch_shapes(int32_t *layout, int32_t *threads, int32_t *min_blocks, int32_t capacity) {
+    for (int i = 0; i < hb::N_LAUNCH_CONFIGS && i < capacity; i++) {
+        if (layout) layout[i] = hb::LAUNCH_CONFIGS[i].layout;
+        if (threads) threads[i] = hb::LAUNCH_CONFIGS[i].threads;
+        if (min_blocks) min_blocks[i] = hb::LAUNCH_CONFIGS[i].min_blocks * 100 + hb::LAUNCH_CONFIGS[i].update_min_blocks;
+    }
+    return hb::N_LAUNCH_CONFIGS;
+}
+
 extern "C" int hb_tile_configs(int32_t *threads, int32_t *min_blocks, int32_t capacity) {
     for (int i = 0; i < hb::N_LAUNCH_CONFIGS && i < capacity; i++) {
         if (threads) threads[i] = hb::LAUNCH_CONFIGS[i].threads;
@@ -1098,21 +1348,30 @@ extern "C" int hb_create_batch(const hb_mesh_desc *meshes, int32_t n, const hb_o
     if (opt_in) opt = *opt_in; else hb_options_default(&opt);
     if (opt.precision != HB_FP64 && opt.precision != HB_FP32 && opt.precision != HB_SPLIT)
         return hb::set_error(HB_E_INVALID, "hb_create: precision %d not available on this path", opt.precision);
-    if (opt.tile_config < 0 || opt.tile_config > hb::N_LAUNCH_CONFIGS)
-        return hb::set_error(HB_E_INVALID, "hb_create: tile_config %d outside 0..%d", opt.tile_config, hb::N_LAUNCH_CONFIGS);
+    if (opt.layout != HB_LAYOUT_EDGE && opt.layout != HB_LAYOUT_TILE)
+        return hb::set_error(HB_E_INVALID, "hb_create: layout %d", opt.layout);
+    if (opt.tile_cells < 0 || opt.tile_cells > 1024)   // 5/4 x 1024 fp64 cells: 160 KB of shared memory
+        return hb::set_error(HB_E_INVALID, "hb_create: tile_cells %d outside 0..1024", opt.tile_cells);
+    if (config_for(opt.layout, opt.tile_config) < 0)
+        return hb::set_error(HB_E_INVALID, "hb_create: tile_config %d is no shape of layout %d", opt.tile_config, opt.layout);
     long long total = 0;
     for (int s = 0; s < n; s++) total += std::max(meshes[s].cells, 0);
     if (total > (1 << 29)) return hb::set_error(HB_E_TOO_LARGE, "hb_create: %lld cells", total);
     HB_CUDA_RET(cudaSetDevice(opt.device));
     auto h = new hb_handle();
     h->opt = opt;
-    h->launch_config = opt.tile_config == 0 ? hb::DEFAULT_LAUNCH_CONFIG : opt.tile_config - 1;
+    h->launch_config = config_for(opt.layout, opt.tile_config);
     int st;
     if ((st = dev_alloc(h, &h->d_err, 1)) != HB_OK || (st = dev_alloc(h, &h->d_ctr, 1)) != HB_OK) {
         delete h;
         return st;
     }
     st = h->with_mesh([&](auto &m) { return build_device_mesh(h, meshes, n, m); });
+    if (st == HB_OK && opt.layout == HB_LAYOUT_TILE)
+        st = h->with_mesh([&](auto &m) {
+            using A = typename std::remove_reference<decltype(m)>::type::Policy;
+            return opt.variant == HB_VARIANT_F ? set_tile_smem<A, 1>(m) : set_tile_smem<A, 0>(m);
+        });
     if (st != HB_OK) { delete h; return st; }
     *out = h;
     return HB_OK;
@@ -1388,9 +1647,8 @@ extern "C" int hb_get_permutation_at(hb_handle *h, int32_t s, int32_t *perm) {
 
 extern "C" int hb_set_tile_config(hb_handle *h, int32_t tile_config) {
     if (!h) return hb::set_error(HB_E_INVALID, "null handle");
-    if (tile_config < 0 || tile_config > hb::N_LAUNCH_CONFIGS)
-        return hb::set_error(HB_E_INVALID, "tile_config %d outside 0..%d", tile_config, hb::N_LAUNCH_CONFIGS);
-    const int c = tile_config == 0 ? hb::DEFAULT_LAUNCH_CONFIG : tile_config - 1;
+    const int c = config_for(h->opt.layout, tile_config);
+    if (c < 0) return hb::set_error(HB_E_INVALID, "tile_config %d is no shape of this handle's layout", tile_config);
     if (c != h->launch_config) h->drop_graph();
     h->launch_config = c;
     return HB_OK;
@@ -1448,7 +1706,10 @@ extern "C" int hb_autotune(hb_handle *h, int32_t steps, void *stream, float *ms_
         rc = hb::set_error(HB_E_CUDA, "hb_autotune: cudaEventCreate failed");
     int best_c = saved_config;
     float best_ms = 0.f;
+    bool first = true;
     for (int c = 0; rc == HB_OK && c < hb::N_LAUNCH_CONFIGS; c++) {
+        if (ms_per_step && c < capacity) ms_per_step[c] = 0.f;
+        if (hb::LAUNCH_CONFIGS[c].layout != h->opt.layout) continue;
         h->launch_config = c;
         if ((rc = copy_all(false)) != HB_OK) break;
         if ((rc = enqueue_steps(h, 1, st)) != HB_OK) break;
@@ -1462,7 +1723,7 @@ extern "C" int hb_autotune(hb_handle *h, int32_t steps, void *stream, float *ms_
         cudaEventElapsedTime(&ms, e0, e1);
         ms /= (float)steps;
         if (ms_per_step && c < capacity) ms_per_step[c] = ms;
-        if (c == 0 || ms < best_ms) { best_ms = ms; best_c = c; }
+        if (first || ms < best_ms) { best_ms = ms; best_c = c; first = false; }
     }
     if (rc == HB_OK) rc = copy_all(false);
     cudaStreamSynchronize(st);

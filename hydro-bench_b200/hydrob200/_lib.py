@@ -14,6 +14,7 @@ STATUS = {0: "HB_OK", 1: "HB_E_INVALID", 2: "HB_E_BADMESH", 3: "HB_E_CUDA", 4: "
 VARIANT_H, VARIANT_F = 0, 1
 REF_STEP_STATIC_MAX_CELLS = 65536   # HB_REF_STEP_STATIC_MAX_CELLS
 FP64, FP32, SPLIT = 0, 1, 2
+LAYOUT_EDGE, LAYOUT_TILE = 0, 1
 
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
@@ -36,7 +37,8 @@ class MeshDesc(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("variant", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32), ("renumber", C.c_int32),
-                ("tile_config", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("tile_config", C.c_int32), ("layout", C.c_int32), ("tile_cells", C.c_int32),
+                ("reserved", C.c_int32 * 1)]
 
 
 def _view_types(real):
@@ -79,6 +81,7 @@ def lib():
     sig = {
         "hb_options_default": (None, [C.POINTER(Options)]),
         "hb_tile_configs": (C.c_int, [_ip, _ip, C.c_int32]),
+        "hb_launch_shapes": (C.c_int, [_ip, _ip, _ip, C.c_int32]),
         "hb_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(Options), C.POINTER(vp)]),
         "hb_destroy": (C.c_int, [vp]),
         "hb_create_batch": (C.c_int, [C.POINTER(MeshDesc), C.c_int32, C.POINTER(Options), C.POINTER(vp)]),
@@ -135,7 +138,7 @@ def check(status: int) -> None:
 
 
 # every symbol the C headers declare (checked by the CPU tests)
-EXPORTED = ["hb_options_default", "hb_tile_configs", "hb_create", "hb_destroy", "hb_set_state", "hb_get_state", "hb_get_flux",
+EXPORTED = ["hb_options_default", "hb_tile_configs", "hb_launch_shapes", "hb_create", "hb_destroy", "hb_set_state", "hb_get_state", "hb_get_flux",
             "hb_get_klas", "hb_step", "hb_sync", "hb_position", "hb_set_position", "hb_step_host", "hb_capture_graph",
             "hb_graph_launch", "hb_device_state", "hb_get_permutation", "hb_device_errors", "hb_last_error",
             "hb_last_error_string", "hb_status_string", "hb_deck_load", "hb_deck_mesh", "hb_deck_state",

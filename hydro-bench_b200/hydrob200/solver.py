@@ -18,6 +18,31 @@ from ._lib import check, lib, HydroError, VARIANT_H, VARIANT_F, FP64, FP32, SPLI
 
 _VARIANTS = {"H": VARIANT_H, "F": VARIANT_F, VARIANT_H: VARIANT_H, VARIANT_F: VARIANT_F}
 _PRECISIONS = {"fp64": FP64, "fp32": FP32, "split": SPLIT, FP64: FP64, FP32: FP32, SPLIT: SPLIT}
+_LAYOUTS = {"edge": _lib.LAYOUT_EDGE, "tile": _lib.LAYOUT_TILE, _lib.LAYOUT_EDGE: _lib.LAYOUT_EDGE,
+            _lib.LAYOUT_TILE: _lib.LAYOUT_TILE}
+
+
+def launch_shapes():
+    """The compiled launch shapes (hb_launch_shapes): tile_config -> layout, threads, CTAs per SM."""
+    n = lib().hb_launch_shapes(None, None, None, 0)
+    lay, thr, mb = (C.c_int32 * n)(), (C.c_int32 * n)(), (C.c_int32 * n)()
+    lib().hb_launch_shapes(lay, thr, mb, n)
+    names = {_lib.LAYOUT_EDGE: "edge", _lib.LAYOUT_TILE: "tile"}
+    return {i + 1: dict(layout=names[lay[i]], threads=thr[i], min_blocks=mb[i] // 100, update_min_blocks=mb[i] % 100)
+            for i in range(n)}
+
+
+def _options(variant, precision, device, renumber, tile_config, layout, tile_cells):
+    opt = _lib.Options()
+    lib().hb_options_default(C.byref(opt))
+    opt.variant = _VARIANTS[variant]
+    opt.precision = _PRECISIONS[precision]
+    opt.device = device
+    opt.renumber = 1 if renumber else 0
+    opt.tile_config = int(tile_config)
+    opt.layout = _LAYOUTS[layout]
+    opt.tile_cells = int(tile_cells)
+    return opt
 
 CELL_ARRAYS = ("zbc", "zb1", "area", "fnc", "bfeat")
 SLOT_ARRAYS = ("nac", "klas", "side", "cosf", "sinf", "slcos", "slsin")
@@ -78,15 +103,10 @@ class Solver:
     """
 
     def __init__(self, deck: Deck, variant="H", precision="fp64", device: int = 0, renumber: bool = True,
-                 init_state: bool = True, tile_config: int = 0):
+                 init_state: bool = True, tile_config: int = 0, layout="edge", tile_cells: int = 0):
         self.deck = deck   # keeps the host arrays alive
-        opt = _lib.Options()
-        lib().hb_options_default(C.byref(opt))
-        opt.variant = _VARIANTS[variant]
-        opt.precision = _PRECISIONS[precision]
-        opt.device = device
-        opt.renumber = 1 if renumber else 0
-        opt.tile_config = int(tile_config)
+        opt = _options(variant, precision, device, renumber, tile_config, layout, tile_cells)
+        self.layout = opt.layout
         self.variant = opt.variant
         self.precision = opt.precision
         self._h = C.c_void_p()
@@ -177,14 +197,20 @@ class Solver:
     def tile_config(self, cfg: int) -> None:
         check(lib().hb_set_tile_config(self._h, int(cfg)))
 
+    def shapes(self):
+        """tile_config values of this handle's layout."""
+        names = {_lib.LAYOUT_EDGE: "edge", _lib.LAYOUT_TILE: "tile"}
+        return [k for k, v in launch_shapes().items() if v["layout"] == names[self.layout]]
+
     def autotune(self, steps: int = 20, stream=None):
-        """hb_autotune: times every launch shape on this handle's mesh(es) and
-        keeps the fastest; returns (best tile_config, ms per step by config)."""
+        """hb_autotune: times every launch shape of this handle's layout on its
+        mesh(es) and keeps the fastest; returns (best tile_config, ms per step
+        by tile_config)."""
         n = lib().hb_tile_configs(None, None, 0)
         ms = (C.c_float * n)()
         best = C.c_int32()
         check(lib().hb_autotune(self._h, int(steps), _stream_handle(stream), ms, n, C.byref(best)))
-        return best.value, {i + 1: float(ms[i]) for i in range(n)}
+        return best.value, {k: float(ms[k - 1]) for k in self.shapes()}
 
     def permutation(self) -> np.ndarray:
         p = np.empty(self.cells, dtype=np.int32)
@@ -218,15 +244,11 @@ class Batch(Solver):
     """
 
     def __init__(self, decks: Sequence[Deck], variant="H", precision="fp64", device: int = 0,
-                 renumber: bool = True, init_state: bool = True, tile_config: int = 0):
+                 renumber: bool = True, init_state: bool = True, tile_config: int = 0, layout="edge",
+                 tile_cells: int = 0):
         self.decks = list(decks)   # keeps the host arrays alive
-        opt = _lib.Options()
-        lib().hb_options_default(C.byref(opt))
-        opt.variant = _VARIANTS[variant]
-        opt.precision = _PRECISIONS[precision]
-        opt.device = device
-        opt.renumber = 1 if renumber else 0
-        opt.tile_config = int(tile_config)
+        opt = _options(variant, precision, device, renumber, tile_config, layout, tile_cells)
+        self.layout = opt.layout
         self.variant = opt.variant
         self.precision = opt.precision
         meshes = (_lib.MeshDesc * len(self.decks))(*[d.mesh for d in self.decks])

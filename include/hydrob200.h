@@ -44,6 +44,13 @@ typedef enum { HB_VARIANT_H = 0, HB_VARIANT_F = 1 } hb_variant;
  * cell's depth update is Kahan-compensated.  Its device state is the fp32
  * quadruple {H, U, V, H_lo} (no Z; hb_get_state rebuilds Z in fp64). */
 typedef enum { HB_FP64 = 0, HB_FP32 = 1, HB_SPLIT = 2 } hb_precision;
+/* HB_LAYOUT_EDGE: two kernels per step, one thread per flux record then one
+ * per cell, with the slots' terms of the cell sums passed through device
+ * memory.  HB_LAYOUT_TILE: one kernel per step; the cells are grouped into
+ * compact tiles of about tile_cells cells, and one CTA computes every flux of
+ * its tile into shared memory and updates the tile's cells.  Both give the
+ * same bits. */
+typedef enum { HB_LAYOUT_EDGE = 0, HB_LAYOUT_TILE = 1 } hb_layout;
 
 /* Host description of a mesh and its boundary tables, reference layout.
  * Mirrors what MeshView/CellView/SideView hold after FromHost
@@ -70,13 +77,18 @@ typedef struct hb_options {
     int32_t precision;        /* hb_precision */
     int32_t device;           /* CUDA device ordinal */
     int32_t renumber;         /* 1: reverse Cuthill-McKee cell order on the device (default), 0: input order */
-    int32_t tile_config;      /* step-kernel tile shape: 0 = default, k > 0 = entry k-1 of hb_tile_configs() */
-    int32_t reserved[3];
+    int32_t tile_config;      /* launch shape: 0 = the layout's default, k > 0 = entry k-1 of hb_launch_shapes() */
+    int32_t layout;           /* hb_layout */
+    int32_t tile_cells;       /* HB_LAYOUT_TILE: cells per tile, <= 1024 (0 = 256); tiles hold up to 5*tile_cells/4 */
+    int32_t reserved[1];
 } hb_options;
 
-/* The compiled launch shapes of the flux kernel: threads per CTA, and
- * 100 * (flux CTAs per SM) + (cell-update CTAs per SM) asked of the compiler;
- * returns how many there are (hb_options.tile_config = index + 1). */
+/* The compiled launch shapes: the layout each runs, threads per CTA, and
+ * 100 * (flux or tile CTAs per SM) + (cell-update CTAs per SM, edge layout)
+ * asked of the compiler; returns how many there are (tile_config = index + 1).
+ * A handle takes only shapes of its own layout. */
+int hb_launch_shapes(int32_t *layout, int32_t *threads, int32_t *min_blocks, int32_t capacity);
+/* hb_launch_shapes without the layouts. */
 int hb_tile_configs(int32_t *threads, int32_t *min_blocks, int32_t capacity);
 
 /* Default options: variant H, fp64, device 0, renumbered. */

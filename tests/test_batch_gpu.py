@@ -28,11 +28,12 @@ def _run_single(deck, steps, **kw):
     return s.get_state(), s.flux(), s.klas()
 
 
+@pytest.mark.parametrize("layout", ["edge", "tile"])
 @pytest.mark.parametrize("precision,variant", [("fp64", "H"), ("fp64", "F"), ("split", "H"), ("fp32", "H")])
-def test_batch_equals_single_handles(deck_dir, precision, variant):
+def test_batch_equals_single_handles(deck_dir, precision, variant, layout):
     decks = [hb.Deck(deck_dir[n]) for n in NAMES]
     steps = 1   # breach has tables for one step
-    b = hb.Batch(decks, precision=precision, variant=variant)
+    b = hb.Batch(decks, precision=precision, variant=variant, layout=layout, tile_cells=64)
     assert len(b) == len(decks)
     b.step(steps)
     b.sync()
@@ -53,9 +54,8 @@ def test_batch_many_steps_and_shapes(deck_dir, precision):
     names = ["stress_a", "f1", "stress_b", "probe"]
     decks = [hb.Deck(deck_dir[n]) for n in names]
     ref = [_run_single(d, 50, precision=precision)[0] for d in decks]
-    n = hb._lib.lib().hb_tile_configs(None, None, 0)
-    for cfg in range(1, n + 1):
-        b = hb.Batch(decks, precision=precision, tile_config=cfg)
+    for cfg, shape in hb.launch_shapes().items():
+        b = hb.Batch(decks, precision=precision, tile_config=cfg, layout=shape["layout"], tile_cells=96)
         if cfg % 2:
             b.step(50)
         else:
@@ -70,14 +70,15 @@ def test_batch_many_steps_and_shapes(deck_dir, precision):
         b.close()
 
 
-def test_autotune_leaves_state_and_picks_a_shape(deck_dir):
+@pytest.mark.parametrize("layout", ["edge", "tile"])
+def test_autotune_leaves_state_and_picks_a_shape(deck_dir, layout):
     decks = [hb.Deck(deck_dir[n]) for n in ["stress_a", "f1", "stress_b"]]
-    a = hb.Batch(decks, precision="split")
-    b = hb.Batch(decks, precision="split")
+    a = hb.Batch(decks, precision="split", layout=layout)
+    b = hb.Batch(decks, precision="split", layout=layout)
     a.step(5)
     b.step(5)
     best, ms = a.autotune(steps=10)
-    assert best == a.tile_config and 1 <= best <= len(ms)
+    assert best == a.tile_config and best in ms and set(ms) == set(a.shapes())
     assert all(v > 0 for v in ms.values())
     assert a.position == b.position
     a.step(20)
@@ -100,3 +101,5 @@ def test_batch_arguments(deck_dir):
         b.step_host(*[np.zeros(decks[0].cells) for _ in range(5)], n=1)
     with pytest.raises(hb.HydroError):
         b.tile_config = 99
+    with pytest.raises(hb.HydroError):   # a tile-layout shape on an edge-layout handle
+        b.tile_config = next(k for k, v in hb.launch_shapes().items() if v["layout"] == "tile")

@@ -46,10 +46,11 @@ def _fp64_cases():
                 yield name, b
 
 
+@pytest.mark.parametrize("layout,tile_cells", [("edge", 0), ("tile", 0), ("tile", 64)])
 @pytest.mark.parametrize("name,binary", list(_fp64_cases()))
-def test_handle_path_bit_exact(deck_dir, name, binary):
+def test_handle_path_bit_exact(deck_dir, name, binary, layout, tile_cells):
     deck = hb.Deck(deck_dir[name])
-    s = hb.Solver(deck, variant="H" if binary == "h64" else "F")
+    s = hb.Solver(deck, variant="H" if binary == "h64" else "F", layout=layout, tile_cells=tile_cells)
     done = 0
     for steps in DECKS[name]["steps"]:
         s.step(steps - done)
