@@ -24,7 +24,7 @@ CPP_SOURCES = ["hb_deck.cpp"]
 
 def _sources():
     srcs = [os.path.join(CSRC, f) for f in CU_SOURCES + CPP_SOURCES]
-    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h", ".hpp"))]
     deps += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
     return srcs, deps
 

@@ -1,0 +1,552 @@
+// hb_step.cuh -- device side of the handle path: the device mesh, the step
+// kernels of both layouts, and the staging and setup kernels.  Shared by
+// hb_solver.cu (the forward step) and hb_adjoint.cu (the reverse step).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+#include "hb_common.cuh"
+#include "hb_physics.cuh"
+#include "hydrob200.h"
+
+namespace hb {
+
+// ---------------------------------------------------------------------------
+// device mesh
+// ---------------------------------------------------------------------------
+enum : uint8_t { META_CODE = 0x0F, META_OWN_FIRST = 0x10, META_HAS_NB = 0x20 };
+
+// Launch shapes.  Edge layout: the flux kernel's threads per CTA and CTAs per
+// SM asked of the compiler through __launch_bounds__ (which caps registers
+// per thread), and the cell kernel's CTAs per SM (it has UPDATE_THREADS
+// threads).  Tile layout: the tile kernel's threads per CTA and CTAs per SM.
+enum Layout : int { LAYOUT_EDGE = HB_LAYOUT_EDGE, LAYOUT_TILE = HB_LAYOUT_TILE };
+struct LaunchConfig { int layout, threads, min_blocks, update_min_blocks; };
+constexpr LaunchConfig LAUNCH_CONFIGS[] = {
+    {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 8}, {LAYOUT_EDGE, 128, 8, 8}, {LAYOUT_EDGE, 256, 3, 6},
+    {LAYOUT_EDGE, 256, 4, 8}, {LAYOUT_EDGE, 128, 4, 6}, {LAYOUT_EDGE, 256, 2, 6}, {LAYOUT_EDGE, 64, 12, 8},
+    {LAYOUT_TILE, 256, 3, 0}, {LAYOUT_TILE, 256, 2, 0}, {LAYOUT_TILE, 128, 6, 0}, {LAYOUT_TILE, 128, 4, 0},
+    {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0}};
+constexpr int N_LAUNCH_CONFIGS = sizeof(LAUNCH_CONFIGS) / sizeof(LAUNCH_CONFIGS[0]);
+constexpr int DEFAULT_EDGE_CONFIG = 0;
+constexpr int DEFAULT_TILE_CONFIG = 8;
+constexpr int UPDATE_THREADS = 128;
+
+// One tile of the tile layout: a compact group of cells, contiguous in the
+// device order, with its records (mirror pairs inside the tile, then every
+// other real slot of its cells).
+struct TileDesc { int scn, cell0, cells, rec0, npairs, nsingles; };
+
+// Constants of one scenario of a batch (the only entry for a single mesh).
+struct ScnParams {
+    double hm1, hm2, jl, dt;
+    int per_day, ndays;        // steps per table interval; intervals in the tables
+    int cell0, cells;          // the scenario's cells in the device order
+};
+
+// Device mesh.  Cells are in reverse Cuthill-McKee order.  The flux work is a
+// list of records: first the interior edges whose two slots both have code 0
+// and mirror each other exactly (reciprocal neighbours, negated normal, same
+// length), then every other real slot on its own.  The zero-length fourth slot
+// of a triangle is no record; the cell update evaluates it.
+template <class A>
+struct DevMesh {
+    using Policy = A;
+    using R = typename A::real;
+    using L = typename A::level;
+    int C;                     // cells
+    int per_day;               // steps per table interval (steps_per_day - 1)
+    int ndays, nb, nhq;
+    int npairs, nrecords;
+    double hm1, hm2, jl, dt;
+    R *S[2];                   // [C][4] state {H, U, V, Z}, split precision {H, U, V, H_lo};
+                               // a step reads S[step & 1], writes the other
+    R *W;
+    const L *zbc;
+    const R *fnc, *dta;        // dta: DT/AREA (variant H) or AREA (variant F)
+    const R *sidex;            // variant F CFL length
+    const int32_t *bcell;      // [C] row of the boundary tables, -1 = none
+    const uint8_t *cmask;      // [C] bit j: slot j is a real slot
+    R *slotw;                  // [4C][4] per-slot terms of the cell sums {F0, dWU, dWV, SIDE}
+    // records [nrecords]
+    const int4 *rix;           // {a, b, sa, sb}: cell of the slot, its neighbour (-1 = none),
+                               // slot 4*a+j, and for a pair the slot of b (-1 otherwise)
+    uint8_t *rmeta;            // code | own_first | has_nb of slot a (code changes on breach)
+    const R *rgeo;             // [nrecords][4] {COSF, SINF, SIDE, 0} of slot a
+    R *f0, *f1, *f2, *f3;      // [4C] fluxes of the last step, index 4*cell + j
+    const R *bqt, *bdqt;       // [ndays*nb]
+    const L *bzt, *bdzt;       // [ndays*nb]
+    const L *btop;             // [nb]
+    const int32_t *bnhq1;      // [nb]
+    const L *bzw;              // [nb*nhq]; one extra zero row at index nb
+    const R *bqw;              // [nb*nhq]; one extra zero row at index nb
+    uint32_t *err;
+    const long long *step_ctr;
+    // batches: per-CTA segment tables, one scenario per CTA
+    int nscen;
+    const ScnParams *scn;      // [nscen]
+    const int4 *fseg;          // flux CTAs {scenario, first record, records, 1 = mirror pairs}
+    const int4 *useg;          // update CTAs {scenario, first cell, cells, 0}
+    // tile layout
+    const TileDesc *tiles;     // [ntiles]
+    int ntiles, max_tile_cells, max_tile_pairs;
+};
+
+struct StepIndex { int par, kt, jt; };
+
+template <class A>
+__device__ __forceinline__ StepIndex step_index(const DevMesh<A> &m, int k, int per_day, int ndays) {
+    const long long step = *m.step_ctr + k;
+    StepIndex si;
+    si.par = (int)(step & 1);
+    si.jt = (int)(step / per_day);
+    si.kt = 1 + (int)(step % per_day);
+    if (si.jt >= ndays) {   // beyond the boundary tables: never read past them
+        if (threadIdx.x == 0) atomicOr(m.err, ERRBIT_TABLE_RANGE);
+        si.jt = ndays - 1;
+    }
+    return si;
+}
+
+template <class R> struct Vec4 { R x, y, z, w; };
+__device__ __forceinline__ Vec4<double> ld4(const double *p) {
+    const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+    return {a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ Vec4<float> ld4(const float *p) {
+    const float4 a = *reinterpret_cast<const float4 *>(p);
+    return {a.x, a.y, a.z, a.w};
+}
+__device__ __forceinline__ void st4(double *p, double x, double y, double z, double w) {
+    *reinterpret_cast<double2 *>(p) = make_double2(x, y);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2(z, w);
+}
+__device__ __forceinline__ void st4(float *p, float x, float y, float z, float w) {
+    *reinterpret_cast<float4 *>(p) = make_float4(x, y, z, w);
+}
+
+template <class A>
+__device__ __forceinline__ CellStateA<A> load_cell(const DevMesh<A> &m, int par, int c) {
+    const Vec4<typename A::real> v = ld4(m.S[par] + 4 * (size_t)c);
+    const typename A::level zbc = m.zbc[c];
+    if constexpr (is_split<A>::value) return {v.x, v.y, v.z, split_level<A>(v.x, v.w, zbc), zbc};
+    else return {v.x, v.y, v.z, v.w, zbc};
+}
+
+// Where a step keeps the slots' terms of the cell sums between the flux and
+// the update: slot s at p + 4 * (s - slot0).  Global memory (m.slotw, slot0 =
+// 0) between the two kernels of the edge layout; shared memory (slot0 = the
+// tile's first slot) inside the tile kernel.
+template <class R>
+struct Terms { R *p; int slot0; };
+
+// the slot's terms of the cell sums (functors.cu:733-741): F0 and SIDE for
+// WH = fma(SIDE, F0, WH), and the complete WU / WV increments
+template <class A>
+__device__ __forceinline__ void store_terms(const Terms<typename A::real> &t, int s, const typename A::real f[4],
+                                            typename A::real side, typename A::real cs, typename A::real sn) {
+    using R = typename A::real;
+    const R fr1 = A::add(f[1], f[3]);
+    const R slcos = A::mul(side, cs), slsin = A::mul(side, sn);
+    const R dwu = A::dot(slcos, fr1, -slsin, f[2], M_WU);
+    const R dwv = A::dot(slsin, fr1, slcos, f[2], M_WV);
+    st4(t.p + 4 * (size_t)(s - t.slot0), f[0], dwu, dwv, side);
+}
+
+template <class A>
+__device__ __forceinline__ void store_flux(const DevMesh<A> &m, int s, const typename A::real f[4]) {
+    m.f0[s] = f[0]; m.f1[s] = f[1]; m.f2[s] = f[2]; m.f3[s] = f[3];
+}
+
+// One slot on its own: flux_slot with its boundary tables (functors.cu:47-202).
+template <class A, int VARIANT>
+__device__ __forceinline__ void single_record(const DevMesh<A> &m, int r, const StepIndex &si,
+                                              const StepParams &p, int write_flux, const Terms<typename A::real> &tout) {
+    using R = typename A::real;
+    const int4 ix = m.rix[r];
+    const int a = ix.x, b = ix.y, sa = ix.z;
+    const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
+    using L = typename A::level;
+    SlotInA<A> in;
+    in.own = load_cell(m, si.par, a);
+    const uint8_t meta = m.rmeta[r];
+    in.code = (int8_t)(meta & META_CODE);
+    in.own_first = meta & META_OWN_FIRST;
+    in.has_nb = meta & META_HAS_NB;
+    in.nb = in.has_nb ? load_cell(m, si.par, b) : CellStateA<A>{R(0), R(0), R(0), L(0), L(0)};
+    in.cosj = g.x; in.sinj = g.y; in.side = g.z;
+    auto fetch = [&]() {
+        BoundaryInA<A> bi;
+        const int row = m.bcell[a];
+        if (row >= 0) {
+            const size_t q = (size_t)si.jt * m.nb + row;
+            bi.qt = m.bqt[q]; bi.dqt = m.bdqt[q]; bi.zt = m.bzt[q]; bi.dzt = m.bdzt[q];
+            bi.top = m.btop[row]; bi.nhq1 = m.bnhq1[row];
+            bi.zw = m.bzw + (size_t)row * m.nhq; bi.qw = m.bqw + (size_t)row * m.nhq;
+        } else {
+            bi.qt = bi.dqt = R(0); bi.zt = bi.dzt = bi.top = L(0); bi.nhq1 = 0;
+            bi.zw = m.bzw + (size_t)m.nb * m.nhq; bi.qw = m.bqw + (size_t)m.nb * m.nhq;
+        }
+        bi.nhq = m.nhq;
+        return bi;
+    };
+    const R cl = A::sqrt(A::mul(A::c(9.81), in.own.h));
+    SlotOut<R> o;
+    flux_slot<A, VARIANT>(in, cl, p, fetch, o);
+    if (o.mask != 0xF) {   // codes that leave fluxes unwritten keep the old values (functors.cu:525-565)
+        if (!(o.mask & 1)) o.f[0] = m.f0[sa];
+        if (!(o.mask & 2)) o.f[1] = m.f1[sa];
+        if (!(o.mask & 4)) o.f[2] = m.f2[sa];
+        if (!(o.mask & 8)) o.f[3] = m.f3[sa];
+    }
+    if (write_flux || o.mask != 0xF) store_flux(m, sa, o.f);
+    store_terms<A>(tout, sa, o.f, in.side, in.cosj, in.sinj);
+    if (o.klas_to_zero) m.rmeta[r] = (uint8_t)((meta & ~META_CODE) | CODE_ZERO);
+    if (o.undefined) atomicOr(m.err, ERRBIT_UNDEFINED);
+}
+
+// The mirrored Osher of a pair computed on its own (when its inputs differ
+// from the direct route's in the normal velocity).
+template <class A>
+__device__ __forceinline__ void pair_mirror(const DevMesh<A> &m, int r, const StepIndex &si,
+                                            const StepParams &p, int write_flux, const Terms<typename A::real> &tout) {
+    using R = typename A::real;
+    const int4 ix = m.rix[r];
+    const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
+    const CellStateA<A> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
+    const R cs = g.x, sn = g.y;
+    const R clA = A::sqrt(A::mul(A::c(9.81), A_.h));
+    const OsherIn<R> oi = osher_inputs<A>(A_, B_, cs, sn, clA, true, p);
+    R fo[4], fb[4];
+    osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo);
+    fb[0] = -fo[0];
+    fb[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, oi.ur);
+    fb[2] = fo[2];
+    fb[3] = mirror_f3<A>(fo[3], A_.zbc, B_.zbc);
+    if (write_flux) store_flux(m, ix.w, fb);
+    store_terms<A>(tout, ix.w, fb, g.z, -cs, -sn);
+}
+
+template <class R>
+__device__ __forceinline__ bool same_bits(R a, R b) {
+    if constexpr (sizeof(R) == 8) return __double_as_longlong((double)a) == __double_as_longlong((double)b);
+    else return __float_as_int((float)a) == __float_as_int((float)b);
+}
+
+// One mirror-pair record.  It evaluates both slots' branch chains
+// (functors.cu:98-150) and, when both reach Osher, runs it once: the direct
+// route at a and the mirrored route at b have the same cells, normal and
+// inputs except two rotations that the reference build rounds differently.
+// When those agree bit for bit the two Osher evaluations are identical, and
+// the b side's FLUX2 is re-summed with its own tangent if only that differs;
+// otherwise the pair goes to the CTA's queue, whose mirrored Osher
+// evaluations run together after the main pass (pair_mirror).
+template <class A, int VARIANT>
+__device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const StepIndex &si, const StepParams &p,
+                                            int write_flux, const Terms<typename A::real> &tout, int *queue, int *qn) {
+    using R = typename A::real;
+    const int4 ix = m.rix[r];
+    const Vec4<R> g = ld4(m.rgeo + 4 * (size_t)r);
+    const CellStateA<A> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
+    const R cs = g.x, sn = g.y;
+    const R clA = A::sqrt(A::mul(A::c(9.81), A_.h));
+    auto nofetch = []() { return BoundaryInA<A>{}; };
+    SlotInA<A> ia, ib;
+    ia.own = A_; ia.nb = B_; ia.has_nb = true; ia.own_first = true; ia.code = CODE_ZERO;
+    ia.cosj = cs; ia.sinj = sn; ia.side = g.z;
+    ib.own = B_; ib.nb = A_; ib.has_nb = true; ib.own_first = false; ib.code = CODE_ZERO;
+    ib.cosj = -cs; ib.sinj = -sn; ib.side = ia.side;
+    // each side's branch chain; a side whose fluxes are final is written at once
+    int ra_, rb_;
+    {
+        SlotOut<R> oa;
+        ra_ = flux_chain<A, VARIANT>(ia, clA, p, nofetch, oa);   // 0 or 1 (direct)
+        if (!ra_) {
+            if (write_flux) store_flux(m, ix.z, oa.f);
+            store_terms<A>(tout, ix.z, oa.f, g.z, cs, sn);
+        }
+    }
+    {
+        SlotOut<R> ob;
+        rb_ = flux_chain<A, VARIANT>(ib, R(0), p, nofetch, ob);  // 0 or 2 (mirrored)
+        if (!rb_) {
+            if (write_flux) store_flux(m, ix.w, ob.f);
+            store_terms<A>(tout, ix.w, ob.f, g.z, -cs, -sn);
+        }
+    }
+    if (ra_ | rb_) {
+        // the two routes' inputs differ only in QL2, UR and so QR1 (osher_inputs)
+        OsherIn<R> oi = osher_inputs<A>(A_, B_, cs, sn, clA, ra_ == 0, p);
+        const R ql2_d = oi.ql[2], ur_d = oi.ur, qr1_d = oi.qr[1];
+        const R ql2_m = ra_ ? A::dot(A_.v, cs, -A_.u, sn, M_QL2M) : ql2_d;
+        const R ur_m = ra_ ? A::dot(B_.u, cs, B_.v, sn, M_UR1) : ur_d;
+        R qr1_m = A::mul(ur_m, oi.ratio);
+        if (oi.hcR <= A::c(p.hm2) || oi.qr[0] <= A::c(p.hm2)) qr1_m = A::copysign(A::c(K::VMIN), ur_m);
+        R fo[4];
+        OsherTrace<R> tr;
+        osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo, &tr);
+        if (ra_) {
+            R f[4];
+            f[0] = fo[0];
+            f[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, ur_d);
+            f[2] = fo[2];
+            f[3] = fo[3];
+            if (write_flux) store_flux(m, ix.z, f);
+            store_terms<A>(tout, ix.z, f, g.z, cs, sn);
+        }
+        if (rb_) {
+            if (!ra_ || same_bits(qr1_d, qr1_m)) {
+                R f[4];
+                f[0] = -fo[0];
+                f[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, ur_m);
+                f[2] = (!ra_ || same_bits(ql2_d, ql2_m)) ? fo[2] : osher_f2<A>(tr, ql2_m, oi.qr[2]);
+                f[3] = mirror_f3<A>(fo[3], A_.zbc, B_.zbc);
+                if (write_flux) store_flux(m, ix.w, f);
+                store_terms<A>(tout, ix.w, f, g.z, -cs, -sn);
+            } else {
+                queue[atomicAdd(qn, 1)] = r;
+            }
+        }
+    }
+}
+
+// Flux of every record of one step.  Single mesh (SEG = false): records
+// [0, npairs) are mirror pairs and the rest single slots, one per thread.
+// Batch (SEG = true): CTA b takes the scenario and record range of fseg[b].
+template <class A, int VARIANT, int THREADS, int MINB, bool SEG>
+__global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k, int write_flux) {
+    __shared__ int queue[THREADS];
+    __shared__ int qn;
+    if (threadIdx.x == 0) qn = 0;
+    int r;
+    bool valid, pair;
+    StepIndex si;
+    StepParams p;
+    if constexpr (SEG) {
+        const int4 d = m.fseg[blockIdx.x];   // constant tables: read before the dependency wait
+        const ScnParams sp = m.scn[d.x];
+        cudaGridDependencySynchronize();
+        cudaTriggerProgrammaticLaunchCompletion();
+        si = step_index(m, k, sp.per_day, sp.ndays);
+        p = StepParams{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
+        r = d.y + (int)threadIdx.x;
+        valid = (int)threadIdx.x < d.z;
+        pair = d.w != 0;
+    } else {
+        cudaGridDependencySynchronize();
+        cudaTriggerProgrammaticLaunchCompletion();
+        si = step_index(m, k, m.per_day, m.ndays);
+        p = StepParams{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
+        r = blockIdx.x * THREADS + threadIdx.x;
+        valid = r < m.nrecords;
+        pair = r < m.npairs;
+    }
+    __syncthreads();
+    const Terms<typename A::real> tout{m.slotw, 0};
+    if (valid) {
+        if (pair) pair_record<A, VARIANT>(m, r, si, p, write_flux, tout, queue, &qn);
+        else single_record<A, VARIANT>(m, r, si, p, write_flux, tout);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < qn; i += THREADS) pair_mirror<A>(m, queue[i], si, p, write_flux, tout);
+}
+
+// Sums and update of one cell (UpdateCellKernel, functors.cu:717-784).  The
+// zero-length fourth slot of a triangle is evaluated here without pow
+// (flux_slot's ZERO_LEN), exactly when fluxes are written out.
+template <class A, int VARIANT>
+__device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const StepIndex &si, const StepParams &p,
+                                           int write_flux, const typename A::real *terms) {
+    using R = typename A::real;
+    using L = typename A::level;
+    const Vec4<R> raw = ld4(m.S[si.par] + 4 * (size_t)c);
+    CellStateA<A> st;
+    st.h = raw.x; st.u = raw.y; st.v = raw.z; st.zbc = m.zbc[c];
+    if constexpr (is_split<A>::value) st.z = split_level<A>(raw.x, raw.w, st.zbc);
+    else st.z = raw.w;
+    const unsigned mask = m.cmask[c];
+    const R fnc = m.fnc[c], dta = m.dta[c], sidex = VARIANT == 1 ? m.sidex[c] : R(0);
+    Vec4<R> t[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) t[j] = ld4(terms + 4 * j);
+    R wh = R(0), wu = R(0), wv = R(0);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int s = 4 * c + j;
+        if (mask & (1u << j)) {
+            // F0 and SIDE for WH; the WU/WV increments were formed by the flux kernel
+            wh = A::madd(t[j].w, t[j].x, wh, M_WH);
+            wu = A::add(wu, t[j].y);
+            wv = A::add(wv, t[j].z);
+        } else {
+            SlotInA<A> in;
+            in.own = st;
+            in.nb = {R(0), R(0), R(0), L(0), L(0)};
+            in.has_nb = false; in.own_first = false; in.code = CODE_ZERO;
+            in.cosj = R(0); in.sinj = R(0); in.side = R(0);
+            auto nofetch = []() { return BoundaryInA<A>{}; };
+            SlotOut<R> o;
+            if (write_flux) {
+                flux_slot<A, VARIANT, decltype(nofetch), false>(in, A::sqrt(A::mul(A::c(9.81), st.h)), p, nofetch, o);
+                store_flux(m, s, o.f);
+            } else {
+                flux_chain<A, VARIANT, decltype(nofetch), true>(in, R(0), p, nofetch, o);
+            }
+            // zero-length slot: SIDE = SLCOS = SLSIN = 0 (mesh.cpp:293-306, :347-370)
+            wsum_add<A>(wh, wu, wv, o.f[0], o.f[1], o.f[2], o.f[3], R(0), R(0), R(0));
+        }
+    }
+    CellUpdateIn<R, L> ci;
+    ci.h = st.h; ci.u = st.u; ci.v = st.v; ci.zbc = st.zbc;
+    ci.hlo = is_split<A>::value ? raw.w : R(0);
+    ci.fnc = fnc;
+    ci.dta_or_area = dta;
+    ci.sidex = sidex;
+    CellUpdateOut<R, L> o = update_cell<A, VARIANT>(ci, wh, wu, wv, p);
+    const int np = si.par ^ 1;
+    if constexpr (is_split<A>::value) st4(m.S[np] + 4 * (size_t)c, o.h, o.u, o.v, o.hlo);
+    else st4(m.S[np] + 4 * (size_t)c, o.h, o.u, o.v, o.z);
+    m.W[c] = o.w;
+    if (!(isfinite((double)o.h) && isfinite((double)o.u) && isfinite((double)o.v))) atomicOr(m.err, ERRBIT_NONFINITE);
+}
+
+// Every cell of one step.  Single mesh: a grid-stride loop over the cells.
+// Batch: CTA b takes the scenario and cell range of useg[b].
+template <class A, int VARIANT, int UMINB, bool SEG>
+__global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<A> m, int k, int write_flux) {
+    if constexpr (SEG) {
+        const int4 d = m.useg[blockIdx.x];
+        const ScnParams sp = m.scn[d.x];
+        cudaGridDependencySynchronize();
+        cudaTriggerProgrammaticLaunchCompletion();
+        const StepIndex si = step_index(m, k, sp.per_day, sp.ndays);
+        const StepParams p{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
+        const int c = d.y + (int)threadIdx.x;
+        if ((int)threadIdx.x < d.z) update_one<A, VARIANT>(m, c, si, p, write_flux, m.slotw + 16 * (size_t)c);
+    } else {
+        cudaGridDependencySynchronize();
+        cudaTriggerProgrammaticLaunchCompletion();
+        const StepIndex si = step_index(m, k, m.per_day, m.ndays);
+        const StepParams p{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
+        for (int c = blockIdx.x * UPDATE_THREADS + threadIdx.x; c < m.C; c += gridDim.x * UPDATE_THREADS)
+            update_one<A, VARIANT>(m, c, si, p, write_flux, m.slotw + 16 * (size_t)c);
+    }
+}
+
+// The whole step of one tile (tile layout): every record of the tile writes
+// its slots' terms into shared memory, then each cell of the tile sums its
+// four slots in order and is updated.  Slots of edges that leave the tile are
+// single records, computed by each tile for its own slot as the reference
+// computes every slot; the state of the neighbour across is read from global
+// memory, where the previous step (the previous launch) left it.
+template <class A, int VARIANT, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) tile_kernel(DevMesh<A> m, int k, int write_flux) {
+    using R = typename A::real;
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    R *terms = reinterpret_cast<R *>(tile_smem);                                       // [max cells][4 slots][4]
+    int *queue = reinterpret_cast<int *>(tile_smem + 16 * sizeof(R) * (size_t)m.max_tile_cells);
+    __shared__ int qn;
+    const TileDesc td = m.tiles[blockIdx.x];   // constant tables: read before the dependency wait
+    const ScnParams sp = m.scn[td.scn];
+    if (threadIdx.x == 0) qn = 0;
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
+    const StepIndex si = step_index(m, k, sp.per_day, sp.ndays);
+    const StepParams p{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
+    const Terms<R> tout{terms, 4 * td.cell0};
+    __syncthreads();
+    const int nrec = td.npairs + td.nsingles;
+    for (int i = threadIdx.x; i < nrec; i += THREADS) {
+        if (i < td.npairs) pair_record<A, VARIANT>(m, td.rec0 + i, si, p, write_flux, tout, queue, &qn);
+        else single_record<A, VARIANT>(m, td.rec0 + i, si, p, write_flux, tout);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < qn; i += THREADS) pair_mirror<A>(m, queue[i], si, p, write_flux, tout);
+    __syncthreads();
+    for (int c = threadIdx.x; c < td.cells; c += THREADS)
+        update_one<A, VARIANT>(m, td.cell0 + c, si, p, write_flux, terms + 16 * c);
+}
+
+__global__ void tick_kernel(long long *ctr, int n) { *ctr += n; }
+
+// Split precision state <-> the reference's (H, Z) of one cell.  The depth is
+// kept as the fp32 pair (h, hlo) with h + hlo = H; a cell at or below the dry
+// threshold keeps in hlo the offset of its level instead (split_level).
+struct SplitCodec {
+    static __host__ __device__ inline void encode(double H, double Z, double zbc, float hm1f, float &h, float &hlo) {
+        h = (float)H;
+        hlo = h > hm1f ? (float)(H - (double)h) : (float)((Z - zbc) - (double)h);
+    }
+    static __host__ __device__ inline double depth(float h, float hlo, float hm1f, double hm1) {
+        return h > hm1f ? (double)h + (double)hlo : (h == hm1f ? hm1 : (double)h);
+    }
+    static __host__ __device__ inline double level(float h, float hlo, double zbc) {
+        return (double)h + ((double)hlo + zbc);
+    }
+};
+
+// Reference-order staging <-> device-order state of one scenario: cells
+// [cell0, cell0 + C) of the device state, perm[new] = old within the scenario.
+template <class A>
+__global__ void stage_in_kernel(DevMesh<A> m, int cell0, int C, double hm1, const int32_t *__restrict__ perm,
+                                const double *__restrict__ stage) {
+    using R = typename A::real;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) return;
+    const int o = perm[i];
+    R *d = m.S[(*m.step_ctr) & 1] + 4 * ((size_t)cell0 + i);
+    d[1] = (R)stage[(size_t)C + o];
+    d[2] = (R)stage[2 * (size_t)C + o];
+    if constexpr (is_split<A>::value) {
+        float h, hlo;
+        SplitCodec::encode(stage[o], stage[3 * (size_t)C + o], m.zbc[cell0 + i], (float)hm1, h, hlo);
+        d[0] = h; d[3] = hlo;
+    } else {
+        d[0] = (R)stage[o];
+        d[3] = (R)stage[3 * (size_t)C + o];
+    }
+}
+template <class A>
+__global__ void stage_out_kernel(DevMesh<A> m, int cell0, int C, double hm1, const int32_t *__restrict__ perm,
+                                 double *__restrict__ stage) {
+    using R = typename A::real;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) return;
+    const int o = perm[i];
+    const R *d = m.S[(*m.step_ctr) & 1] + 4 * ((size_t)cell0 + i);
+    stage[(size_t)C + o] = (double)d[1];
+    stage[2 * (size_t)C + o] = (double)d[2];
+    if constexpr (is_split<A>::value) {
+        stage[o] = SplitCodec::depth(d[0], d[3], (float)hm1, hm1);
+        stage[3 * (size_t)C + o] = SplitCodec::level(d[0], d[3], m.zbc[cell0 + i]);
+    } else {
+        stage[o] = (double)d[0];
+        stage[3 * (size_t)C + o] = (double)d[3];
+    }
+    stage[4 * (size_t)C + o] = (double)m.W[cell0 + i];
+}
+
+// per-cell constants that the update needs, computed on the device with the
+// reference's arithmetic (functors.cu:750, v0 functors.cu:752-763)
+template <class A, int VARIANT>
+__global__ void setup_cells_kernel(int C, double dt, const typename A::real *area, const typename A::real *side4,
+                                   typename A::real *dta, typename A::real *sidex) {
+    using R = typename A::real;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) return;
+    if (VARIANT == 1) {
+        const R s0 = side4[4 * i], s1 = side4[4 * i + 1], s2 = side4[4 * i + 2], s3 = side4[4 * i + 3];
+        if (s3 > R(0)) sidex[i] = A::fmin(A::mul(A::c(0.5), A::add(s0, s2)), A::mul(A::c(0.5), A::add(s1, s3)));
+        else {
+            R ss = A::mul(A::c(0.5), A::add(A::add(s0, s1), s2));
+            sidex[i] = A::sqrt(A::div(A::mul(A::mul(A::sub(ss, s0), A::sub(ss, s1)), A::sub(ss, s2)), ss));
+        }
+        dta[i] = area[i];
+    } else {
+        dta[i] = A::div(A::c(dt), area[i]);
+    }
+}
+
+}  // namespace hb
