@@ -18,7 +18,7 @@ OBJ_DIR = os.path.join(HERE, "_build")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["hb_solver.cu", "hb_ref_layout.cu"]
+CU_SOURCES = ["hb_solver.cu", "hb_ref_layout.cu", "hb_adjoint.cu"]
 CPP_SOURCES = ["hb_deck.cpp"]
 
 
@@ -43,12 +43,18 @@ def build(force: bool = False, verbose: bool = True) -> str:
     os.makedirs(OBJ_DIR, exist_ok=True)
     objs = []
     common = ["-O3", "-std=c++17", "-I", INCLUDE, "-I", CSRC]
+    # the translation units compile in parallel
+    from concurrent.futures import ThreadPoolExecutor
+    jobs = []
     for f in CU_SOURCES:
         o = os.path.join(OBJ_DIR, f + ".o")
         cmd = [NVCC, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC", "-Xptxas", "-v", "-c",
                os.path.join(CSRC, f), "-o", o]
-        _run(cmd, verbose, os.path.join(OBJ_DIR, f + ".ptxas.txt"))
+        jobs.append((cmd, os.path.join(OBJ_DIR, f + ".ptxas.txt")))
         objs.append(o)
+    with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+        for fut in [ex.submit(_run, cmd, verbose, log) for cmd, log in jobs]:
+            fut.result()
     for f in CPP_SOURCES:
         o = os.path.join(OBJ_DIR, f + ".o")
         # host arithmetic of the deck reader must round every operation like the reference's host code

@@ -1,0 +1,904 @@
+// hb_adjoint.cu -- reverse-mode adjoint of the fp64 timestep (variant H).
+//
+// A rollout of T steps x_{t+1} = F(x_t; n, ZBC) from the initial level and
+// velocities, with the loss
+//     L = sum over observation steps t (every `obs_every`) and gauge cells g
+//         of (H_t[g] - Hobs_t[g])^2,
+// and its gradient with respect to the per-cell Manning coefficient n
+// (FNC = 9.81 n^2, mesh.cpp:364) and bed elevation ZBC.  The initial depth
+// follows the bed as in mesh.cpp:350-361: H0 = Z0 - ZBC where Z0 > ZBC, else
+// H0 = HM1 and Z0 = ZBC + HM1.
+//
+// The reverse sweep is written out by hand.  Every branch choice of the
+// forward step (the slot's branch chain and Osher's wave case, wet/dry and
+// velocity clamps, max/min picks, the iteration counts of the KLAS 10 and
+// KLAS 1 fixed points) is taken from the forward state, recomputed with the
+// forward's own arithmetic, and the derivative is that of the chosen branch.
+// Adjoint arithmetic is plain fp64.
+//
+// Memory: the state is kept every `checkpoint_every` = k steps; the backward
+// pass recomputes each k-step segment from its checkpoint, keeping that
+// segment's states and slot terms, then runs the segment's reverse steps:
+//   adj_slot_kernel    four lanes per cell: the update's reverse (each lane
+//                      redundantly) and lane j's slot flux reverse, writing the
+//                      slot's contributions to its own cell and its neighbour;
+//   adj_gather_kernel  per cell: the state adjoint of the step's input, from the
+//                      update's direct terms, its own slots' contributions and
+//                      those of the neighbours' slots that face it (a gather in
+//                      slot order, no atomics: the gradient is deterministic).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "hb_handle.hpp"
+
+namespace hb {
+namespace adj {
+
+using A = F64Exact;
+
+// adjoint of one cell's slot inputs {h, u, v, z, zbc}
+struct Adj5 { double h, u, v, z, b; };
+
+// QF(h, u, v) = (h u, h u^2, h u v, 4.905 h^2) times `sign`, reversed with
+// output adjoint ob (functors.cu:505-511)
+__device__ __forceinline__ void qf_rev(double h, double u, double v, double sign, const double ob[4], double &hb,
+                                       double &ub, double &vb) {
+    hb += sign * (ob[0] * u + ob[1] * u * u + ob[2] * u * v + ob[3] * 9.81 * h);
+    ub += sign * (ob[0] * h + ob[1] * 2.0 * h * u + ob[2] * h * v);
+    vb += sign * (ob[2] * h * u);
+}
+
+// Reverse of osher() (functors.cu:570-712) for the case its forward picks.
+// In: the forward inputs and the adjoint fb of out[4].  Out (added): ql_b,
+// qr_b, fil_b.  cl enters only the case choice.
+__device__ void osher_rev(double cl, const double ql[3], const double qr[3], double fil, const double fb[4],
+                          double qlb[3], double qrb[3], double &filb) {
+    const double cr = A::sqrt(A::mul(A::c(9.81), qr[0]));
+    const double fir = A::sub(qr[1], A::mul(A::c(2.0), cr));
+    const double ua = A::mul(A::add(fil, fir), A::c(0.5));
+    const double ca = A::fabs(A::mul(A::sub(fil, fir), A::c(0.25)));
+    int k2 = 0, k1 = 0;
+    if (ca < ua) k2 = 1;
+    else if (ua >= 0.0 && ua < ca) k2 = 2;
+    else if (ua >= -ca && ua < 0.0) k2 = 3;
+    else if (ua < -ca) k2 = 4;
+    if (ql[1] < cl && qr[1] >= -cr) k1 = 1;
+    else if (ql[1] >= cl && qr[1] >= -cr) k1 = 2;
+    else if (ql[1] < cl && qr[1] < -cr) k1 = 3;
+    else if (ql[1] >= cl && qr[1] < -cr) k1 = 4;
+    const bool any = k1 != 0 && k2 != 0;
+    if (!any) return;
+    const bool p1 = k1 == 2 || k1 == 4;
+    const bool p2 = k2 == 1 ? (k1 == 1 || k1 == 3) : (k1 == 2 || k1 == 4);
+    const double s2 = k2 != 1 ? -1.0 : 1.0;
+    const bool p3 = k2 == 2, p5 = k2 == 3;
+    const bool p6 = k2 == 4 ? k1 <= 2 : k1 >= 3;
+    const double s6 = k2 != 4 ? -1.0 : 1.0;
+    const bool p7 = k1 >= 3;
+    // forward values of the pieces
+    const double us = fil / 3.0, hs = us * us / 9.81;
+    const double ua35 = 0.5 * (fil + fir);
+    const double fil3 = fil - ua35, ha3 = fil3 * fil3 / 39.24;
+    const double fir5 = fir - ua35, ha5 = fir5 * fir5 / 39.24;
+    const double f6 = p5 ? fir5 : fir;
+    const double us6 = f6 / 3.0, hs6 = us6 * us6 / 9.81;
+    double firb = 0.0, ua35b = 0.0, fir5b = 0.0;
+    if (p1) qf_rev(ql[0], ql[1], ql[2], 1.0, fb, qlb[0], qlb[1], qlb[2]);
+    if (p2) {
+        double hsb = 0.0, usb = 0.0;
+        qf_rev(hs, us, ql[2], s2, fb, hsb, usb, qlb[2]);
+        usb += hsb * 2.0 * us / 9.81;
+        filb += usb / 3.0;
+    }
+    if (p3) {
+        double hab = 0.0;
+        qf_rev(ha3, ua35, ql[2], 1.0, fb, hab, ua35b, qlb[2]);
+        const double fil3b = hab * 2.0 * fil3 / 39.24;
+        filb += fil3b;
+        ua35b -= fil3b;
+    }
+    if (p5) {
+        double hab = 0.0;
+        qf_rev(ha5, ua35, qr[2], 1.0, fb, hab, ua35b, qrb[2]);
+        fir5b += hab * 2.0 * fir5 / 39.24;
+    }
+    if (p6) {
+        double hsb = 0.0, usb = 0.0;
+        qf_rev(hs6, us6, qr[2], s6, fb, hsb, usb, qrb[2]);
+        usb += hsb * 2.0 * us6 / 9.81;
+        const double f6b = usb / 3.0;
+        if (p5) fir5b += f6b;
+        else firb += f6b;
+    }
+    if (p7) qf_rev(qr[0], qr[1], qr[2], 1.0, fb, qrb[0], qrb[1], qrb[2]);
+    firb += fir5b;
+    ua35b -= fir5b;
+    filb += 0.5 * ua35b;
+    firb += 0.5 * ua35b;
+    qrb[1] += firb;
+    const double crb = -2.0 * firb;
+    if (cr > 0.0) qrb[0] += crb * 9.81 / (2.0 * cr);
+}
+
+// Reverse of the Osher route of a slot (functors.cu:151-200): left cell L,
+// right cell R, normal (cs, sn) from L to R; `mir` = the mirrored route
+// (left = the neighbour).  fb: adjoint of the slot's fluxes.
+__device__ void osher_route_rev(const CellStateA<A> &L, const CellStateA<A> &R, double cs, double sn, bool mir,
+                                const StepParams &p, const double fb[4], Adj5 &Lb, Adj5 &Rb) {
+    const double HM1 = p.hm1, HM2 = p.hm2;
+    const double clL = A::sqrt(A::mul(A::c(9.81), L.h));
+    const OsherIn<double> oi = osher_inputs<A>(L, R, cs, sn, clL, mir, p);
+    double fo[4];
+    osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo);
+    // outputs: F0 = +-fo0, F1 = fo1 + (1-ratio) hcR ur^2 / 2, F2 = fo2, F3 = fo3 or mirror_f3(fo3)
+    double fob[4] = {mir ? -fb[0] : fb[0], fb[1], fb[2], 0.0};
+    if (!mir) {
+        fob[3] = fb[3];
+    } else {
+        // F3 = 4.905 hc3^2, hc3 = za - ZBC_R where za = sqrt(fo3/4.905) + ZBC_L > ZBC_R (functors.cu:191-199)
+        const double za = A::ladd(A::lvl(A::sqrt(A::divk(fo[3], 4.905))), L.zbc);
+        if (za > R.zbc) {
+            const double hc3 = za - R.zbc;
+            const double hc3b = fb[3] * 9.81 * hc3;
+            Rb.b -= hc3b;
+            Lb.b += hc3b;
+            const double t = sqrt(fo[3] / 4.905);
+            if (t > 0.0) fob[3] = hc3b / (2.0 * t) / 4.905;
+        }
+    }
+    double ratiob = 0.0, hcRb = 0.0, urb = 0.0;
+    ratiob -= fb[1] * oi.hcR * oi.ur * oi.ur * 0.5;
+    hcRb += fb[1] * (1.0 - oi.ratio) * oi.ur * oi.ur * 0.5;
+    urb += fb[1] * (1.0 - oi.ratio) * oi.hcR * oi.ur;
+    double qlb[3] = {0, 0, 0}, qrb[3] = {0, 0, 0}, filb = 0.0;
+    osher_rev(oi.cl, oi.ql, oi.qr, oi.fil, fob, qlb, qrb, filb);
+    // fil = ql1 + 2 clL, clL = sqrt(9.81 h_L)
+    qlb[1] += filb;
+    if (clL > 0.0) Lb.h += 2.0 * filb * 9.81 / (2.0 * clL);
+    // ql = (h_L, u_L cs + v_L sn, v_L cs - u_L sn)
+    Lb.h += qlb[0];
+    Lb.u += qlb[1] * cs - qlb[2] * sn;
+    Lb.v += qlb[1] * sn + qlb[2] * cs;
+    // qr2 = v_R cs - u_R sn
+    Rb.v += qrb[2] * cs;
+    Rb.u -= qrb[2] * sn;
+    // qr1 = ur * ratio unless clamped to +-VMIN
+    if (!(oi.hcR <= HM2 || oi.qr[0] <= HM2)) {
+        urb += qrb[1] * oi.ratio;
+        ratiob += qrb[1] * oi.ur;
+    }
+    double qr0b = qrb[0];
+    // ratio = min(hcR / qr0, 1.5)
+    const double q = A::div(oi.hcR, oi.qr[0]);
+    if (q < 1.5) {
+        hcRb += ratiob / oi.qr[0];
+        qr0b -= ratiob * oi.hcR / (oi.qr[0] * oi.qr[0]);
+    }
+    // ur = u_R cs + v_R sn
+    Rb.u += urb * cs;
+    Rb.v += urb * sn;
+    // qr0 = max(zR - ZBC_L, HM1), zR = max(ZBC_R, Z_R)
+    const double zR = A::lmax(R.zbc, R.z);
+    if (A::depth(zR, L.zbc) > HM1) {
+        if (R.z > R.zbc) Rb.z += qr0b;
+        else Rb.b += qr0b;
+        Lb.b -= qr0b;
+    }
+    // hcR = max(h_R, HM1)
+    if (R.h > HM1) Rb.h += hcRb;
+}
+
+// Reverse of the boundary slots of BOUNDA (functors.cu:513-568) for KLAS 4,
+// 10 and 1 (variant H).  hb/ql1b/ql2b/filb: adjoints of the slot's own depth,
+// rotated velocity and FIL; b1b that of its bed.
+template <class TableFetch>
+__device__ void bounda_rev(const SlotInA<A> &in, const StepParams &p, double ql1, double ql2, double fil, double cl,
+                           const TableFetch &fetch, const double fb[4], double &hb, double &ql1b, double &ql2b,
+                           double &filb, double &b1b, uint32_t *err) {
+    const double h = in.own.h;
+    const double HM2 = p.hm2;
+    const bool super = ql1 > cl && h < HM2;   // variant H (functors.cu:517)
+    if (super) {
+        hb += fb[0] * ql1 + fb[1] * ql1 * ql1 + fb[2] * ql1 * ql2 + fb[3] * 9.81 * h;
+        ql1b += fb[0] * h + fb[1] * 2.0 * h * ql1 + fb[2] * h * ql2;
+        ql2b += fb[2] * h * ql1;
+        return;
+    }
+    switch (in.code) {
+    case CODE_K4:
+        hb += fb[3] * 9.81 * h;
+        break;
+    case CODE_K10: {   // functors.cu:204-232
+        BoundaryInA<A> b = fetch();
+        double f0 = -A::madd(b.dqt, A::c((double)p.kt), b.qt, M_K10);
+        f0 = A::div(f0, in.side);
+        // forward iterates of inflow_depth
+        double hb0s[21];
+        hb0s[0] = h;
+        double hbv = 0.0;
+        int K = 0;
+        for (int k = 1; k <= 20; k++) {
+            const double w = A::sub(fil, A::div(f0, hb0s[k - 1]));
+            hbv = A::divk(A::mul(w, w), 39.24);
+            K = k;
+            if (A::fabs(A::sub(hb0s[k - 1], hbv)) <= A::c(0.005)) break;
+            hb0s[k] = A::add(A::mul(hb0s[k - 1], A::c(0.5)), A::mul(hbv, A::c(0.5)));
+        }
+        // F1 = hb <= 1 ? 0 : f0^2 / hb, F3 = 4.905 hb^2
+        double hbb = fb[3] * 9.81 * hbv;
+        if (!(hbv <= 1.0)) hbb -= fb[1] * f0 * f0 / (hbv * hbv);
+        // back through the iterations: hb_k = (fil - f0/hb0_{k-1})^2 / 39.24,
+        // hb0_k = (hb0_{k-1} + hb_k) / 2
+        double hb_k_b = hbb;      // adjoint of hb_k for the current k
+        double hb0_b = 0.0;       // adjoint of hb0_{k-1} through hb0_k's average
+        for (int k = K; k >= 1; k--) {
+            const double w = fil - f0 / hb0s[k - 1];
+            const double wb = hb_k_b * 2.0 * w / 39.24;
+            filb += wb;
+            const double hb0prev_b = wb * f0 / (hb0s[k - 1] * hb0s[k - 1]) + hb0_b;
+            if (k - 1 >= 1) {
+                hb_k_b = 0.5 * hb0prev_b;
+                hb0_b = 0.5 * hb0prev_b;
+            } else {
+                hb += hb0prev_b;   // hb0_0 = h
+            }
+        }
+        break;
+    }
+    case CODE_K1: {   // functors.cu:371-392, variant H: DZT * jt
+        BoundaryInA<A> b = fetch();
+        const double lev = A::lmadd(b.dzt, A::lc((double)p.jt), b.zt, M_K1);
+        const double d = A::lsub(lev, in.own.zbc);
+        const double hb1 = A::fmax(d, A::c(p.hm2));
+        // forward iterates of invariant_iter
+        const double fial = A::madd(A::c(6.264), A::sqrt(h), ql1, M_FIAL1);
+        const double shb = A::sqrt(hb1);
+        double us[31];
+        us[0] = ql1;
+        double ur0 = ql1, urb = ql1;
+        int K = 0;
+        for (int k = 1; k <= 30; k++) {
+            const double fiar = A::madd(A::c(-6.264), shb, urb, M_FIAR1);
+            const double dsum = A::add(fial, fiar), ddif = A::sub(fial, fiar);
+            urb = A::divk(A::div(A::mul(A::mul(dsum, ddif), ddif), hb1), 313.92);
+            us[k] = urb;
+            K = k;
+            if (A::fabs(A::sub(urb, ur0)) <= A::c(0.0001)) break;
+            ur0 = urb;
+        }
+        // F0 = hb1 urb, F1 = hb1 urb^2, F3 = 4.905 hb1^2; F2 from the prelude
+        double ub = fb[0] * hb1 + fb[1] * 2.0 * hb1 * urb;
+        double hb1b = fb[0] * urb + fb[1] * urb * urb + fb[3] * 9.81 * hb1;
+        double fialb = 0.0, shbb = 0.0;
+        for (int k = K; k >= 1; k--) {
+            const double fiar = us[k - 1] - 6.264 * shb;
+            const double dsum = fial + fiar, ddif = fial - fiar;
+            const double g = us[k];
+            const double dsumb = ub * ddif * ddif / (hb1 * 313.92);
+            const double ddifb = ub * 2.0 * dsum * ddif / (hb1 * 313.92);
+            hb1b -= ub * g / hb1;
+            fialb += dsumb + ddifb;
+            const double fiarb = dsumb - ddifb;
+            shbb -= 6.264 * fiarb;
+            ub = fiarb;          // adjoint of us[k-1]
+        }
+        ql1b += ub;              // us[0] = ql1
+        ql1b += fialb;
+        if (h > 0.0) hb += fialb * 6.264 / (2.0 * sqrt(h));
+        if (shb > 0.0) hb1b += shbb / (2.0 * shb);
+        if (d > p.hm2) b1b -= hb1b;
+        // prelude FLUX2 = h ql1 ql2 when ql1 > 0
+        if (ql1 > 0.0) {
+            hb += fb[2] * ql1 * ql2;
+            ql1b += fb[2] * h * ql2;
+            ql2b += fb[2] * h * ql1;
+        }
+        break;
+    }
+    default:
+        atomicOr(err, ERRBIT_UNDEFINED);   // rejected at creation; never reached
+        break;
+    }
+}
+
+// Reverse of one slot's flux (functors.cu:47-202, variant H) for fluxes'
+// adjoint fb; adds the adjoints of the own cell's and the neighbour's
+// {h, u, v, z, zbc}.
+template <class TableFetch>
+__device__ void slot_rev(const SlotInA<A> &in, const StepParams &p, const TableFetch &fetch, const double fb[4],
+                         Adj5 &go, Adj5 &gn, uint32_t *err) {
+    const double HM1 = p.hm1, HM2 = p.hm2, C1 = K::C1;
+    const double h1 = in.own.h, u1 = in.own.u, v1 = in.own.v, z1 = in.own.z, b1 = in.own.zbc;
+    const double cs = in.cosj, sn = in.sinj;
+    const double ql1 = A::dot(u1, cs, v1, sn, M_QL1);
+    const double ql2 = A::dot(v1, cs, -u1, sn, M_QL2);
+    const double zb1 = A::ladd(b1, A::lc(p.hm1));
+    const double zi = A::lmax(z1, zb1);
+    double hc = 0, bc = 0, zc = 0, uc = 0, vc = 0;
+    if (in.has_nb) {
+        hc = A::fmax(in.nb.h, HM1);
+        bc = in.nb.zbc;
+        zc = A::lmax(bc, in.nb.z);
+        uc = in.nb.u;
+        vc = in.nb.v;
+    }
+    double ql1b = 0, ql2b = 0, zib = 0, hcb = 0, bcb = 0, zcb = 0, ucb = 0, vcb = 0;
+    const double cl = A::sqrt(A::mul(A::c(9.81), h1));
+    if (code_is_bounda(in.code)) {
+        const double fil = A::add(ql1, A::mul(A::c(2.0), cl));
+        double filb = 0.0;
+        bounda_rev(in, p, ql1, ql2, fil, cl, fetch, fb, go.h, ql1b, ql2b, filb, go.b, err);
+        ql1b += filb;
+        if (cl > 0.0) go.h += 2.0 * filb * 9.81 / (2.0 * cl);
+    } else if (h1 <= HM1 && hc <= HM1) {
+        // all fluxes zero
+    } else if (zi <= bc) {
+        hcb += fb[0] * (-C1) * 1.5 * sqrt(hc);
+        go.h += fb[1] * ql1 * fabs(ql1) + fb[3] * 9.81 * h1;
+        ql1b += fb[1] * h1 * 2.0 * fabs(ql1);
+    } else if (zc <= b1) {
+        go.h += fb[0] * C1 * 1.5 * sqrt(h1) + fb[1] * ql1 * fabs(ql1) + fb[2] * fabs(ql1) * ql2;
+        ql1b += fb[1] * 2.0 * h1 * fabs(ql1) + fb[2] * h1 * (ql1 > 0 ? 1.0 : ql1 < 0 ? -1.0 : 0.0) * ql2;
+        ql2b += fb[2] * h1 * fabs(ql1);
+    } else if (h1 <= HM2) {
+        if (zc > zi) {
+            const double dz = A::depth(zc, b1);
+            const double dh = A::fmax(dz, HM1);
+            const double sq = sqrt(dh);
+            const double vt = A::dot(vc, cs, -uc, sn, M_SHALLOW_VT);
+            const double F0 = -C1 * dh * sq;
+            const double dhb = fb[0] * (-C1 * 1.5 * sq) + fb[1] * (C1 * C1 * 2.0 * dh) + fb[2] * vt * (-C1 * 1.5 * sq);
+            const double vtb = fb[2] * F0;
+            vcb += vtb * cs;
+            ucb -= vtb * sn;
+            go.h += fb[3] * 9.81 * h1;
+            if (dz > HM1) { zcb += dhb; go.b -= dhb; }
+        } else {
+            go.h += fb[0] * C1 * 1.5 * sqrt(h1) + fb[3] * 9.81 * h1;
+        }
+    } else if (hc <= HM2) {
+        if (zi > zc) {
+            const double dz = A::depth(zi, bc);
+            const double dh = A::fmax(dz, HM1);
+            const double sq = sqrt(dh);
+            const double hc1 = A::depth(zc, b1);
+            const double F0 = C1 * dh * sq;
+            const double dhb = fb[0] * (C1 * 1.5 * sq) + fb[1] * (C1 * C1 * 2.0 * dh) + fb[2] * ql2 * (C1 * 1.5 * sq);
+            ql2b += fb[2] * F0;
+            const double hc1b = fb[3] * 9.81 * hc1;
+            zcb += hc1b;
+            go.b -= hc1b;
+            if (dz > HM1) { zib += dhb; bcb -= dhb; }
+        } else {
+            hcb += fb[0] * (-C1) * 1.5 * sqrt(hc);
+            go.h += fb[1] * ql1 * ql1 + fb[3] * 9.81 * h1;
+            ql1b += fb[1] * 2.0 * h1 * ql1;
+        }
+    } else if (in.code == CODE_ZERO && in.own_first) {
+        Adj5 lb{0, 0, 0, 0, 0}, rb{0, 0, 0, 0, 0};
+        osher_route_rev(in.own, in.nb, cs, sn, false, p, fb, lb, rb);
+        go.h += lb.h; go.u += lb.u; go.v += lb.v; go.z += lb.z; go.b += lb.b;
+        gn.h += rb.h; gn.u += rb.u; gn.v += rb.v; gn.z += rb.z; gn.b += rb.b;
+    } else if (!in.has_nb) {
+        atomicOr(err, ERRBIT_UNDEFINED);
+    } else {
+        Adj5 lb{0, 0, 0, 0, 0}, rb{0, 0, 0, 0, 0};
+        osher_route_rev(in.nb, in.own, -cs, -sn, true, p, fb, lb, rb);
+        gn.h += lb.h; gn.u += lb.u; gn.v += lb.v; gn.z += lb.z; gn.b += lb.b;
+        go.h += rb.h; go.u += rb.u; go.v += rb.v; go.z += rb.z; go.b += rb.b;
+    }
+    // ql = (h1, u1 cs + v1 sn, v1 cs - u1 sn)
+    go.u += ql1b * cs - ql2b * sn;
+    go.v += ql1b * sn + ql2b * cs;
+    // zi = max(z1, ZBC + HM1)
+    if (z1 >= zb1) go.z += zib;
+    else go.b += zib;
+    if (in.has_nb) {
+        if (in.nb.h > HM1) gn.h += hcb;
+        gn.b += bcb;
+        if (in.nb.z > bc) gn.z += zcb;
+        else gn.b += zcb;
+        gn.u += ucb;
+        gn.v += vcb;
+    }
+}
+
+// Adjoint-side mesh: per device slot its geometry, neighbour, code and the
+// neighbour's slot that faces back.
+struct AdjMesh {
+    const double *cs4, *sn4, *side4;
+    const int32_t *nbr4, *mirror4;
+    const uint8_t *meta4;        // code | own_first | has_nb; 0xFF = no real slot
+    const int32_t *gauge_of;     // [C] gauge index of the cell, -1
+    double *dir;                 // [C][4] the update's direct terms of the state adjoint
+    double *so, *sn;             // [4C][5] a slot's contributions to its own cell and to its neighbour
+    double *fnc_g, *zbc_g;       // [C] accumulated gradients
+    double *lam;                 // [C][4] state adjoint {H, U, V, Z}
+    const double *res;           // [nobs][ng] residuals H - Hobs
+    int ng, obs_every;
+};
+
+// One reverse step t: four lanes per cell.  x: the state before the step;
+// terms: the forward's slot terms of the step; a.lam: adjoint of the state
+// after the step.
+__global__ void __launch_bounds__(128) adj_slot_kernel(DevMesh<A> m, AdjMesh a, const double *__restrict__ x,
+                                                       const double *__restrict__ terms, StepParams p) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = gid >> 2, j = gid & 3;
+    if (c >= m.C) return;
+    const double hv = x[4 * (size_t)c], uv = x[4 * (size_t)c + 1], vv = x[4 * (size_t)c + 2];
+    const double zbc = m.zbc[c];
+    // ---- the update (UpdateCellKernel, functors.cu:717-784, variant H), forward values
+    double wh = 0.0, wu = 0.0, wv = 0.0;
+    const unsigned mask = m.cmask[c];
+    for (int q = 0; q < 4; q++) {
+        if (!(mask & (1u << q))) continue;
+        const double *t = terms + 16 * (size_t)c + 4 * q;
+        wh = A::madd(t[3], t[0], wh, M_WH);
+        wu = A::add(wu, t[1]);
+        wv = A::add(wv, t[2]);
+    }
+    const double HM1 = p.hm1, HM2 = p.hm2, DT = p.dt;
+    const double dta = m.dta[c], fnc = m.fnc[c];
+    const double h2raw = A::add(A::madd(-dta, wh, hv, M_H2), A::c(K::QLUA));
+    const double h2 = A::fmax(h2raw, HM1);
+    const double lh = a.lam[4 * (size_t)c], lu = a.lam[4 * (size_t)c + 1], lv = a.lam[4 * (size_t)c + 2],
+                 lz = a.lam[4 * (size_t)c + 3];
+    double h2b = lh + lz;   // Z2 = H2 + ZBC
+    double hb = 0.0, ub = 0.0, vb = 0.0, whb = 0.0, wub = 0.0, wvb = 0.0, fncb = 0.0;
+    if (h2 > HM2) {
+        const double s2 = A::dot(uv, uv, vv, vv, M_SQ1);
+        const double s = A::sqrt(s2);
+        const double hp = A::pow(hv, A::c(0.33333));
+        const double wsf = A::div(A::mul(fnc, s), hp);
+        const double dtw = A::mul(DT, wsf);
+        const double u2 = A::div(A::madd(-dtw, uv, A::dot(hv, uv, -dta, wu, M_U2A), M_U2B), h2);
+        const double v2 = A::div(A::madd(-dtw, vv, A::dot(hv, vv, -dta, wv, M_U2A), M_U2B), h2);
+        const double ue = fabs(u2) < 15.0 ? lu : 0.0;
+        const double ve = fabs(v2) < 15.0 ? lv : 0.0;
+        const double nub = ue / h2, nvb = ve / h2;
+        h2b -= ue * u2 / h2 + ve * v2 / h2;
+        hb += nub * uv + nvb * vv;
+        ub += nub * (hv - dtw);
+        vb += nvb * (hv - dtw);
+        wub -= nub * dta;
+        wvb -= nvb * dta;
+        const double dtwb = -(nub * uv + nvb * vv);
+        // dtw = DT fnc s / h^p
+        fncb += dtwb * DT * s / hp;
+        const double sb = dtwb * DT * fnc / hp;
+        hb += dtwb * DT * fnc * s * (-0.33333) / (hp * hv);
+        if (s > 0.0) { ub += sb * uv / s; vb += sb * vv / s; }
+    } else if (h2 > HM1) {
+        if (fabs(uv) < K::VMIN) ub += lu;
+        if (fabs(vv) < K::VMIN) vb += lv;
+    }
+    if (h2raw > HM1) { hb += h2b; whb -= h2b * dta; }
+    if (j == 0) {
+        double *d = a.dir + 4 * (size_t)c;
+        d[0] = hb; d[1] = ub; d[2] = vb; d[3] = 0.0;
+        a.fnc_g[c] += fncb;
+        a.zbc_g[c] += lz;
+    }
+    // ---- lane j: slot 4c+j
+    const size_t s = 4 * (size_t)c + j;
+    double *so = a.so + 5 * s, *sno = a.sn + 5 * s;
+    const uint8_t meta = a.meta4[s];
+    if (meta == 0xFF) {
+        for (int q = 0; q < 5; q++) { so[q] = 0.0; sno[q] = 0.0; }
+        return;
+    }
+    const double cs = a.cs4[s], sn = a.sn4[s], side = a.side4[s];
+    const double slcos = side * cs, slsin = side * sn;
+    double fb[4];
+    fb[0] = side * whb;
+    fb[1] = slcos * wub + slsin * wvb;
+    fb[2] = -slsin * wub + slcos * wvb;
+    fb[3] = fb[1];
+    SlotInA<A> in;
+    in.own = CellStateA<A>{hv, uv, vv, x[4 * (size_t)c + 3], zbc};
+    in.code = (int8_t)(meta & META_CODE);
+    in.own_first = meta & META_OWN_FIRST;
+    in.has_nb = meta & META_HAS_NB;
+    const int nb = a.nbr4[s];
+    if (in.has_nb)
+        in.nb = CellStateA<A>{x[4 * (size_t)nb], x[4 * (size_t)nb + 1], x[4 * (size_t)nb + 2], x[4 * (size_t)nb + 3],
+                              m.zbc[nb]};
+    else
+        in.nb = CellStateA<A>{0, 0, 0, 0, 0};
+    in.cosj = cs; in.sinj = sn; in.side = side;
+    auto fetch = [&]() {
+        BoundaryInA<A> bi;
+        const int row = m.bcell[c];
+        if (row >= 0) {
+            const size_t q = (size_t)p.jt * m.nb + row;
+            bi.qt = m.bqt[q]; bi.dqt = m.bdqt[q]; bi.zt = m.bzt[q]; bi.dzt = m.bdzt[q];
+            bi.top = m.btop[row]; bi.nhq1 = m.bnhq1[row];
+            bi.zw = m.bzw + (size_t)row * m.nhq; bi.qw = m.bqw + (size_t)row * m.nhq;
+        } else {
+            bi.qt = bi.dqt = 0.0; bi.zt = bi.dzt = bi.top = 0.0; bi.nhq1 = 0;
+            bi.zw = m.bzw + (size_t)m.nb * m.nhq; bi.qw = m.bqw + (size_t)m.nb * m.nhq;
+        }
+        bi.nhq = m.nhq;
+        return bi;
+    };
+    Adj5 go{0, 0, 0, 0, 0}, gn{0, 0, 0, 0, 0};
+    slot_rev(in, p, fetch, fb, go, gn, m.err);
+    so[0] = go.h; so[1] = go.u; so[2] = go.v; so[3] = go.z; so[4] = go.b;
+    sno[0] = gn.h; sno[1] = gn.u; sno[2] = gn.v; sno[3] = gn.z; sno[4] = gn.b;
+}
+
+// State adjoint of step t's input, per cell, in slot order; then the loss
+// term of observation step t.  `obs_row` = t / obs_every - 1 when t is an
+// observation step (t > 0), else -1.
+__global__ void adj_gather_kernel(int C, AdjMesh a, int obs_row) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    double l[4] = {a.dir[4 * (size_t)c], a.dir[4 * (size_t)c + 1], a.dir[4 * (size_t)c + 2], a.dir[4 * (size_t)c + 3]};
+    double zg = 0.0;
+    for (int j = 0; j < 4; j++) {
+        const double *so = a.so + 5 * (4 * (size_t)c + j);
+        for (int q = 0; q < 4; q++) l[q] += so[q];
+        zg += so[4];
+        const int mj = a.mirror4[4 * (size_t)c + j];
+        if (mj >= 0) {
+            const double *sn = a.sn + 5 * (size_t)mj;
+            for (int q = 0; q < 4; q++) l[q] += sn[q];
+            zg += sn[4];
+        }
+    }
+    if (obs_row >= 0) {
+        const int g = a.gauge_of[c];
+        if (g >= 0) l[0] += 2.0 * a.res[(size_t)obs_row * a.ng + g];
+    }
+    for (int q = 0; q < 4; q++) a.lam[4 * (size_t)c + q] = l[q];
+    a.zbc_g[c] += zg;
+}
+
+// lam = dL/dx_T (the last observation), zero elsewhere
+__global__ void adj_seed_kernel(int C, AdjMesh a, int obs_row) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    double lh = 0.0;
+    if (obs_row >= 0) {
+        const int g = a.gauge_of[c];
+        if (g >= 0) lh = 2.0 * a.res[(size_t)obs_row * a.ng + g];
+    }
+    a.lam[4 * (size_t)c] = lh;
+    a.lam[4 * (size_t)c + 1] = 0.0;
+    a.lam[4 * (size_t)c + 2] = 0.0;
+    a.lam[4 * (size_t)c + 3] = 0.0;
+}
+
+// Initial state from the level (mesh.cpp:350-361) and its reverse.
+__global__ void adj_init_state_kernel(int C, const double *__restrict__ z0, const double *__restrict__ u0,
+                                      const double *__restrict__ v0, const double *__restrict__ zbc, double hm1,
+                                      double *x) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    double h, z;
+    if (z0[c] <= zbc[c]) { h = hm1; z = zbc[c] + hm1; }
+    else { h = z0[c] - zbc[c]; z = z0[c]; }
+    x[4 * (size_t)c] = h; x[4 * (size_t)c + 1] = u0[c]; x[4 * (size_t)c + 2] = v0[c]; x[4 * (size_t)c + 3] = z;
+}
+__global__ void adj_init_rev_kernel(int C, AdjMesh a, const double *__restrict__ z0, const double *__restrict__ zbc) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    if (z0[c] <= zbc[c]) a.zbc_g[c] += a.lam[4 * (size_t)c + 3];   // Z0 = ZBC + HM1
+    else a.zbc_g[c] -= a.lam[4 * (size_t)c];                        // H0 = Z0 - ZBC
+}
+
+// depths of the gauge cells after a step, into gd [ng]
+__global__ void adj_gauge_kernel(const double *__restrict__ S, const int32_t *__restrict__ gcell, int ng, double *gd) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < ng) gd[g] = S[4 * (size_t)gcell[g]];
+}
+
+__global__ void set_counter_kernel(long long *ctr, long long v) { *ctr = v; }
+
+}  // namespace adj
+}  // namespace hb
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+struct hb_adjoint {
+    hb_handle *h = nullptr;
+    int C = 0, T = 0, k = 0, obs_every = 0, ng = 0, nobs = 0;
+    std::vector<void *> allocs;
+    std::vector<int32_t> gauges_dev;        // gauge cells, device order
+    int32_t *d_gcell = nullptr;
+    double *d_ckpt = nullptr;               // [T/k + 1][C][4]
+    double *d_seg = nullptr;                // [k + 1][C][4] states of a segment
+    double *d_terms = nullptr;              // [k][4C][4] slot terms of a segment
+    double *d_gd = nullptr;                 // [nobs][ng] gauge depths of the forward
+    double *d_obs = nullptr;                // [nobs][ng]
+    double *d_res = nullptr;                // [nobs][ng]
+    double *d_z0 = nullptr, *d_u0 = nullptr, *d_v0 = nullptr;   // initial level and velocities (device order)
+    hb::adj::AdjMesh am{};
+    bool forward_done = false;
+    ~hb_adjoint() { for (void *p : allocs) cudaFree(p); }
+};
+
+namespace {
+
+template <class T>
+int adj_alloc(hb_adjoint *a, T **dst, size_t count) {
+    void *p = nullptr;
+    const size_t n = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) return hb::set_error(HB_E_NOMEM, "adjoint: cudaMalloc(%zu): %s", n, cudaGetErrorString(e));
+    a->allocs.push_back(p);
+    HB_CUDA_RET(cudaMemset(p, 0, n));
+    *dst = (T *)p;
+    return HB_OK;
+}
+template <class T>
+int adj_upload(hb_adjoint *a, T **dst, const std::vector<T> &v) {
+    TRY(adj_alloc(a, dst, v.size()));
+    if (!v.empty()) HB_CUDA_RET(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return HB_OK;
+}
+
+hb::StepParams step_params(const hb_handle *h, long long step) {
+    const hb::Scenario &sc = h->scn[0];
+    hb::StepParams p;
+    p.hm1 = sc.hm1; p.hm2 = sc.hm2; p.jl = sc.jl; p.dt = sc.dt;
+    p.jt = (int)(step / sc.per_day);
+    p.kt = 1 + (int)(step % sc.per_day);
+    return p;
+}
+
+}  // namespace
+
+extern "C" int hb_adjoint_create(hb_handle *h, const int32_t *gauges, int32_t ngauges, int32_t obs_every,
+                                 int32_t nsteps, int32_t checkpoint_every, hb_adjoint **out) {
+    if (!h || !out || !gauges || ngauges <= 0 || obs_every <= 0 || nsteps <= 0 || checkpoint_every <= 0)
+        return hb::set_error(HB_E_INVALID, "hb_adjoint_create: bad argument");
+    *out = nullptr;
+    if (h->opt.precision != HB_FP64 || h->opt.variant != HB_VARIANT_H || h->opt.layout != HB_LAYOUT_EDGE ||
+        h->scn.size() != 1)
+        return hb::set_error(HB_E_INVALID, "hb_adjoint_create: needs a single-mesh fp64 variant-H edge-layout handle");
+    if (nsteps > h->step_limit()) return hb::set_error(HB_E_INVALID, "hb_adjoint_create: %d steps beyond the boundary tables", nsteps);
+    const hb::Scenario &sc = h->scn[0];
+    const int C = sc.cells;
+    for (int i = 0; i < ngauges; i++)
+        if (gauges[i] < 0 || gauges[i] >= C) return hb::set_error(HB_E_INVALID, "hb_adjoint_create: gauge %d out of range", gauges[i]);
+    // per-slot geometry, codes and facing slots (device order); codes without a reverse are rejected
+    std::vector<double> cs4(4 * (size_t)C, 0.0), sn4(4 * (size_t)C, 0.0), side4(4 * (size_t)C, 0.0);
+    std::vector<int32_t> nbr4(4 * (size_t)C, -1), mirror4(4 * (size_t)C, -1);
+    std::vector<uint8_t> meta4(4 * (size_t)C, 0xFF);
+    auto a = new hb_adjoint();
+    a->h = h; a->C = C; a->T = nsteps; a->k = checkpoint_every; a->obs_every = obs_every; a->ng = ngauges;
+    a->nobs = nsteps / obs_every;
+    const int nrec = h->m64.nrecords;
+    std::vector<int4> rix(nrec);
+    std::vector<uint8_t> rmeta(nrec);
+    std::vector<double> rgeo(4 * (size_t)nrec);
+    int st = HB_OK;
+    auto fail = [&](int s) { delete a; return s; };
+    if (cudaMemcpy(rix.data(), h->m64.rix, nrec * sizeof(int4), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(rmeta.data(), h->m64.rmeta, nrec, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(rgeo.data(), h->m64.rgeo, 4 * (size_t)nrec * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(hb::set_error(HB_E_CUDA, "hb_adjoint_create: reading the device mesh"));
+    for (int r = 0; r < nrec; r++) {
+        const int4 ix = rix[r];
+        const int code = rmeta[r] & hb::META_CODE;
+        if (code != hb::CODE_ZERO && code != hb::CODE_K4 && code != hb::CODE_K10 && code != hb::CODE_K1)
+            return fail(hb::set_error(HB_E_INVALID, "hb_adjoint_create: boundary code %d has no reverse here (KLAS 0, 1, 4, 10 only)", code));
+        const double *g = &rgeo[4 * (size_t)r];
+        cs4[ix.z] = g[0]; sn4[ix.z] = g[1]; side4[ix.z] = g[2]; nbr4[ix.z] = ix.y; meta4[ix.z] = rmeta[r];
+        if (ix.w >= 0) {
+            // the other slot of a mirror pair: reversed normal, neighbour a, not the lower-numbered side
+            cs4[ix.w] = -g[0]; sn4[ix.w] = -g[1]; side4[ix.w] = g[2]; nbr4[ix.w] = ix.x;
+            meta4[ix.w] = (uint8_t)(hb::CODE_ZERO | hb::META_HAS_NB);
+        }
+    }
+    // The gather of cell c reads the neighbours' slots that face c through
+    // mirror4 of c's own slots: a one-to-one pairing of the slots of c that
+    // face a neighbour with the neighbour's slots that face c.
+    std::vector<char> claimed(4 * (size_t)C, 0);
+    for (int c = 0; c < C; c++)
+        for (int j = 0; j < 4; j++) {
+            const size_t s = 4 * (size_t)c + j;
+            const int nb = nbr4[s];
+            if (meta4[s] == 0xFF || nb < 0) continue;
+            for (int q = 0; q < 4; q++) {
+                const size_t t = 4 * (size_t)nb + q;
+                if (nbr4[t] == c && meta4[t] != 0xFF && !claimed[t]) { mirror4[s] = (int32_t)t; claimed[t] = 1; break; }
+            }
+            if (mirror4[s] < 0) return fail(hb::set_error(HB_E_BADMESH, "hb_adjoint_create: cell %d slot %d has no facing slot", c, j));
+        }
+    std::vector<int32_t> gauge_of(C, -1);
+    a->gauges_dev.resize(ngauges);
+    for (int g = 0; g < ngauges; g++) {
+        const int d = sc.inv[gauges[g]];
+        a->gauges_dev[g] = d;
+        gauge_of[d] = g;
+    }
+    hb::adj::AdjMesh &am = a->am;
+    double *dp;
+    int32_t *ip;
+    uint8_t *up;
+    if ((st = adj_upload(a, &dp, cs4)) != HB_OK) return fail(st);
+    am.cs4 = dp;
+    if ((st = adj_upload(a, &dp, sn4)) != HB_OK) return fail(st);
+    am.sn4 = dp;
+    if ((st = adj_upload(a, &dp, side4)) != HB_OK) return fail(st);
+    am.side4 = dp;
+    if ((st = adj_upload(a, &ip, nbr4)) != HB_OK) return fail(st);
+    am.nbr4 = ip;
+    if ((st = adj_upload(a, &ip, mirror4)) != HB_OK) return fail(st);
+    am.mirror4 = ip;
+    if ((st = adj_upload(a, &up, meta4)) != HB_OK) return fail(st);
+    am.meta4 = up;
+    if ((st = adj_upload(a, &ip, gauge_of)) != HB_OK) return fail(st);
+    am.gauge_of = ip;
+    if ((st = adj_upload(a, &a->d_gcell, a->gauges_dev)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &am.dir, 4 * (size_t)C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &am.so, 20 * (size_t)C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &am.sn, 20 * (size_t)C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &am.fnc_g, C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &am.zbc_g, C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &am.lam, 4 * (size_t)C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &a->d_res, (size_t)std::max(a->nobs, 1) * ngauges)) != HB_OK) return fail(st);
+    am.res = a->d_res;
+    am.ng = ngauges;
+    am.obs_every = obs_every;
+    const int nck = nsteps / checkpoint_every + 1;
+    if ((st = adj_alloc(a, &a->d_ckpt, (size_t)nck * 4 * C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &a->d_seg, (size_t)(checkpoint_every + 1) * 4 * C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &a->d_terms, (size_t)checkpoint_every * 16 * C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &a->d_gd, (size_t)std::max(a->nobs, 1) * ngauges)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &a->d_obs, (size_t)std::max(a->nobs, 1) * ngauges)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &a->d_z0, C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &a->d_u0, C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &a->d_v0, C)) != HB_OK) return fail(st);
+    *out = a;
+    return HB_OK;
+}
+
+extern "C" int hb_adjoint_destroy(hb_adjoint *a) {
+    delete a;
+    return HB_OK;
+}
+
+extern "C" int hb_adjoint_set_parameters(hb_adjoint *a, const double *manning_n, const double *zbc) {
+    if (!a) return hb::set_error(HB_E_INVALID, "null adjoint");
+    const hb::Scenario &sc = a->h->scn[0];
+    const int C = a->C;
+    std::vector<double> v(C);
+    if (manning_n) {
+        for (int i = 0; i < C; i++) { const double n = manning_n[sc.perm[i]]; v[i] = 9.81 * n * n; }
+        HB_CUDA_RET(cudaMemcpy(const_cast<double *>(a->h->m64.fnc), v.data(), C * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (zbc) {
+        for (int i = 0; i < C; i++) v[i] = zbc[sc.perm[i]];
+        HB_CUDA_RET(cudaMemcpy(const_cast<double *>(a->h->m64.zbc), v.data(), C * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    a->forward_done = false;
+    return HB_OK;
+}
+
+extern "C" int hb_adjoint_set_initial(hb_adjoint *a, const double *Z0, const double *U0, const double *V0) {
+    if (!a || !Z0 || !U0 || !V0) return hb::set_error(HB_E_INVALID, "hb_adjoint_set_initial: bad argument");
+    const hb::Scenario &sc = a->h->scn[0];
+    const int C = a->C;
+    std::vector<double> v(C);
+    const double *src[3] = {Z0, U0, V0};
+    double *dst[3] = {a->d_z0, a->d_u0, a->d_v0};
+    for (int k = 0; k < 3; k++) {
+        for (int i = 0; i < C; i++) v[i] = src[k][sc.perm[i]];
+        HB_CUDA_RET(cudaMemcpy(dst[k], v.data(), C * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    a->forward_done = false;
+    return HB_OK;
+}
+
+extern "C" int hb_adjoint_set_observations(hb_adjoint *a, const double *obs) {
+    if (!a || !obs) return hb::set_error(HB_E_INVALID, "hb_adjoint_set_observations: bad argument");
+    HB_CUDA_RET(cudaMemcpy(a->d_obs, obs, (size_t)a->nobs * a->ng * sizeof(double), cudaMemcpyHostToDevice));
+    return HB_OK;
+}
+
+extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_depths, void *stream) {
+    if (!a) return hb::set_error(HB_E_INVALID, "null adjoint");
+    hb_handle *h = a->h;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int C = a->C;
+    const size_t S4 = 4 * (size_t)C;
+    hb::adj::adj_init_state_kernel<<<(C + 255) / 256, 256, 0, st>>>(C, a->d_z0, a->d_u0, a->d_v0, h->m64.zbc,
+                                                                     h->scn[0].hm1, h->m64.S[0]);
+    HB_CUDA_RET(cudaGetLastError());
+    hb::adj::set_counter_kernel<<<1, 1, 0, st>>>(h->d_ctr, 0);
+    HB_CUDA_RET(cudaMemsetAsync(h->d_err, 0, sizeof(uint32_t), st));
+    h->steps_done = 0;
+    for (int t = 0; t < a->T; t++) {
+        const int par = t & 1;
+        if (t % a->k == 0)
+            HB_CUDA_RET(cudaMemcpyAsync(a->d_ckpt + (size_t)(t / a->k) * S4, h->m64.S[par], S4 * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, st));
+        TRY(hb_enqueue_steps(h, 1, st));
+        if ((t + 1) % a->obs_every == 0) {
+            const int row = (t + 1) / a->obs_every - 1;
+            hb::adj::adj_gauge_kernel<<<(a->ng + 127) / 128, 128, 0, st>>>(h->m64.S[par ^ 1], a->d_gcell, a->ng,
+                                                                           a->d_gd + (size_t)row * a->ng);
+            HB_CUDA_RET(cudaGetLastError());
+        }
+    }
+    h->steps_done = a->T;
+    HB_CUDA_RET(cudaStreamSynchronize(st));
+    uint32_t bits = 0;
+    HB_CUDA_RET(cudaMemcpy(&bits, h->d_err, sizeof bits, cudaMemcpyDeviceToHost));
+    if (bits) return hb::set_error(HB_E_NONFINITE, "hb_adjoint_forward: device error bits 0x%x", bits);
+    const size_t no = (size_t)a->nobs * a->ng;
+    std::vector<double> gd(no), ob(no), res(no);
+    HB_CUDA_RET(cudaMemcpy(gd.data(), a->d_gd, no * sizeof(double), cudaMemcpyDeviceToHost));
+    HB_CUDA_RET(cudaMemcpy(ob.data(), a->d_obs, no * sizeof(double), cudaMemcpyDeviceToHost));
+    double L = 0.0;
+    for (size_t i = 0; i < no; i++) { res[i] = gd[i] - ob[i]; L += res[i] * res[i]; }
+    HB_CUDA_RET(cudaMemcpy(a->d_res, res.data(), no * sizeof(double), cudaMemcpyHostToDevice));
+    if (loss) *loss = L;
+    if (gauge_depths) memcpy(gauge_depths, gd.data(), no * sizeof(double));
+    a->forward_done = true;
+    return HB_OK;
+}
+
+extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_zbc, void *stream) {
+    if (!a) return hb::set_error(HB_E_INVALID, "null adjoint");
+    if (!a->forward_done) return hb::set_error(HB_E_INVALID, "hb_adjoint_backward: run hb_adjoint_forward first");
+    hb_handle *h = a->h;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int C = a->C;
+    const size_t S4 = 4 * (size_t)C;
+    hb::adj::AdjMesh am = a->am;
+    HB_CUDA_RET(cudaMemsetAsync(am.fnc_g, 0, C * sizeof(double), st));
+    HB_CUDA_RET(cudaMemsetAsync(am.zbc_g, 0, C * sizeof(double), st));
+    const int cb = (C + 255) / 256;
+    hb::adj::adj_seed_kernel<<<cb, 256, 0, st>>>(C, am, a->T % a->obs_every == 0 ? a->T / a->obs_every - 1 : -1);
+    HB_CUDA_RET(cudaGetLastError());
+    const int nseg = (a->T + a->k - 1) / a->k;
+    for (int sgi = nseg - 1; sgi >= 0; sgi--) {
+        const int t0 = sgi * a->k, t1 = std::min(t0 + a->k, a->T), len = t1 - t0;
+        // recompute the segment: its states and the slot terms of its steps
+        HB_CUDA_RET(cudaMemcpyAsync(a->d_seg, a->d_ckpt + (size_t)sgi * S4, S4 * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, st));
+        for (int i = 0; i < len; i++) {
+            hb::adj::set_counter_kernel<<<1, 1, 0, st>>>(h->d_ctr, t0 + i);
+            TRY(hb_forward_step_into(h, t0 + i, a->d_seg + (size_t)i * S4, a->d_seg + (size_t)(i + 1) * S4,
+                                     a->d_terms + (size_t)i * 16 * C, st));
+        }
+        for (int i = len - 1; i >= 0; i--) {
+            const int t = t0 + i;
+            const hb::StepParams p = step_params(h, t);
+            hb::adj::adj_slot_kernel<<<(4 * C + 127) / 128, 128, 0, st>>>(h->m64, am, a->d_seg + (size_t)i * S4,
+                                                                          a->d_terms + (size_t)i * 16 * C, p);
+            HB_CUDA_RET(cudaGetLastError());
+            const int row = (t > 0 && t % a->obs_every == 0) ? t / a->obs_every - 1 : -1;
+            hb::adj::adj_gather_kernel<<<cb, 256, 0, st>>>(C, am, row);
+            HB_CUDA_RET(cudaGetLastError());
+        }
+    }
+    hb::adj::adj_init_rev_kernel<<<cb, 256, 0, st>>>(C, am, a->d_z0, h->m64.zbc);
+    HB_CUDA_RET(cudaGetLastError());
+    // leave the handle's counter where the forward left it
+    hb::adj::set_counter_kernel<<<1, 1, 0, st>>>(h->d_ctr, a->T);
+    HB_CUDA_RET(cudaStreamSynchronize(st));
+    uint32_t bits = 0;
+    HB_CUDA_RET(cudaMemcpy(&bits, h->d_err, sizeof bits, cudaMemcpyDeviceToHost));
+    if (bits) return hb::set_error(HB_E_UNDEFINED_REF, "hb_adjoint_backward: device error bits 0x%x", bits);
+    const hb::Scenario &sc = h->scn[0];
+    std::vector<double> g(C), fnc(C);
+    if (grad_n) {
+        HB_CUDA_RET(cudaMemcpy(g.data(), am.fnc_g, C * sizeof(double), cudaMemcpyDeviceToHost));
+        HB_CUDA_RET(cudaMemcpy(fnc.data(), h->m64.fnc, C * sizeof(double), cudaMemcpyDeviceToHost));
+        // FNC = 9.81 n^2: dL/dn = dL/dFNC * 2 * 9.81 * n, n = sqrt(FNC / 9.81)
+        for (int i = 0; i < C; i++) grad_n[sc.perm[i]] = g[i] * 2.0 * 9.81 * std::sqrt(fnc[i] / 9.81);
+    }
+    if (grad_zbc) {
+        HB_CUDA_RET(cudaMemcpy(g.data(), am.zbc_g, C * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < C; i++) grad_zbc[sc.perm[i]] = g[i];
+    }
+    return HB_OK;
+}

@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(THREADS, MINB) tile_kernel(DevMesh<A> m, int k
         update_one<A, VARIANT>(m, td.cell0 + c, si, p, write_flux, terms + 16 * c);
 }
 
-__global__ void tick_kernel(long long *ctr, int n) { *ctr += n; }
+static __global__ void tick_kernel(long long *ctr, int n) { *ctr += n; }
 
 // Split precision state <-> the reference's (H, Z) of one cell.  The depth is
 // kept as the fp32 pair (h, hlo) with h + hlo = H; a cell at or below the dry

@@ -174,6 +174,33 @@ int hb_last_error(void);
 const char *hb_last_error_string(void);
 const char *hb_status_string(int status);
 
+/* ---- reverse-mode adjoint (no reference counterpart) ----
+ * Gradient of a gauge loss over a rollout with respect to the per-cell
+ * Manning coefficient n (FNC = 9.81 n^2, mesh.cpp:364) and bed ZBC:
+ *   L = sum over steps t = obs_every, 2 obs_every, ..., <= nsteps and gauge
+ *       cells g of (H_t[g] - Hobs_t[g])^2,
+ * for a rollout of nsteps steps from an initial level Z0 and velocities
+ * (H0 = Z0 - ZBC where Z0 > ZBC, else H0 = HM1 and Z0 = ZBC + HM1,
+ * mesh.cpp:350-361).  Branch choices (wet/dry, Osher's wave case, clamps,
+ * fixed-point iteration counts) are those of the forward state.  The state is
+ * checkpointed every checkpoint_every steps and each segment recomputed in
+ * the backward pass.  Needs a single-mesh fp64 variant-H edge-layout handle
+ * whose boundary codes are among KLAS 0, 1, 4, 10.  The rollout runs on the
+ * handle's own mesh and state (its state is the rollout's end afterwards). */
+typedef struct hb_adjoint hb_adjoint;
+int hb_adjoint_create(hb_handle *h, const int32_t *gauges, int32_t ngauges, int32_t obs_every, int32_t nsteps,
+                      int32_t checkpoint_every, hb_adjoint **out);
+int hb_adjoint_destroy(hb_adjoint *a);
+/* Reference order [CELL]; either may be NULL (kept).  Rewrites the handle's FNC / ZBC. */
+int hb_adjoint_set_parameters(hb_adjoint *a, const double *manning_n, const double *zbc);
+int hb_adjoint_set_initial(hb_adjoint *a, const double *Z0, const double *U0, const double *V0);
+/* [nobs][ngauges], nobs = nsteps / obs_every; row r is after step (r + 1) * obs_every. */
+int hb_adjoint_set_observations(hb_adjoint *a, const double *obs);
+/* The rollout and its loss; gauge_depths ([nobs][ngauges]) may be NULL. */
+int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_depths, void *stream);
+/* dL/dn and dL/dZBC of the last forward, reference order [CELL]; either may be NULL. */
+int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_zbc, void *stream);
+
 /* ---- deck reader (cuda_native_impl/hydro-cal-src/src/mesh.cpp:5-533, cell.cpp:72-128) ---- */
 typedef struct hb_deck hb_deck;
 /* Read a hydro-cal text deck (BINFOR/, SOURCES/, BOUNDE/ under `root`). */
