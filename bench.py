@@ -1,10 +1,23 @@
 #!/usr/bin/env python
 """Benchmark: the plain fp64 hydro-cal timestep on the 207,234-cell channel.
 
-One step = CalculateFlux + UpdateCell over the whole mesh (one fused kernel
-launch here), replayed from a captured CUDA graph.  Prints ONE JSON line.
+One step = CalculateFlux + UpdateCell over the whole mesh (the flux and cell
+kernels of the edge layout, chained by programmatic dependent launch),
+replayed from a captured CUDA graph.  Prints ONE JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--extras all|none|ensemble|adjoint|split]
+
+On one GPU the line also carries the three additions, each with its error
+against fp64 (``--extras`` chooses which; ``--only-extras`` skips the main
+measurement, for profiling one of them):
+  split_207k  split precision, tile layout, on the same 207K mesh;
+  ensemble    64 independent channel scenarios in one launch per step
+              (fp64 edge layout vs split precision tile layout, autotuned),
+              1000 steps each, with the split form's depth error;
+  adjoint     gradient of the gauge loss on the 24,020-cell channel over
+              1000 steps for checkpoint intervals 10, 50, 100: its time over
+              the plain forward's.
 
 Multi-GPU: one process per GPU (torchrun); each rank runs its own replica of
 the scenario (the path has no exchange step between independent meshes), the
@@ -218,6 +231,142 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+
+# ---------------------------------------------------------------------------
+# the three additions (one GPU)
+# ---------------------------------------------------------------------------
+def _ensemble_deck_dir(spec):
+    """Pool worker: writes one ensemble scenario's deck once; returns its directory."""
+    sys.path.insert(0, os.path.join(ROOT, "hydro-bench_b200"))
+    from hydrob200 import deck as D
+    root = os.path.join(tempfile.gettempdir(), "hb_ensemble", spec["name"])
+    if not os.path.exists(os.path.join(root, "BINFOR", "TIME.DAT")):
+        tmp = root + f".tmp{os.getpid()}"
+        D.write_deck(D.ensemble_deck(spec), tmp)
+        shutil.rmtree(root, ignore_errors=True)
+        os.replace(tmp, root)
+    return root
+
+
+def _time_graph(h, steps, graph, torch):
+    """us per step of `steps` steps replayed from `graph`-step CUDA graphs (events on the stream)."""
+    graph = max(1, min(graph, steps))
+    st = torch.cuda.current_stream()
+    h.capture_graph(graph, st)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps // graph):
+        h.graph_launch(st)
+    e1.record(st)
+    h.sync(st)
+    return e0.elapsed_time(e1) * 1e3 / (graph * (steps // graph))
+
+
+def ensemble_leg(local, steps=1000, graph=100):
+    import multiprocessing as mp
+    import numpy as np
+    import torch
+    import hydrob200 as hb
+    from hydrob200 import deck as D
+    from hydrob200.accuracy import depth_error
+    specs = D.ensemble_specs(steps=steps)
+    with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
+        roots = pool.map(_ensemble_deck_dir, specs)
+    decks = [hb.Deck(r) for r in roots]
+    cells = sum(d.cells for d in decks)
+    out = {"scenarios": len(decks), "cells": cells, "steps": steps, "dt_s": 0.5,
+           "cells_range": [min(d.cells for d in decks), max(d.cells for d in decks)],
+           "l2": "not flushed: the working set (> 300 MB) exceeds L2",
+           "launch": "one launch (tile layout) or launch pair (edge layout) per step for all scenarios, "
+                     f"{graph}-step CUDA graphs"}
+    H = {}
+    for name, prec, layout, tc in (("fp64", "fp64", "edge", 0), ("split", "split", "tile", 512)):
+        b = hb.Batch(decks, precision=prec, layout=layout, tile_cells=tc, device=local)
+        best, ms = b.autotune(steps=10)
+        us = _time_graph(b, steps, graph, torch)
+        out[name] = {"us_per_step": us, "value": cells / (us * 1e-6), "unit": METRIC, "layout": layout,
+                     "tile_cells": tc or None, "tile_config": best,
+                     "autotune_us": {str(k): round(v * 1e3, 1) for k, v in ms.items()}}
+        H[name] = [b.get_state(i)["H"] for i in range(len(decks))]
+        b.close()
+    worst, wet_deep, normwise, mass = 0.0, 0.0, 0.0, 0.0
+    for i, d in enumerate(decks):
+        e = depth_error(H["split"][i], H["fp64"][i], d.mesh.hm2, d.array("area"))
+        worst, normwise, mass = max(worst, e["rel_max"]), max(normwise, e["normwise"]), max(mass, abs(e["mass_rel"]))
+        deep = H["fp64"][i] > 0.1
+        if deep.any():
+            wet_deep = max(wet_deep, float(np.max(np.abs(H["split"][i][deep] - H["fp64"][i][deep]) / H["fp64"][i][deep])))
+    out["split"]["error_vs_fp64"] = {"after_steps": steps, "rel_max_wet": worst, "rel_max_deeper_0.1m": wet_deep,
+                                     "normwise": normwise, "mass_rel_max": mass,
+                                     "wet": "H_fp64 > HM2 = 0.01 m"}
+    out["split_vs_fp64"] = out["fp64"]["us_per_step"] / out["split"]["us_per_step"]
+    return out
+
+
+def adjoint_leg(local, steps=1000, ks=(10, 50, 100)):
+    import numpy as np
+    import torch
+    import hydrob200 as hb
+    from hydrob200 import deck as D
+    from hydrob200.adjoint import Adjoint
+    d, n_true, gauges = D.adjoint_case(steps=steps)
+    root = os.path.join(tempfile.gettempdir(), f"hb_adjoint_{steps}")
+    if not os.path.exists(os.path.join(root, "BINFOR", "TIME.DAT")):
+        D.write_deck(d, root)
+    deck = hb.Deck(root)
+    s = hb.Solver(deck, device=local)
+    s.step(100)
+    s.set_position(0)
+    fwd_us = _time_graph(s, steps, 100, torch)
+    s.close()
+    out = {"cells": deck.cells, "steps": steps, "gauges": len(gauges), "obs_every": 10,
+           "forward_ms": fwd_us * steps / 1e3, "forward": "plain fp64 rollout, 100-step CUDA graphs (CUDA events)",
+           "gradient": "hb_adjoint_forward (checkpoints) + hb_adjoint_backward, host wall time after sync",
+           "by_checkpoint_interval": {}}
+    n0 = np.full(deck.cells, 0.025)
+    for k in ks:
+        a = Adjoint(deck, gauges, 10, steps, checkpoint_every=k, device=local)
+        a.set_parameters(n_true)
+        _, obs = a.forward()
+        a.set_observations(obs)
+        a.set_parameters(n0)
+        a.forward()
+        a.backward()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss, _ = a.forward()
+        t1 = time.perf_counter()
+        gn, gz = a.backward()
+        t2 = time.perf_counter()
+        out["by_checkpoint_interval"][str(k)] = {
+            "forward_ms": (t1 - t0) * 1e3, "backward_ms": (t2 - t1) * 1e3,
+            "ratio_to_forward": (t2 - t0) * 1e3 / out["forward_ms"], "loss": loss,
+            "grad_norm_n": float(np.linalg.norm(gn)), "grad_norm_zbc": float(np.linalg.norm(gz))}
+        a.close()
+    out["ratio_to_forward"] = min(v["ratio_to_forward"] for v in out["by_checkpoint_interval"].values())
+    return out
+
+
+def split_leg(deck, local, steps=900):
+    import torch
+    import hydrob200 as hb
+    from hydrob200.accuracy import depth_error
+    sp = hb.Solver(deck, precision="split", layout="tile", tile_cells=512, device=local)
+    best, _ = sp.autotune(steps=10)
+    us = _time_graph(sp, steps, 100, torch)
+    sp.close()
+    a, b = hb.Solver(deck, device=local), hb.Solver(deck, precision="split", layout="tile", tile_cells=512,
+                                                     device=local)
+    a.step(steps)
+    b.step(steps)
+    a.sync()
+    b.sync()
+    e = depth_error(b.get_state()["H"], a.get_state()["H"], deck.mesh.hm2, deck.array("area"))
+    return {"us_per_step": us, "value": deck.cells / (us * 1e-6), "unit": METRIC, "layout": "tile",
+            "tile_cells": 512, "tile_config": best, "error_vs_fp64": dict(e, after_steps=steps)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -228,6 +377,10 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--extras", default="all", choices=["all", "none", "ensemble", "adjoint", "split"])
+    ap.add_argument("--only-extras", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=1000)
+    ap.add_argument("--ensemble-steps", type=int, default=1000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -260,6 +413,13 @@ def main():
     w = 8 if args.precision == "fp64" else 4
     b_alg = alg_bytes_per_cell_step(C, edges, w)
 
+    if args.only_extras:   # one or more of the additions alone (profiling); not a bench line
+        legs = {"split": lambda: split_leg(deck, local), "ensemble": lambda: ensemble_leg(local, args.ensemble_steps),
+                "adjoint": lambda: adjoint_leg(local, args.adjoint_steps)}
+        out = {k: fn() for k, fn in legs.items() if args.extras in ("all", k)}
+        print(json.dumps(out), flush=True)
+        return 0
+
     solver = hb.Solver(deck, precision=args.precision, device=local)
     stream = torch.cuda.current_stream()
     solver.capture_graph(G, stream)
@@ -285,7 +445,7 @@ def main():
             solver.graph_launch(stream)
             e1.record(stream)
             events.append((e0, e1))
-            launches += G + 1          # G step kernels + the step-counter tick
+            launches += 2 * G + 1      # flux + cell kernel per step, and the step-counter tick
         if rem:
             flush.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -293,7 +453,7 @@ def main():
             solver.step(rem, stream)
             e1.record(stream)
             events.append((e0, e1))
-            launches += rem + 1
+            launches += 2 * rem + 1
         torch.cuda.synchronize()
         barrier()
     clocks = clk.summary()
@@ -325,7 +485,7 @@ def main():
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = world * C * args.e2e_steps / (float(t.item()) / 1e3)
-    launches_e2e = args.e2e_steps * 4
+    launches_e2e = args.e2e_steps * 5   # stage in, flux, cell, tick, stage out
 
     # stated error: a fresh 10-step run against the CPU oracle
     err = None
@@ -355,6 +515,17 @@ def main():
         except Exception as ex:
             cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "reference", "sample": f"failed: {ex}"[:200]}
 
+    extras = {}
+    if rank == 0 and world == 1 and args.extras != "none":
+        legs = {"split": lambda: split_leg(deck, local), "ensemble": lambda: ensemble_leg(local, args.ensemble_steps),
+                "adjoint": lambda: adjoint_leg(local, args.adjoint_steps)}
+        for name, fn in legs.items():
+            if args.extras in ("all", name):
+                try:
+                    extras[name if name != "split" else "split_207k"] = fn()
+                except Exception as ex:   # the bench line still prints
+                    extras[name] = {"error": f"{type(ex).__name__}: {ex}"[:300]}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": W,
@@ -376,6 +547,7 @@ def main():
             "gpu_launches_e2e": launches_e2e,
             "cpu_baseline": cpu,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

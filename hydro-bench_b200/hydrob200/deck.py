@@ -646,3 +646,43 @@ def config_ensemble(n: int = 64, seed: int = 20240604, steps: int = 1000, cmin: 
     (sigma 100 s); dt = 0.5 s.  Each domain is 5:1 with the cell area of the
     207,234-cell configuration (40 km x 8 km), bumps of 1 m."""
     return [ensemble_deck(sp) for sp in ensemble_specs(n, seed, steps, cmin, cmax, dt)]
+
+
+def centroids(deck: Deck) -> np.ndarray:
+    """[CELL, 2] centroid of every cell (mean of its nodes)."""
+    nap = deck.nap
+    nv = np.where(nap[:, 3] > 0, 4, 3)
+    pts = deck.xy[np.maximum(nap - 1, 0)]                      # [C, 4, 2]
+    pts[nv == 3, 3] = 0.0
+    return pts.sum(axis=1) / nv[:, None]
+
+
+def gaussian_field(xy: np.ndarray, corr_len: float, seed: int, spacing: Optional[float] = None) -> np.ndarray:
+    """A seeded smooth Gaussian random field of unit variance at the points xy:
+    white noise on a grid (spacing corr_len / 5) smoothed by a Gaussian kernel
+    of standard deviation corr_len / sqrt(2), so that its covariance is
+    exp(-r^2 / (2 corr_len^2)); bilinear interpolation to the points."""
+    from scipy import ndimage
+    h = spacing if spacing is not None else corr_len / 5.0
+    lo = xy.min(axis=0) - 4 * corr_len
+    hi = xy.max(axis=0) + 4 * corr_len
+    shape = tuple(int(np.ceil((hi[k] - lo[k]) / h)) + 1 for k in (1, 0))   # (ny, nx)
+    rng = np.random.default_rng(seed)
+    g = ndimage.gaussian_filter(rng.standard_normal(shape), sigma=corr_len / np.sqrt(2.0) / h, mode="wrap")
+    g /= g.std()
+    coords = np.stack([(xy[:, 1] - lo[1]) / h, (xy[:, 0] - lo[0]) / h])
+    return ndimage.map_coordinates(g, coords, order=1)
+
+
+def adjoint_case(seed: int = 20240603, steps: int = 1000, ngauges: int = 50, obs_every: int = 10,
+                 corr_len: float = 500.0):
+    """The adjoint configuration: the 24,020-cell channel (config_24k) with
+    uniform n = 0.025, the 'true' field n_true = 0.025 exp(0.2 g) for a seeded
+    smooth Gaussian random field g of correlation length 500 m, and 50 seeded
+    gauge cells observed every 10 steps.  Returns (deck, n_true, gauges)."""
+    d = config_24k(seed=seed, steps=steps)
+    g = gaussian_field(centroids(d), corr_len, seed + 17)
+    n_true = 0.025 * np.exp(0.2 * g)
+    rng = np.random.default_rng(seed + 29)
+    gauges = np.sort(rng.choice(d.cells, ngauges, replace=False))
+    return d, n_true, gauges
