@@ -18,14 +18,17 @@
 //
 // Memory: the state is kept every `checkpoint_every` = k steps; the backward
 // pass recomputes each k-step segment from its checkpoint, keeping that
-// segment's states and slot terms, then runs the segment's reverse steps:
-//   adj_slot_kernel    four lanes per cell: the update's reverse (each lane
-//                      redundantly) and lane j's slot flux reverse, writing the
-//                      slot's contributions to its own cell and its neighbour;
-//   adj_gather_kernel  per cell: the state adjoint of the step's input, from the
-//                      update's direct terms, its own slots' contributions and
-//                      those of the neighbours' slots that face it (a gather in
-//                      slot order, no atomics: the gradient is deterministic).
+// segment's states and slot terms, then runs the segment's reverse steps, one
+// kernel each (adj_step_kernel, four lanes per cell):
+//   - the state adjoint after the step, gathered from the later step's
+//     direct terms, the cell's own slots' contributions and those of the
+//     neighbours' slots that face it (fixed order, no atomics: the gradient
+//     is deterministic);
+//   - lane 0: the cell update's reverse, shared with the other lanes;
+//   - lane j: slot j's flux reverse, leaving its contributions to its own
+//     cell and its neighbour for the next (earlier) step.
+// The forward rollout is replayed from a CUDA graph of k steps whose
+// checkpoint and gauge kernels take their slot from the device step counter.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -49,76 +52,109 @@ __device__ __forceinline__ void qf_rev(double h, double u, double v, double sign
     vb += sign * (ob[2] * h * u);
 }
 
-// Reverse of osher() (functors.cu:570-712) for the case its forward picks.
-// In: the forward inputs and the adjoint fb of out[4].  Out (added): ql_b,
-// qr_b, fil_b.  cl enters only the case choice.
-__device__ void osher_rev(double cl, const double ql[3], const double qr[3], double fil, const double fb[4],
-                          double qlb[3], double qrb[3], double &filb) {
-    const double cr = A::sqrt(A::mul(A::c(9.81), qr[0]));
-    const double fir = A::sub(qr[1], A::mul(A::c(2.0), cr));
-    const double ua = A::mul(A::add(fil, fir), A::c(0.5));
-    const double ca = A::fabs(A::mul(A::sub(fil, fir), A::c(0.25)));
+// Forward values of one Osher evaluation (functors.cu:570-712) that its
+// reverse needs: the case, every piece's (h, u) and FLUX3, all computed with
+// the forward's own arithmetic (osher() in hb_physics.cuh), so the case and
+// FLUX3 are the forward's bit for bit.
+struct OsherFwd {
+    bool p1, p2, p3, p5, p6, p7;
+    double s2, s6;                       // signs of pieces 2 and 6
+    double cr, fir, us, hs, ua35, fil3, ha3, fir5, ha5, us6, hs6;
+    double fo3;
+};
+
+__device__ __forceinline__ OsherFwd osher_fwd(double cl, const double ql[3], const double qr[3], double fil) {
+    OsherFwd o;
+    o.cr = A::sqrt(A::mul(A::c(9.81), qr[0]));
+    o.fir = A::sub(qr[1], A::mul(A::c(2.0), o.cr));
+    const double ua = A::mul(A::add(fil, o.fir), A::c(0.5));
+    const double ca = A::fabs(A::mul(A::sub(fil, o.fir), A::c(0.25)));
     int k2 = 0, k1 = 0;
     if (ca < ua) k2 = 1;
     else if (ua >= 0.0 && ua < ca) k2 = 2;
     else if (ua >= -ca && ua < 0.0) k2 = 3;
     else if (ua < -ca) k2 = 4;
-    if (ql[1] < cl && qr[1] >= -cr) k1 = 1;
-    else if (ql[1] >= cl && qr[1] >= -cr) k1 = 2;
-    else if (ql[1] < cl && qr[1] < -cr) k1 = 3;
-    else if (ql[1] >= cl && qr[1] < -cr) k1 = 4;
+    if (ql[1] < cl && qr[1] >= -o.cr) k1 = 1;
+    else if (ql[1] >= cl && qr[1] >= -o.cr) k1 = 2;
+    else if (ql[1] < cl && qr[1] < -o.cr) k1 = 3;
+    else if (ql[1] >= cl && qr[1] < -o.cr) k1 = 4;
     const bool any = k1 != 0 && k2 != 0;
-    if (!any) return;
-    const bool p1 = k1 == 2 || k1 == 4;
-    const bool p2 = k2 == 1 ? (k1 == 1 || k1 == 3) : (k1 == 2 || k1 == 4);
-    const double s2 = k2 != 1 ? -1.0 : 1.0;
-    const bool p3 = k2 == 2, p5 = k2 == 3;
-    const bool p6 = k2 == 4 ? k1 <= 2 : k1 >= 3;
-    const double s6 = k2 != 4 ? -1.0 : 1.0;
-    const bool p7 = k1 >= 3;
-    // forward values of the pieces
-    const double us = fil / 3.0, hs = us * us / 9.81;
-    const double ua35 = 0.5 * (fil + fir);
-    const double fil3 = fil - ua35, ha3 = fil3 * fil3 / 39.24;
-    const double fir5 = fir - ua35, ha5 = fir5 * fir5 / 39.24;
-    const double f6 = p5 ? fir5 : fir;
-    const double us6 = f6 / 3.0, hs6 = us6 * us6 / 9.81;
+    o.p1 = any && (k1 == 2 || k1 == 4);
+    o.p2 = any && (k2 == 1 ? (k1 == 1 || k1 == 3) : (k1 == 2 || k1 == 4));
+    o.s2 = k2 != 1 ? -1.0 : 1.0;
+    o.p3 = any && k2 == 2;
+    o.p5 = any && k2 == 3;
+    o.p6 = any && (k2 == 4 ? k1 <= 2 : k1 >= 3);
+    o.s6 = k2 != 4 ? -1.0 : 1.0;
+    o.p7 = any && k1 >= 3;
+    o.us = A::divk(fil, 3.0);
+    o.hs = A::divk(A::mul(o.us, o.us), 9.81);
+    o.ua35 = A::mul(A::add(fil, o.fir), A::c(0.5));
+    o.fil3 = A::sub(fil, o.ua35);
+    o.ha3 = A::divk(A::mul(o.fil3, o.fil3), 39.24);
+    o.fir5 = A::sub(o.fir, o.ua35);
+    o.ha5 = A::divk(A::mul(o.fir5, o.fir5), 39.24);
+    o.us6 = A::divk(o.p5 ? o.fir5 : o.fir, 3.0);
+    o.hs6 = A::divk(A::mul(o.us6, o.us6), 9.81);
+    // FLUX3 as qf_acc_if sums it: out3 += +-4.905 h * h over the active pieces in order
+    double o3 = 0.0;
+    auto acc = [&](bool on, double sign, double h) {
+        const double h4 = A::mul(A::c(4.905), h);
+        const double v = A::madd(sign < 0 ? -h4 : h4, h, o3, M_ACC123);
+        if (on) o3 = v;
+    };
+    acc(o.p1, 1.0, ql[0]);
+    acc(o.p2, o.s2, o.hs);
+    acc(o.p3, 1.0, o.ha3);
+    acc(o.p5, 1.0, o.ha5);
+    acc(o.p6, o.s6, o.hs6);
+    acc(o.p7, 1.0, qr[0]);
+    o.fo3 = o3;
+    return o;
+}
+
+// Reverse of osher() for the case its forward picked.  In: the forward values
+// and the adjoint fb of out[4].  Out (added): ql_b, qr_b, fil_b.  cl enters
+// only the case choice.
+__device__ __forceinline__ void osher_rev(const OsherFwd &o, const double ql[3], const double qr[3], const double fb[4],
+                                          double qlb[3], double qrb[3], double &filb) {
+    constexpr double R3 = 1.0 / 3.0, R981 = 1.0 / 9.81, R3924 = 1.0 / 39.24;
     double firb = 0.0, ua35b = 0.0, fir5b = 0.0;
-    if (p1) qf_rev(ql[0], ql[1], ql[2], 1.0, fb, qlb[0], qlb[1], qlb[2]);
-    if (p2) {
+    if (o.p1) qf_rev(ql[0], ql[1], ql[2], 1.0, fb, qlb[0], qlb[1], qlb[2]);
+    if (o.p2) {
         double hsb = 0.0, usb = 0.0;
-        qf_rev(hs, us, ql[2], s2, fb, hsb, usb, qlb[2]);
-        usb += hsb * 2.0 * us / 9.81;
-        filb += usb / 3.0;
+        qf_rev(o.hs, o.us, ql[2], o.s2, fb, hsb, usb, qlb[2]);
+        usb += hsb * 2.0 * o.us * R981;
+        filb += usb * R3;
     }
-    if (p3) {
+    if (o.p3) {
         double hab = 0.0;
-        qf_rev(ha3, ua35, ql[2], 1.0, fb, hab, ua35b, qlb[2]);
-        const double fil3b = hab * 2.0 * fil3 / 39.24;
+        qf_rev(o.ha3, o.ua35, ql[2], 1.0, fb, hab, ua35b, qlb[2]);
+        const double fil3b = hab * 2.0 * o.fil3 * R3924;
         filb += fil3b;
         ua35b -= fil3b;
     }
-    if (p5) {
+    if (o.p5) {
         double hab = 0.0;
-        qf_rev(ha5, ua35, qr[2], 1.0, fb, hab, ua35b, qrb[2]);
-        fir5b += hab * 2.0 * fir5 / 39.24;
+        qf_rev(o.ha5, o.ua35, qr[2], 1.0, fb, hab, ua35b, qrb[2]);
+        fir5b += hab * 2.0 * o.fir5 * R3924;
     }
-    if (p6) {
+    if (o.p6) {
         double hsb = 0.0, usb = 0.0;
-        qf_rev(hs6, us6, qr[2], s6, fb, hsb, usb, qrb[2]);
-        usb += hsb * 2.0 * us6 / 9.81;
-        const double f6b = usb / 3.0;
-        if (p5) fir5b += f6b;
+        qf_rev(o.hs6, o.us6, qr[2], o.s6, fb, hsb, usb, qrb[2]);
+        usb += hsb * 2.0 * o.us6 * R981;
+        const double f6b = usb * R3;
+        if (o.p5) fir5b += f6b;
         else firb += f6b;
     }
-    if (p7) qf_rev(qr[0], qr[1], qr[2], 1.0, fb, qrb[0], qrb[1], qrb[2]);
+    if (o.p7) qf_rev(qr[0], qr[1], qr[2], 1.0, fb, qrb[0], qrb[1], qrb[2]);
     firb += fir5b;
     ua35b -= fir5b;
     filb += 0.5 * ua35b;
     firb += 0.5 * ua35b;
     qrb[1] += firb;
     const double crb = -2.0 * firb;
-    if (cr > 0.0) qrb[0] += crb * 9.81 / (2.0 * cr);
+    if (o.cr > 0.0) qrb[0] += crb * 9.81 * 0.5 / o.cr;
 }
 
 // Reverse of the Osher route of a slot (functors.cu:151-200): left cell L,
@@ -129,22 +165,21 @@ __device__ void osher_route_rev(const CellStateA<A> &L, const CellStateA<A> &R, 
     const double HM1 = p.hm1, HM2 = p.hm2;
     const double clL = A::sqrt(A::mul(A::c(9.81), L.h));
     const OsherIn<double> oi = osher_inputs<A>(L, R, cs, sn, clL, mir, p);
-    double fo[4];
-    osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo);
+    const OsherFwd of = osher_fwd(oi.cl, oi.ql, oi.qr, oi.fil);
     // outputs: F0 = +-fo0, F1 = fo1 + (1-ratio) hcR ur^2 / 2, F2 = fo2, F3 = fo3 or mirror_f3(fo3)
     double fob[4] = {mir ? -fb[0] : fb[0], fb[1], fb[2], 0.0};
     if (!mir) {
         fob[3] = fb[3];
     } else {
         // F3 = 4.905 hc3^2, hc3 = za - ZBC_R where za = sqrt(fo3/4.905) + ZBC_L > ZBC_R (functors.cu:191-199)
-        const double za = A::ladd(A::lvl(A::sqrt(A::divk(fo[3], 4.905))), L.zbc);
+        const double za = A::ladd(A::lvl(A::sqrt(A::divk(of.fo3, 4.905))), L.zbc);
         if (za > R.zbc) {
             const double hc3 = za - R.zbc;
             const double hc3b = fb[3] * 9.81 * hc3;
             Rb.b -= hc3b;
             Lb.b += hc3b;
-            const double t = sqrt(fo[3] / 4.905);
-            if (t > 0.0) fob[3] = hc3b / (2.0 * t) / 4.905;
+            const double t = sqrt(of.fo3 * (1.0 / 4.905));
+            if (t > 0.0) fob[3] = hc3b * (0.5 / 4.905) / t;
         }
     }
     double ratiob = 0.0, hcRb = 0.0, urb = 0.0;
@@ -152,10 +187,10 @@ __device__ void osher_route_rev(const CellStateA<A> &L, const CellStateA<A> &R, 
     hcRb += fb[1] * (1.0 - oi.ratio) * oi.ur * oi.ur * 0.5;
     urb += fb[1] * (1.0 - oi.ratio) * oi.hcR * oi.ur;
     double qlb[3] = {0, 0, 0}, qrb[3] = {0, 0, 0}, filb = 0.0;
-    osher_rev(oi.cl, oi.ql, oi.qr, oi.fil, fob, qlb, qrb, filb);
+    osher_rev(of, oi.ql, oi.qr, fob, qlb, qrb, filb);
     // fil = ql1 + 2 clL, clL = sqrt(9.81 h_L)
     qlb[1] += filb;
-    if (clL > 0.0) Lb.h += 2.0 * filb * 9.81 / (2.0 * clL);
+    if (clL > 0.0) Lb.h += filb * 9.81 / clL;
     // ql = (h_L, u_L cs + v_L sn, v_L cs - u_L sn)
     Lb.h += qlb[0];
     Lb.u += qlb[1] * cs - qlb[2] * sn;
@@ -375,18 +410,16 @@ __device__ void slot_rev(const SlotInA<A> &in, const StepParams &p, const TableF
             go.h += fb[1] * ql1 * ql1 + fb[3] * 9.81 * h1;
             ql1b += fb[1] * 2.0 * h1 * ql1;
         }
-    } else if (in.code == CODE_ZERO && in.own_first) {
-        Adj5 lb{0, 0, 0, 0, 0}, rb{0, 0, 0, 0, 0};
-        osher_route_rev(in.own, in.nb, cs, sn, false, p, fb, lb, rb);
-        go.h += lb.h; go.u += lb.u; go.v += lb.v; go.z += lb.z; go.b += lb.b;
-        gn.h += rb.h; gn.u += rb.u; gn.v += rb.v; gn.z += rb.z; gn.b += rb.b;
-    } else if (!in.has_nb) {
+    } else if (!(in.code == CODE_ZERO && in.own_first) && !in.has_nb) {
         atomicOr(err, ERRBIT_UNDEFINED);
     } else {
+        // Osher: direct from the lower-numbered side, mirrored otherwise (one call site)
+        const bool mir = !(in.code == CODE_ZERO && in.own_first);
         Adj5 lb{0, 0, 0, 0, 0}, rb{0, 0, 0, 0, 0};
-        osher_route_rev(in.nb, in.own, -cs, -sn, true, p, fb, lb, rb);
-        gn.h += lb.h; gn.u += lb.u; gn.v += lb.v; gn.z += lb.z; gn.b += lb.b;
-        go.h += rb.h; go.u += rb.u; go.v += rb.v; go.z += rb.z; go.b += rb.b;
+        osher_route_rev(mir ? in.nb : in.own, mir ? in.own : in.nb, mir ? -cs : cs, mir ? -sn : sn, mir, p, fb, lb, rb);
+        Adj5 &gl = mir ? gn : go, &gr = mir ? go : gn;
+        gl.h += lb.h; gl.u += lb.u; gl.v += lb.v; gl.z += lb.z; gl.b += lb.b;
+        gr.h += rb.h; gr.u += rb.u; gr.v += rb.v; gr.z += rb.z; gr.b += rb.b;
     }
     // ql = (h1, u1 cs + v1 sn, v1 cs - u1 sn)
     go.u += ql1b * cs - ql2b * sn;
@@ -411,79 +444,127 @@ struct AdjMesh {
     const int32_t *nbr4, *mirror4;
     const uint8_t *meta4;        // code | own_first | has_nb; 0xFF = no real slot
     const int32_t *gauge_of;     // [C] gauge index of the cell, -1
-    double *dir;                 // [C][4] the update's direct terms of the state adjoint
-    double *so, *sn;             // [4C][5] a slot's contributions to its own cell and to its neighbour
     double *fnc_g, *zbc_g;       // [C] accumulated gradients
-    double *lam;                 // [C][4] state adjoint {H, U, V, Z}
+    double *lam;                 // [C][4] state adjoint {H, U, V, Z} (the seed, and at the end that of x_0)
     const double *res;           // [nobs][ng] residuals H - Hobs
     int ng, obs_every;
 };
 
-// One reverse step t: four lanes per cell.  x: the state before the step;
-// terms: the forward's slot terms of the step; a.lam: adjoint of the state
-// after the step.
-__global__ void __launch_bounds__(128) adj_slot_kernel(DevMesh<A> m, AdjMesh a, const double *__restrict__ x,
-                                                       const double *__restrict__ terms, StepParams p) {
+// What one reverse step leaves for the next (earlier) one: per cell the
+// update's direct terms of the state adjoint; per slot its contributions to
+// its own cell and to its neighbour ({h, u, v, z, zbc} each).  Two copies,
+// step t writing copy (t & 1) and reading the other.
+struct AdjStepBufs {
+    const double *dir_in, *so_in, *sn_in;   // step t + 1's
+    double *dir_out, *so_out, *sn_out;       // step t's
+};
+
+// lambda(c) = dir(c) + sum_j so[4c+j] + sum_j sn[mirror(4c+j)] (+ the loss
+// term of observation row `obs_row`) and c's bed terms, by the four lanes of
+// cell c: lane j adds slot j's pair of contributions, a butterfly over the
+// four lanes sums them.  Every lane of the warp must call this.
+__device__ __forceinline__ void gather4(const AdjMesh &a, const double *dir, const double *so, const double *sn,
+                                        int c, int j, int obs_row, double l[4], double &zg) {
+    const size_t s = 4 * (size_t)c + j;
+    double part[5];
+    for (int q = 0; q < 5; q++) part[q] = so[5 * s + q];
+    const int mj = a.mirror4[s];
+    if (mj >= 0)
+        for (int q = 0; q < 5; q++) part[q] += sn[5 * (size_t)mj + q];
+    for (int q = 0; q < 5; q++) {
+        part[q] += __shfl_xor_sync(0xffffffffu, part[q], 1);
+        part[q] += __shfl_xor_sync(0xffffffffu, part[q], 2);
+    }
+    for (int q = 0; q < 4; q++) l[q] = dir[4 * (size_t)c + q] + part[q];
+    zg = part[4];
+    if (obs_row >= 0) {
+        const int g = a.gauge_of[c];
+        if (g >= 0) l[0] += 2.0 * a.res[(size_t)obs_row * a.ng + g];
+    }
+}
+
+// One reverse step t, four lanes per cell.  x: the state before the step;
+// terms: the forward's slot terms of the step.  The adjoint of the state after
+// the step is gathered first from step t + 1's contributions (`first`: it is
+// the seed a.lam instead), with the loss term of row `obs_row` when step t + 1
+// ends on an observation.  Lane 0 reverses the cell update and shares the
+// adjoints of the slot sums; lane j then reverses slot j.
+__global__ void __launch_bounds__(128) adj_step_kernel(DevMesh<A> m, AdjMesh a, AdjStepBufs b,
+                                                       const double *__restrict__ x, const double *__restrict__ terms,
+                                                       StepParams p, int first, int obs_row) {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int c = gid >> 2, j = gid & 3;
-    if (c >= m.C) return;
+    const bool valid = (gid >> 2) < m.C;
+    const int c = valid ? gid >> 2 : m.C - 1, j = gid & 3;
+    const int lane0 = (int)(threadIdx.x & 31) & ~3;
+    double l[4], zg = 0.0;
+    if (first) {
+        for (int q = 0; q < 4; q++) l[q] = a.lam[4 * (size_t)c + q];
+    } else {
+        gather4(a, b.dir_in, b.so_in, b.sn_in, c, j, obs_row, l, zg);
+    }
     const double hv = x[4 * (size_t)c], uv = x[4 * (size_t)c + 1], vv = x[4 * (size_t)c + 2];
     const double zbc = m.zbc[c];
-    // ---- the update (UpdateCellKernel, functors.cu:717-784, variant H), forward values
-    double wh = 0.0, wu = 0.0, wv = 0.0;
-    const unsigned mask = m.cmask[c];
-    for (int q = 0; q < 4; q++) {
-        if (!(mask & (1u << q))) continue;
-        const double *t = terms + 16 * (size_t)c + 4 * q;
-        wh = A::madd(t[3], t[0], wh, M_WH);
-        wu = A::add(wu, t[1]);
-        wv = A::add(wv, t[2]);
-    }
-    const double HM1 = p.hm1, HM2 = p.hm2, DT = p.dt;
-    const double dta = m.dta[c], fnc = m.fnc[c];
-    const double h2raw = A::add(A::madd(-dta, wh, hv, M_H2), A::c(K::QLUA));
-    const double h2 = A::fmax(h2raw, HM1);
-    const double lh = a.lam[4 * (size_t)c], lu = a.lam[4 * (size_t)c + 1], lv = a.lam[4 * (size_t)c + 2],
-                 lz = a.lam[4 * (size_t)c + 3];
-    double h2b = lh + lz;   // Z2 = H2 + ZBC
-    double hb = 0.0, ub = 0.0, vb = 0.0, whb = 0.0, wub = 0.0, wvb = 0.0, fncb = 0.0;
-    if (h2 > HM2) {
-        const double s2 = A::dot(uv, uv, vv, vv, M_SQ1);
-        const double s = A::sqrt(s2);
-        const double hp = A::pow(hv, A::c(0.33333));
-        const double wsf = A::div(A::mul(fnc, s), hp);
-        const double dtw = A::mul(DT, wsf);
-        const double u2 = A::div(A::madd(-dtw, uv, A::dot(hv, uv, -dta, wu, M_U2A), M_U2B), h2);
-        const double v2 = A::div(A::madd(-dtw, vv, A::dot(hv, vv, -dta, wv, M_U2A), M_U2B), h2);
-        const double ue = fabs(u2) < 15.0 ? lu : 0.0;
-        const double ve = fabs(v2) < 15.0 ? lv : 0.0;
-        const double nub = ue / h2, nvb = ve / h2;
-        h2b -= ue * u2 / h2 + ve * v2 / h2;
-        hb += nub * uv + nvb * vv;
-        ub += nub * (hv - dtw);
-        vb += nvb * (hv - dtw);
-        wub -= nub * dta;
-        wvb -= nvb * dta;
-        const double dtwb = -(nub * uv + nvb * vv);
-        // dtw = DT fnc s / h^p
-        fncb += dtwb * DT * s / hp;
-        const double sb = dtwb * DT * fnc / hp;
-        hb += dtwb * DT * fnc * s * (-0.33333) / (hp * hv);
-        if (s > 0.0) { ub += sb * uv / s; vb += sb * vv / s; }
-    } else if (h2 > HM1) {
-        if (fabs(uv) < K::VMIN) ub += lu;
-        if (fabs(vv) < K::VMIN) vb += lv;
-    }
-    if (h2raw > HM1) { hb += h2b; whb -= h2b * dta; }
+    double whb = 0.0, wub = 0.0, wvb = 0.0;
     if (j == 0) {
-        double *d = a.dir + 4 * (size_t)c;
-        d[0] = hb; d[1] = ub; d[2] = vb; d[3] = 0.0;
-        a.fnc_g[c] += fncb;
-        a.zbc_g[c] += lz;
+        // ---- the update (UpdateCellKernel, functors.cu:717-784, variant H): forward values, then its reverse
+        double wh = 0.0, wu = 0.0, wv = 0.0;
+        const unsigned mask = m.cmask[c];
+        for (int q = 0; q < 4; q++) {
+            if (!(mask & (1u << q))) continue;
+            const double *t = terms + 16 * (size_t)c + 4 * q;
+            wh = A::madd(t[3], t[0], wh, M_WH);
+            wu = A::add(wu, t[1]);
+            wv = A::add(wv, t[2]);
+        }
+        const double HM1 = p.hm1, HM2 = p.hm2, DT = p.dt;
+        const double dta = m.dta[c], fnc = m.fnc[c];
+        const double h2raw = A::add(A::madd(-dta, wh, hv, M_H2), A::c(K::QLUA));
+        const double h2 = A::fmax(h2raw, HM1);
+        double h2b = l[0] + l[3];   // Z2 = H2 + ZBC
+        double hb = 0.0, ub = 0.0, vb = 0.0, fncb = 0.0;
+        if (h2 > HM2) {
+            const double s2 = A::dot(uv, uv, vv, vv, M_SQ1);
+            const double sq = A::sqrt(s2);
+            const double hp = A::pow(hv, A::c(0.33333));
+            const double wsf = A::div(A::mul(fnc, sq), hp);
+            const double dtw = A::mul(DT, wsf);
+            const double u2 = A::div(A::madd(-dtw, uv, A::dot(hv, uv, -dta, wu, M_U2A), M_U2B), h2);
+            const double v2 = A::div(A::madd(-dtw, vv, A::dot(hv, vv, -dta, wv, M_U2A), M_U2B), h2);
+            const double ih2 = 1.0 / h2, ihp = 1.0 / hp;
+            const double ue = fabs(u2) < 15.0 ? l[1] : 0.0;
+            const double ve = fabs(v2) < 15.0 ? l[2] : 0.0;
+            const double nub = ue * ih2, nvb = ve * ih2;
+            h2b -= (ue * u2 + ve * v2) * ih2;
+            hb += nub * uv + nvb * vv;
+            ub += nub * (hv - dtw);
+            vb += nvb * (hv - dtw);
+            wub -= nub * dta;
+            wvb -= nvb * dta;
+            const double dtwb = -(nub * uv + nvb * vv);
+            // dtw = DT fnc s / h^p
+            fncb += dtwb * DT * sq * ihp;
+            const double sb = dtwb * DT * fnc * ihp;
+            hb += dtwb * DT * fnc * sq * (-0.33333) * ihp / hv;
+            if (sq > 0.0) { const double is = 1.0 / sq; ub += sb * uv * is; vb += sb * vv * is; }
+        } else if (h2 > HM1) {
+            if (fabs(uv) < K::VMIN) ub += l[1];
+            if (fabs(vv) < K::VMIN) vb += l[2];
+        }
+        if (h2raw > HM1) { hb += h2b; whb -= h2b * dta; }
+        if (valid) {
+            double *d = b.dir_out + 4 * (size_t)c;
+            d[0] = hb; d[1] = ub; d[2] = vb; d[3] = 0.0;
+            a.fnc_g[c] += fncb;
+            a.zbc_g[c] += l[3] + zg;
+        }
     }
+    whb = __shfl_sync(0xffffffffu, whb, lane0);
+    wub = __shfl_sync(0xffffffffu, wub, lane0);
+    wvb = __shfl_sync(0xffffffffu, wvb, lane0);
+    if (!valid) return;
     // ---- lane j: slot 4c+j
     const size_t s = 4 * (size_t)c + j;
-    double *so = a.so + 5 * s, *sno = a.sn + 5 * s;
+    double *so = b.so_out + 5 * s, *sno = b.sn_out + 5 * s;
     const uint8_t meta = a.meta4[s];
     if (meta == 0xFF) {
         for (int q = 0; q < 5; q++) { so[q] = 0.0; sno[q] = 0.0; }
@@ -529,29 +610,14 @@ __global__ void __launch_bounds__(128) adj_slot_kernel(DevMesh<A> m, AdjMesh a, 
     sno[0] = gn.h; sno[1] = gn.u; sno[2] = gn.v; sno[3] = gn.z; sno[4] = gn.b;
 }
 
-// State adjoint of step t's input, per cell, in slot order; then the loss
-// term of observation step t.  `obs_row` = t / obs_every - 1 when t is an
-// observation step (t > 0), else -1.
-__global__ void adj_gather_kernel(int C, AdjMesh a, int obs_row) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= C) return;
-    double l[4] = {a.dir[4 * (size_t)c], a.dir[4 * (size_t)c + 1], a.dir[4 * (size_t)c + 2], a.dir[4 * (size_t)c + 3]};
-    double zg = 0.0;
-    for (int j = 0; j < 4; j++) {
-        const double *so = a.so + 5 * (4 * (size_t)c + j);
-        for (int q = 0; q < 4; q++) l[q] += so[q];
-        zg += so[4];
-        const int mj = a.mirror4[4 * (size_t)c + j];
-        if (mj >= 0) {
-            const double *sn = a.sn + 5 * (size_t)mj;
-            for (int q = 0; q < 4; q++) l[q] += sn[q];
-            zg += sn[4];
-        }
-    }
-    if (obs_row >= 0) {
-        const int g = a.gauge_of[c];
-        if (g >= 0) l[0] += 2.0 * a.res[(size_t)obs_row * a.ng + g];
-    }
+// The adjoint of x_0 from step 0's contributions, into a.lam, with their bed terms.
+__global__ void adj_gather_kernel(int C, AdjMesh a, const double *dir, const double *so, const double *sn) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = (gid >> 2) < C;
+    const int c = valid ? gid >> 2 : C - 1, j = gid & 3;
+    double l[4], zg;
+    gather4(a, dir, so, sn, c, j, -1, l, zg);
+    if (!valid || j != 0) return;
     for (int q = 0; q < 4; q++) a.lam[4 * (size_t)c + q] = l[q];
     a.zbc_g[c] += zg;
 }
@@ -589,13 +655,28 @@ __global__ void adj_init_rev_kernel(int C, AdjMesh a, const double *__restrict__
     else a.zbc_g[c] -= a.lam[4 * (size_t)c];                        // H0 = Z0 - ZBC
 }
 
-// depths of the gauge cells after a step, into gd [ng]
-__global__ void adj_gauge_kernel(const double *__restrict__ S, const int32_t *__restrict__ gcell, int ng, double *gd) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g < ng) gd[g] = S[4 * (size_t)gcell[g]];
+__global__ void set_counter_kernel(long long *ctr, long long v) { *ctr = v; }
+
+// the state before step t = *ctr into checkpoint t / k (when t is a multiple of k)
+__global__ void ckpt_kernel(const double *S0, const double *S1, double *ckpt, const long long *ctr, int k,
+                            size_t n) {
+    const long long t = *ctr;
+    if (t % k != 0) return;
+    const double *src = (t & 1) ? S1 : S0;
+    double *dst = ckpt + (size_t)(t / k) * n;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
 }
 
-__global__ void set_counter_kernel(long long *ctr, long long v) { *ctr = v; }
+// after t = *ctr steps, when t ends on an observation: the gauge depths into row t / obs_every - 1
+__global__ void gauge_ctr_kernel(const double *S0, const double *S1, const int32_t *__restrict__ gcell, int ng,
+                                 double *gd, const long long *ctr, int obs_every) {
+    const long long t = *ctr;
+    if (t == 0 || t % obs_every != 0) return;
+    const double *S = (t & 1) ? S1 : S0;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < ng) gd[(size_t)(t / obs_every - 1) * ng + g] = S[4 * (size_t)gcell[g]];
+}
 
 }  // namespace adj
 }  // namespace hb
@@ -616,9 +697,16 @@ struct hb_adjoint {
     double *d_obs = nullptr;                // [nobs][ng]
     double *d_res = nullptr;                // [nobs][ng]
     double *d_z0 = nullptr, *d_u0 = nullptr, *d_v0 = nullptr;   // initial level and velocities (device order)
+    double *d_dir[2] = {nullptr, nullptr};  // [C][4] the update's direct terms, by step parity
+    double *d_so[2] = {nullptr, nullptr};   // [4C][5] slots' contributions to their own cells
+    double *d_sn[2] = {nullptr, nullptr};   // [4C][5] slots' contributions to their neighbours
     hb::adj::AdjMesh am{};
+    cudaGraphExec_t fwd_graph = nullptr;    // k forward steps with checkpoint and gauge kernels
     bool forward_done = false;
-    ~hb_adjoint() { for (void *p : allocs) cudaFree(p); }
+    ~hb_adjoint() {
+        if (fwd_graph) cudaGraphExecDestroy(fwd_graph);
+        for (void *p : allocs) cudaFree(p);
+    }
 };
 
 namespace {
@@ -736,9 +824,11 @@ extern "C" int hb_adjoint_create(hb_handle *h, const int32_t *gauges, int32_t ng
     if ((st = adj_upload(a, &ip, gauge_of)) != HB_OK) return fail(st);
     am.gauge_of = ip;
     if ((st = adj_upload(a, &a->d_gcell, a->gauges_dev)) != HB_OK) return fail(st);
-    if ((st = adj_alloc(a, &am.dir, 4 * (size_t)C)) != HB_OK) return fail(st);
-    if ((st = adj_alloc(a, &am.so, 20 * (size_t)C)) != HB_OK) return fail(st);
-    if ((st = adj_alloc(a, &am.sn, 20 * (size_t)C)) != HB_OK) return fail(st);
+    for (int q = 0; q < 2; q++) {
+        if ((st = adj_alloc(a, &a->d_dir[q], 4 * (size_t)C)) != HB_OK) return fail(st);
+        if ((st = adj_alloc(a, &a->d_so[q], 20 * (size_t)C)) != HB_OK) return fail(st);
+        if ((st = adj_alloc(a, &a->d_sn[q], 20 * (size_t)C)) != HB_OK) return fail(st);
+    }
     if ((st = adj_alloc(a, &am.fnc_g, C)) != HB_OK) return fail(st);
     if ((st = adj_alloc(a, &am.zbc_g, C)) != HB_OK) return fail(st);
     if ((st = adj_alloc(a, &am.lam, 4 * (size_t)C)) != HB_OK) return fail(st);
@@ -814,19 +904,43 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
     hb::adj::set_counter_kernel<<<1, 1, 0, st>>>(h->d_ctr, 0);
     HB_CUDA_RET(cudaMemsetAsync(h->d_err, 0, sizeof(uint32_t), st));
     h->steps_done = 0;
-    for (int t = 0; t < a->T; t++) {
-        const int par = t & 1;
-        if (t % a->k == 0)
-            HB_CUDA_RET(cudaMemcpyAsync(a->d_ckpt + (size_t)(t / a->k) * S4, h->m64.S[par], S4 * sizeof(double),
-                                        cudaMemcpyDeviceToDevice, st));
-        TRY(hb_enqueue_steps(h, 1, st));
-        if ((t + 1) % a->obs_every == 0) {
-            const int row = (t + 1) / a->obs_every - 1;
-            hb::adj::adj_gauge_kernel<<<(a->ng + 127) / 128, 128, 0, st>>>(h->m64.S[par ^ 1], a->d_gcell, a->ng,
-                                                                           a->d_gd + (size_t)row * a->ng);
+    // forward steps t0 .. t0+n-1: checkpoint at the segment's start, gauge
+    // depths after every step that ends on an observation (positions fixed
+    // when k is a multiple of obs_every, otherwise after every step)
+    auto enqueue = [&](int t0, int n, cudaStream_t s) -> int {
+        const double *S0 = h->m64.S[0], *S1 = h->m64.S[1];
+        hb::adj::ckpt_kernel<<<64, 256, 0, s>>>(S0, S1, a->d_ckpt, h->d_ctr, a->k, S4);
+        HB_CUDA_RET(cudaGetLastError());
+        // runs of steps up to each observation: one multi-step launch sequence each
+        for (int i = 0; i < n;) {
+            int m = n - i;
+            if (a->k % a->obs_every == 0) m = std::min(m, a->obs_every - (t0 + i) % a->obs_every);
+            else m = 1;
+            TRY(hb_enqueue_steps(h, m, s));
+            i += m;
+            hb::adj::gauge_ctr_kernel<<<(a->ng + 127) / 128, 128, 0, s>>>(S0, S1, a->d_gcell, a->ng, a->d_gd,
+                                                                          h->d_ctr, a->obs_every);
             HB_CUDA_RET(cudaGetLastError());
         }
+        return HB_OK;
+    };
+    const int nfull = a->T / a->k;
+    if (nfull > 0 && !a->fwd_graph) {
+        cudaStream_t cap;
+        HB_CUDA_RET(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        HB_CUDA_RET(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue(0, a->k, cap);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (rc != HB_OK) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return hb::set_error(HB_E_CUDA, "adjoint forward capture: %s", cudaGetErrorString(e));
+        const cudaError_t ei = cudaGraphInstantiate(&a->fwd_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) { a->fwd_graph = nullptr; return hb::set_error(HB_E_CUDA, "adjoint forward graph: %s", cudaGetErrorString(ei)); }
     }
+    for (int sgi = 0; sgi < nfull; sgi++) HB_CUDA_RET(cudaGraphLaunch(a->fwd_graph, st));
+    if (a->T % a->k) TRY(enqueue(nfull * a->k, a->T % a->k, st));
     h->steps_done = a->T;
     HB_CUDA_RET(cudaStreamSynchronize(st));
     uint32_t bits = 0;
@@ -864,22 +978,25 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
         // recompute the segment: its states and the slot terms of its steps
         HB_CUDA_RET(cudaMemcpyAsync(a->d_seg, a->d_ckpt + (size_t)sgi * S4, S4 * sizeof(double),
                                     cudaMemcpyDeviceToDevice, st));
-        for (int i = 0; i < len; i++) {
-            hb::adj::set_counter_kernel<<<1, 1, 0, st>>>(h->d_ctr, t0 + i);
-            TRY(hb_forward_step_into(h, t0 + i, a->d_seg + (size_t)i * S4, a->d_seg + (size_t)(i + 1) * S4,
+        hb::adj::set_counter_kernel<<<1, 1, 0, st>>>(h->d_ctr, t0);
+        for (int i = 0; i < len; i++)
+            TRY(hb_forward_step_into(h, t0, i, a->d_seg + (size_t)i * S4, a->d_seg + (size_t)(i + 1) * S4,
                                      a->d_terms + (size_t)i * 16 * C, st));
-        }
         for (int i = len - 1; i >= 0; i--) {
             const int t = t0 + i;
             const hb::StepParams p = step_params(h, t);
-            hb::adj::adj_slot_kernel<<<(4 * C + 127) / 128, 128, 0, st>>>(h->m64, am, a->d_seg + (size_t)i * S4,
-                                                                          a->d_terms + (size_t)i * 16 * C, p);
-            HB_CUDA_RET(cudaGetLastError());
-            const int row = (t > 0 && t % a->obs_every == 0) ? t / a->obs_every - 1 : -1;
-            hb::adj::adj_gather_kernel<<<cb, 256, 0, st>>>(C, am, row);
+            const int w = t & 1;
+            const hb::adj::AdjStepBufs bufs{a->d_dir[w ^ 1], a->d_so[w ^ 1], a->d_sn[w ^ 1],
+                                            a->d_dir[w], a->d_so[w], a->d_sn[w]};
+            const int row = (t + 1 < a->T && (t + 1) % a->obs_every == 0) ? (t + 1) / a->obs_every - 1 : -1;
+            hb::adj::adj_step_kernel<<<(4 * C + 127) / 128, 128, 0, st>>>(
+                h->m64, am, bufs, a->d_seg + (size_t)i * S4, a->d_terms + (size_t)i * 16 * C, p, t == a->T - 1, row);
             HB_CUDA_RET(cudaGetLastError());
         }
     }
+    // the adjoint of x_0 (step 0 wrote copy 0)
+    hb::adj::adj_gather_kernel<<<(4 * C + 127) / 128, 128, 0, st>>>(C, am, a->d_dir[0], a->d_so[0], a->d_sn[0]);
+    HB_CUDA_RET(cudaGetLastError());
     hb::adj::adj_init_rev_kernel<<<cb, 256, 0, st>>>(C, am, a->d_z0, h->m64.zbc);
     HB_CUDA_RET(cudaGetLastError());
     // leave the handle's counter where the forward left it

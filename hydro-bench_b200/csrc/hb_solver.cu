@@ -692,16 +692,17 @@ int check_range(hb_handle *h, long long n) {
 int hb_enqueue_steps(hb_handle *h, int n, cudaStream_t st) { return enqueue_steps(h, n, st); }
 int hb_check_range(hb_handle *h, long long n) { return check_range(h, n); }
 
-int hb_forward_step_into(hb_handle *h, long long step, const double *in, double *out, double *terms, cudaStream_t st) {
+int hb_forward_step_into(hb_handle *h, long long t0, int k, const double *in, double *out, double *terms,
+                         cudaStream_t st) {
     hb::DevMesh<hb::F64Exact> m = h->m64;
-    const int par = (int)(step & 1);
+    const int par = (int)((t0 + k) & 1);
     m.S[par] = const_cast<double *>(in);
     m.S[par ^ 1] = out;
     m.slotw = terms;
-    hb::flux_kernel<hb::F64Exact, 0, 128, 6, false><<<(m.nrecords + 127) / 128, 128, 0, st>>>(m, 0, 0);
+    hb::flux_kernel<hb::F64Exact, 0, 128, 6, false><<<(m.nrecords + 127) / 128, 128, 0, st>>>(m, k, 0);
     HB_CUDA_RET(cudaGetLastError());
     hb::update_kernel<hb::F64Exact, 0, 6, false>
-        <<<(m.C + hb::UPDATE_THREADS - 1) / hb::UPDATE_THREADS, hb::UPDATE_THREADS, 0, st>>>(m, 0, 0);
+        <<<(m.C + hb::UPDATE_THREADS - 1) / hb::UPDATE_THREADS, hb::UPDATE_THREADS, 0, st>>>(m, k, 0);
     HB_CUDA_RET(cudaGetLastError());
     return HB_OK;
 }
