@@ -489,9 +489,12 @@ __device__ __forceinline__ void gather4(const AdjMesh &a, const double *dir, con
 // the seed a.lam instead), with the loss term of row `obs_row` when step t + 1
 // ends on an observation.  Lane 0 reverses the cell update and shares the
 // adjoints of the slot sums; lane j then reverses slot j.
-__global__ void __launch_bounds__(128) adj_step_kernel(DevMesh<A> m, AdjMesh a, AdjStepBufs b,
-                                                       const double *__restrict__ x, const double *__restrict__ terms,
-                                                       StepParams p, int first, int obs_row) {
+__global__ void __launch_bounds__(128, 5) adj_step_kernel(DevMesh<A> m, AdjMesh a, AdjStepBufs b,
+                                                          const double *__restrict__ x, const double *__restrict__ terms,
+                                                          StepParams p, int first, int obs_row) {
+    // launched with programmatic dependent launch: wait for the previous kernel's results
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = (gid >> 2) < m.C;
     const int c = valid ? gid >> 2 : m.C - 1, j = gid & 3;
@@ -972,6 +975,15 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
     const int cb = (C + 255) / 256;
     hb::adj::adj_seed_kernel<<<cb, 256, 0, st>>>(C, am, a->T % a->obs_every == 0 ? a->T / a->obs_every - 1 : -1);
     HB_CUDA_RET(cudaGetLastError());
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)((4 * C + 127) / 128));
+    cfg.blockDim = dim3(128);
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     const int nseg = (a->T + a->k - 1) / a->k;
     for (int sgi = nseg - 1; sgi >= 0; sgi--) {
         const int t0 = sgi * a->k, t1 = std::min(t0 + a->k, a->T), len = t1 - t0;
@@ -989,9 +1001,9 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
             const hb::adj::AdjStepBufs bufs{a->d_dir[w ^ 1], a->d_so[w ^ 1], a->d_sn[w ^ 1],
                                             a->d_dir[w], a->d_so[w], a->d_sn[w]};
             const int row = (t + 1 < a->T && (t + 1) % a->obs_every == 0) ? (t + 1) / a->obs_every - 1 : -1;
-            hb::adj::adj_step_kernel<<<(4 * C + 127) / 128, 128, 0, st>>>(
-                h->m64, am, bufs, a->d_seg + (size_t)i * S4, a->d_terms + (size_t)i * 16 * C, p, t == a->T - 1, row);
-            HB_CUDA_RET(cudaGetLastError());
+            const double *xs = a->d_seg + (size_t)i * S4, *ts = a->d_terms + (size_t)i * 16 * C;
+            HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::adj::adj_step_kernel, h->m64, am, bufs, xs, ts, p,
+                                           (int)(t == a->T - 1), row));
         }
     }
     // the adjoint of x_0 (step 0 wrote copy 0)

@@ -699,11 +699,20 @@ int hb_forward_step_into(hb_handle *h, long long t0, int k, const double *in, do
     m.S[par] = const_cast<double *>(in);
     m.S[par ^ 1] = out;
     m.slotw = terms;
-    hb::flux_kernel<hb::F64Exact, 0, 128, 6, false><<<(m.nrecords + 127) / 128, 128, 0, st>>>(m, k, 0);
-    HB_CUDA_RET(cudaGetLastError());
-    hb::update_kernel<hb::F64Exact, 0, 6, false>
-        <<<(m.C + hb::UPDATE_THREADS - 1) / hb::UPDATE_THREADS, hb::UPDATE_THREADS, 0, st>>>(m, k, 0);
-    HB_CUDA_RET(cudaGetLastError());
+    // programmatic dependent launch, as in the step sequence (launch_steps_t)
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3((unsigned)((m.nrecords + 127) / 128));
+    cfg.blockDim = dim3(128);
+    HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::flux_kernel<hb::F64Exact, 0, 128, 6, false>, m, k, 0));
+    cfg.gridDim = dim3((unsigned)((m.C + hb::UPDATE_THREADS - 1) / hb::UPDATE_THREADS));
+    cfg.blockDim = dim3(hb::UPDATE_THREADS);
+    HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::update_kernel<hb::F64Exact, 0, 6, false>, m, k, 0));
     return HB_OK;
 }
 
