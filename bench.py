@@ -17,7 +17,9 @@ measurement, for profiling one of them):
               1000 steps each, with the split form's depth error;
   adjoint     gradient of the gauge loss on the 24,020-cell channel over
               1000 steps for checkpoint intervals 10, 50, 100: its time over
-              the plain forward's.
+              the plain forward's;
+  dambreak    2,000,000-cell dam break on a fractal bed, 2000 steps: split
+              precision against fp64 every 100 steps, and both speeds.
 
 Multi-GPU: one process per GPU (torchrun); each rank runs its own replica of
 the scenario (the path has no exchange step between independent meshes), the
@@ -367,6 +369,80 @@ def split_leg(deck, local, steps=900):
             "tile_cells": 512, "tile_config": best, "error_vs_fp64": dict(e, after_steps=steps)}
 
 
+
+def dambreak_leg(local, steps=2000, every=100, ncells=2_000_000):
+    """The wetting/drying configuration: split precision (tile layout) and
+    fp64 (edge layout) stepped side by side, depths compared every `every`
+    steps; the fp64 run is checked against the CPU oracle over its first 10
+    steps."""
+    import numpy as np
+    import torch
+    import hydrob200 as hb
+    from hydrob200 import deck as D
+    from hydrob200.accuracy import depth_error
+    root = os.path.join(tempfile.gettempdir(), f"hb_dambreak_{ncells}_{steps}")
+    if not os.path.exists(os.path.join(root, "BINFOR", "TIME.DAT")):
+        tmp = root + f".tmp{os.getpid()}"
+        D.write_deck(D.dam_break_deck(ncells=ncells, steps=steps), tmp)
+        shutil.rmtree(root, ignore_errors=True)
+        os.replace(tmp, root)
+    deck = hb.Deck(root)
+    C = deck.cells
+    area = deck.array("area")
+    hm2 = deck.mesh.hm2
+    out = {"cells": C, "steps": steps, "compare_every": every, "domain": "20 km x 20 km, walls",
+           "bed": "fractal, spectral slope -2, 5 m relief", "start": "level 5 m for x < 10 km, dry bed elsewhere",
+           "manning_n": 0.03, "dt_s": deck.mesh.dt}
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import OracleDeck
+    a = hb.Solver(deck, device=local)
+    o = OracleDeck(root)
+    a.step(10)
+    o.run(10)
+    a.sync()
+    g, od = a.get_state(), o.dump()
+    out["fp64_vs_cpu_oracle_10_steps"] = {k: float(np.max(np.abs(g[k] - od[k])) / max(float(np.max(np.abs(od[k]))), 1e-300))
+                                          for k in ("H", "U", "V")}
+    del o
+    a.close()
+    runs = {"fp64": hb.Solver(deck, device=local),
+            "split": hb.Solver(deck, precision="split", layout="tile", tile_cells=512, device=local),
+            "fp32": hb.Solver(deck, precision="fp32", layout="tile", tile_cells=512, device=local)}
+    st = torch.cuda.current_stream()
+    for h in runs.values():
+        h.capture_graph(every, st)
+    times = {k: 0.0 for k in runs}
+    rows = {"split": [], "fp32": []}
+    for k in range(steps // every):
+        for name, h in runs.items():
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            h.graph_launch(st)
+            e1.record(st)
+            h.sync(st)
+            times[name] += e0.elapsed_time(e1)
+        h64 = runs["fp64"].get_state()["H"]
+        wet64 = h64 > hm2
+        for name in ("split", "fp32"):
+            hs = runs[name].get_state()["H"]
+            e = depth_error(hs, h64, hm2, area)
+            rows[name].append({"step": (k + 1) * every, "rel_max_wet": e["rel_max"], "normwise": e["normwise"],
+                               "mass_rel": e["mass_rel"], "wet_cells": int(wet64.sum()),
+                               "wet_dry_mismatch": int(np.sum(wet64 != (hs > hm2))),
+                               "rel_max_deeper_0.1m": float(np.max((np.abs(hs - h64) / h64)[h64 > 0.1]))})
+    out["error_vs_fp64"] = rows["split"]
+    out["fp32_error_vs_fp64"] = rows["fp32"]
+    n = every * (steps // every)
+    for name in runs:
+        out[f"{name}_us_per_step"] = times[name] * 1e3 / n
+    out["split_vs_fp64"] = times["fp64"] / times["split"]
+    out["value_split"] = C / (out["split_us_per_step"] * 1e-6)
+    out["unit"] = METRIC
+    for h in runs.values():
+        h.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -377,10 +453,11 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--extras", default="all", choices=["all", "none", "ensemble", "adjoint", "split"])
+    ap.add_argument("--extras", default="all", choices=["all", "none", "ensemble", "adjoint", "split", "dambreak"])
     ap.add_argument("--only-extras", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=1000)
     ap.add_argument("--ensemble-steps", type=int, default=1000)
+    ap.add_argument("--dambreak-cells", type=int, default=2_000_000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -415,7 +492,8 @@ def main():
 
     if args.only_extras:   # one or more of the additions alone (profiling); not a bench line
         legs = {"split": lambda: split_leg(deck, local), "ensemble": lambda: ensemble_leg(local, args.ensemble_steps),
-                "adjoint": lambda: adjoint_leg(local, args.adjoint_steps)}
+                "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
+                "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells)}
         out = {k: fn() for k, fn in legs.items() if args.extras in ("all", k)}
         print(json.dumps(out), flush=True)
         return 0
@@ -518,7 +596,8 @@ def main():
     extras = {}
     if rank == 0 and world == 1 and args.extras != "none":
         legs = {"split": lambda: split_leg(deck, local), "ensemble": lambda: ensemble_leg(local, args.ensemble_steps),
-                "adjoint": lambda: adjoint_leg(local, args.adjoint_steps)}
+                "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
+                "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells)}
         for name, fn in legs.items():
             if args.extras in ("all", name):
                 try:

@@ -686,3 +686,51 @@ def adjoint_case(seed: int = 20240603, steps: int = 1000, ngauges: int = 50, obs
     rng = np.random.default_rng(seed + 29)
     gauges = np.sort(rng.choice(d.cells, ngauges, replace=False))
     return d, n_true, gauges
+
+
+def fractal_surface(xy: np.ndarray, lx: float, ly: float, relief: float, seed: int, slope: float = -2.0,
+                    n: int = 512) -> np.ndarray:
+    """A seeded random surface with power spectrum ~ |k|^slope (Fourier
+    synthesis on an n x n periodic grid over the domain), scaled to span
+    [0, relief] and interpolated bilinearly at the points xy."""
+    from scipy import ndimage
+    rng = np.random.default_rng(seed)
+    kx = np.fft.fftfreq(n)[:, None]
+    ky = np.fft.fftfreq(n)[None, :]
+    k = np.hypot(kx, ky)
+    k[0, 0] = np.inf
+    amp = k ** (slope / 2.0)
+    spec = amp * np.exp(2j * np.pi * rng.uniform(size=(n, n)))
+    z = np.real(np.fft.ifft2(spec))
+    z = (z - z.min()) / (z.max() - z.min()) * relief
+    coords = np.stack([xy[:, 0] / lx * (n - 1), xy[:, 1] / ly * (n - 1)])
+    return ndimage.map_coordinates(z, coords, order=1)
+
+
+def dam_break_deck(ncells: int = 2_000_000, length: float = 20_000.0, seed: int = 20240605, *,
+                   relief: float = 5.0, level: float = 5.0, dam_x: float = 10_000.0, n_manning: float = 0.03,
+                   dt: float = 0.5, steps: int = 2000, mdt: int = 60, hm1: float = 0.001,
+                   hm2: float = 0.01) -> Deck:
+    """The wetting/drying configuration: ``ncells`` Delaunay triangles on a
+    ``length`` x ``length`` square closed by walls (KLAS 4), bed = a seeded
+    fractal surface of spectral slope -2 spanning ``relief`` m, water level
+    ``level`` m for x < ``dam_x`` and a dry bed elsewhere (the reference's
+    preprocessing then sets H = HM1 where the level is at or below the bed,
+    mesh.cpp:350-361), Manning n = 0.03.  No boundary tables are read; NDAYS
+    covers ``steps`` steps."""
+    xy, tris, (hx, hy) = delaunay_channel(ncells, length, length, seed)
+    nodes4 = np.concatenate([tris, -np.ones((tris.shape[0], 1), dtype=np.int64)], axis=1)
+    nv3 = np.ones(tris.shape[0], dtype=bool)
+    nap, nac = _assemble("DAM", xy, nodes4, nv3)
+    cen = xy[tris].mean(axis=1)
+    zbc = fractal_surface(cen, length, length, relief, seed + 7)
+    z0 = np.where(cen[:, 0] < dam_x, level, zbc - 1.0)
+    klas = np.zeros_like(nac)
+    bc, bs = _boundary_slots(nac, nap)
+    klas[bc, bs] = KLAS_WALL
+    spd = int(mdt / dt)
+    ndays = int(math.ceil(steps / (spd - 1))) + 1
+    return Deck(name=f"DAM_{ncells}", xy=xy, nap=nap, nac=nac, klas=klas, zbc=zbc, z0=z0,
+                u0=np.zeros(nac.shape[0]), v0=np.zeros(nac.shape[0]), manning=np.full(nac.shape[0], n_manning),
+                mdt=mdt, ndays=ndays, dt=dt, hm1=hm1, hm2=hm2,
+                meta=dict(seed=seed, ncells=ncells, length=length, hx=hx, hy=hy, relief=relief, steps=steps))
