@@ -265,28 +265,45 @@ def _time_graph(h, steps, graph, torch):
     return e0.elapsed_time(e1) * 1e3 / (graph * (steps // graph))
 
 
-def ensemble_leg(local, steps=1000, graph=100):
+def ensemble_leg(local, steps=1000, graph=100, rank=0, world=1):
+    """64 channel scenarios, each rank stepping its longest-processing-time
+    share as one batch (no data-path exchange); time = max over ranks."""
     import multiprocessing as mp
     import numpy as np
     import torch
     import hydrob200 as hb
     from hydrob200 import deck as D
     from hydrob200.accuracy import depth_error
+    from hydrob200.shard import lpt_shards
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     specs = D.ensemble_specs(steps=steps)
-    with mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1)) as pool:
-        roots = pool.map(_ensemble_deck_dir, specs)
+    sizes = [sp["ncells"] for sp in specs]
+    mine = lpt_shards(sizes, world)[rank]
+    with mp.get_context("spawn").Pool(max(1, min(32, (os.cpu_count() or 1) // world))) as pool:
+        roots = pool.map(_ensemble_deck_dir, [specs[i] for i in mine])
     decks = [hb.Deck(r) for r in roots]
-    cells = sum(d.cells for d in decks)
-    out = {"scenarios": len(decks), "cells": cells, "steps": steps, "dt_s": 0.5,
-           "cells_range": [min(d.cells for d in decks), max(d.cells for d in decks)],
+    cells = sum(sizes)
+    out = {"scenarios": len(specs), "cells": cells, "steps": steps, "dt_s": 0.5,
+           "cells_range": [min(sizes), max(sizes)],
            "l2": "not flushed: the working set (> 300 MB) exceeds L2",
-           "launch": "one launch (tile layout) or launch pair (edge layout) per step for all scenarios, "
+           "launch": "one launch (tile layout) or launch pair (edge layout) per step for all scenarios of a GPU, "
                      f"{graph}-step CUDA graphs"}
+    if world > 1:
+        out["sharding"] = {"gpus": world, "rule": "longest processing time first, by cells",
+                           "cells_per_gpu": [sum(sizes[i] for i in sh) for sh in lpt_shards(sizes, world)]}
     H = {}
     for name, prec, layout, tc in (("fp64", "fp64", "edge", 0), ("split", "split", "tile", 512)):
         b = hb.Batch(decks, precision=prec, layout=layout, tile_cells=tc, device=local)
         best, ms = b.autotune(steps=10)
-        us = _time_graph(b, steps, graph, torch)
+        us = max_over_ranks(_time_graph(b, steps, graph, torch))
         out[name] = {"us_per_step": us, "value": cells / (us * 1e-6), "unit": METRIC, "layout": layout,
                      "tile_cells": tc or None, "tile_config": best,
                      "autotune_us": {str(k): round(v * 1e3, 1) for k, v in ms.items()}}
@@ -299,8 +316,9 @@ def ensemble_leg(local, steps=1000, graph=100):
         deep = H["fp64"][i] > 0.1
         if deep.any():
             wet_deep = max(wet_deep, float(np.max(np.abs(H["split"][i][deep] - H["fp64"][i][deep]) / H["fp64"][i][deep])))
-    out["split"]["error_vs_fp64"] = {"after_steps": steps, "rel_max_wet": worst, "rel_max_deeper_0.1m": wet_deep,
-                                     "normwise": normwise, "mass_rel_max": mass,
+    out["split"]["error_vs_fp64"] = {"after_steps": steps, "rel_max_wet": max_over_ranks(worst),
+                                     "rel_max_deeper_0.1m": max_over_ranks(wet_deep),
+                                     "normwise": max_over_ranks(normwise), "mass_rel_max": max_over_ranks(mass),
                                      "wet": "H_fp64 > HM2 = 0.01 m"}
     out["split_vs_fp64"] = out["fp64"]["us_per_step"] / out["split"]["us_per_step"]
     return out
@@ -491,11 +509,17 @@ def main():
     b_alg = alg_bytes_per_cell_step(C, edges, w)
 
     if args.only_extras:   # one or more of the additions alone (profiling); not a bench line
-        legs = {"split": lambda: split_leg(deck, local), "ensemble": lambda: ensemble_leg(local, args.ensemble_steps),
+        legs = {"split": lambda: split_leg(deck, local),
+                "ensemble": lambda: ensemble_leg(local, args.ensemble_steps, rank=rank, world=world),
                 "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
                 "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells)}
+        if world > 1 and args.extras != "ensemble":
+            raise SystemExit("--only-extras on several GPUs runs the ensemble only (--extras ensemble)")
         out = {k: fn() for k, fn in legs.items() if args.extras in ("all", k)}
-        print(json.dumps(out), flush=True)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
         return 0
 
     solver = hb.Solver(deck, precision=args.precision, device=local)
@@ -594,7 +618,7 @@ def main():
             cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "reference", "sample": f"failed: {ex}"[:200]}
 
     extras = {}
-    if rank == 0 and world == 1 and args.extras != "none":
+    if world == 1 and rank == 0 and args.extras != "none":
         legs = {"split": lambda: split_leg(deck, local), "ensemble": lambda: ensemble_leg(local, args.ensemble_steps),
                 "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
                 "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells)}
@@ -604,6 +628,11 @@ def main():
                     extras[name if name != "split" else "split_207k"] = fn()
                 except Exception as ex:   # the bench line still prints
                     extras[name] = {"error": f"{type(ex).__name__}: {ex}"[:300]}
+    elif world > 1 and args.extras in ("all", "ensemble"):
+        # the ensemble shards over the GPUs; every rank takes part (same collectives on every rank)
+        ens = ensemble_leg(local, args.ensemble_steps, rank=rank, world=world)
+        if rank == 0:
+            extras["ensemble"] = ens
 
     if rank == 0:
         line = {
