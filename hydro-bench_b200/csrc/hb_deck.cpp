@@ -19,7 +19,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <fstream>
+#include <iomanip>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -39,6 +41,10 @@ struct hb_deck {
     std::vector<int32_t> nhq1;                                                // [C]
     std::vector<double> zw, qw;                                               // [C*NHQ]
     std::vector<double> qt, dqt, zt, dzt;                                     // [NDAYS*C]
+    // for the OUTPUT writers
+    std::vector<double> xp, yp;                                               // [NOD] node coordinates - (XIMIN, YIMIN)
+    double ximin = 0, yimin = 0;
+    std::vector<int32_t> nap;                                                 // [4C] node ids as read
 };
 
 namespace {
@@ -237,6 +243,8 @@ extern "C" int hb_deck_load(const char *root_c, hb_deck **out) {
     double ximin = xp[0], yimin = yp[0];
     for (int i = 1; i < d->nod; i++) { ximin = std::min(ximin, xp[i]); yimin = std::min(yimin, yp[i]); }
     for (int i = 0; i < d->nod; i++) { xp[i] -= ximin; yp[i] -= yimin; }
+    d->ximin = ximin;
+    d->yimin = yimin;
     d->zb1.assign(C, 0.0); d->area.assign(C, 0.0);
     d->side.assign(S, 0.0); d->sinf.assign(S, 0.0); d->cosf.assign(S, 0.0);
     d->slcos.assign(S, 0.0); d->slsin.assign(S, 0.0);
@@ -374,6 +382,9 @@ extern "C" int hb_deck_load(const char *root_c, hb_deck **out) {
         const int pos = (int)mbw[i] - 1;
         if (pos >= 0 && pos < C) d->bfeat[pos] = topw[i];
     }
+    d->xp = std::move(xp);
+    d->yp = std::move(yp);
+    d->nap.assign(nap.begin(), nap.end());
     *out = d;
     return HB_OK;
 }
@@ -404,7 +415,179 @@ extern "C" int hb_deck_state(const hb_deck *d, const double **H, const double **
     return HB_OK;
 }
 
+extern "C" int hb_deck_ntoutput(const hb_deck *d, int32_t *ntoutput) {
+    if (!d || !ntoutput) return hb::set_error(HB_E_INVALID, "hb_deck_ntoutput: null argument");
+    *ntoutput = d->ntoutput;
+    return HB_OK;
+}
+
 extern "C" int hb_deck_free(hb_deck *d) {
     delete d;
     return HB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// OUTPUT writers: the reference's text result files (mesh.cpp:535-839)
+// ---------------------------------------------------------------------------
+struct hb_output {
+    const hb_deck *d = nullptr;
+    std::ofstream side, zuv, h2u2v2, tec, timelog;
+    bool sides_written = false;
+};
+
+namespace {
+
+// Flow direction in radians from the velocity components, quadrant by
+// quadrant with pi taken as 3.1416; components below 1e-9 count as zero
+// (mesh.cpp:841-875).
+double flow_angle(double x, double y) {
+    const double pi = 3.1416;
+    if (std::fabs(x) < 1e-9) x = 0.0;
+    if (std::fabs(y) < 1e-9) y = 0.0;
+    if (x * y != 0.0) {
+        const double w = std::atan2(std::fabs(y), std::fabs(x));
+        if (x * y > 0.0) return x > 0.0 ? w : pi + w;
+        return y > 0.0 ? pi - w : 2 * pi - w;
+    }
+    double f = 0.0;
+    if (x == 0.0 && y >= 0.0) f = pi / 2;
+    if (x == 0.0 && y < 0.0) f = 3 * pi / 2;
+    if (y == 0.0 && x >= 0.0) f = 0.0;
+    if (y == 0.0 && x < 0.0) f = pi;
+    return f;
+}
+
+// the frame header of H2U2V2.OUT and ZUV.OUT
+void frame_header(std::ostream &os, int jt2, int kt, double dt) {
+    os << " " << std::endl << " " << std::endl;
+    os << std::setw(1) << " " << std::setw(3) << "JT=" << std::setw(5) << jt2 << std::setw(2) << " " << "KT="
+       << std::setw(5) << kt - 1 << std::setw(2) << " " << "DT=" << std::setw(3) << dt << std::setw(1) << " "
+       << "SEC" << std::setw(2) << " " << "T=" << std::setw(2) << 0 << std::setw(1) << "H" << std::setw(2) << " "
+       << "NSF=" << std::setw(2) << 0 << "/" << 0 << std::setw(2) << " " << "WEC=" << std::fixed
+       << std::setprecision(2) << 0 << "/" << std::setw(2) << " " << "CQL=" << std::fixed << std::setprecision(2) << 0
+       << std::setw(2) << " " << "INE=" << std::setw(1) << 0 << std::endl;
+}
+
+// one labelled block of per-cell values: 10 per line, an extra break every 100
+template <class F>
+void value_block(std::ostream &os, const char *label, int n, F value) {
+    os << std::setw(5) << " " << std::endl << std::setw(5) << " " << std::setw(3) << label;
+    for (int i = 0; i < n; i++) {
+        if (i % 10 == 0) os << std::endl << std::setw(5) << " ";
+        if (i != 0 && i % 100 == 0) os << std::endl << std::setw(5) << " ";
+        os << std::setw(10) << std::fixed << std::setprecision(4) << value(i);
+    }
+}
+
+// one block of XY-TEC.DAT: 10 values per line
+template <class F>
+void tec_block(std::ostream &os, int n, bool break_first, F value) {
+    for (int i = 0; i < n; i++) {
+        if (i % 10 == 0 && (i != 0 || break_first)) os << std::endl;
+        os << std::fixed << std::setprecision(4) << value(i) << " ";
+    }
+}
+
+}  // namespace
+
+extern "C" int hb_output_open(const hb_deck *d, const char *dir, hb_output **out) {
+    if (!d || !dir || !out) return hb::set_error(HB_E_INVALID, "hb_output_open: null argument");
+    *out = nullptr;
+    const std::string base = std::string(dir) + "/";
+    auto o = new hb_output();
+    o->d = d;
+    o->side.open(base + "SIDE.OUT", std::ios::out | std::ofstream::trunc);
+    o->zuv.open(base + "ZUV.OUT", std::ios::out | std::ofstream::trunc);
+    o->h2u2v2.open(base + "H2U2V2.OUT", std::ios::out | std::ofstream::trunc);
+    o->tec.open(base + "XY-TEC.DAT", std::ios::out | std::ofstream::trunc);
+    o->timelog.open(base + "TIMELOG.OUT", std::ios::out | std::ofstream::trunc);
+    if (!o->side.is_open() || !o->zuv.is_open() || !o->h2u2v2.is_open() || !o->tec.is_open() || !o->timelog.is_open()) {
+        delete o;
+        return hb::set_error(HB_E_IO, "hb_output_open: cannot create the output files in %s", dir);
+    }
+    *out = o;
+    return HB_OK;
+}
+
+extern "C" int hb_output_frame(hb_output *o, int32_t jt, int32_t kt, const double *H, const double *U,
+                               const double *V, const double *Z) {
+    if (!o || !H || !U || !V || !Z) return hb::set_error(HB_E_INVALID, "hb_output_frame: null argument");
+    const hb_deck *d = o->d;
+    const int C = d->cells;
+    const double HM1 = d->hm1;
+    if (jt == 0 && kt == 1 && !o->sides_written) {   // the geometry, with the first frame
+        o->sides_written = true;
+        const std::vector<double> *per_slot[3] = {&d->cosf, &d->sinf, &d->side};
+        const char *names[3] = {"COSF", "SINF", "SIDE"};
+        for (int a = 0; a < 3; a++) {
+            o->side << names[a] << std::endl;
+            for (int i = 0; i < C; i++) {
+                o->side << i + 1 << "    ";
+                for (int k = 0; k < 4; k++) o->side << (*per_slot[a])[4 * (size_t)i + k] << "     ";
+                o->side << std::endl;
+            }
+        }
+        o->side << "AREA" << std::endl;
+        for (int i = 0; i < C; i++) o->side << i + 1 << "    " << d->area[i] << std::endl;
+    }
+    const int jt2 = jt + (kt != 1 ? 1 : 0);
+    auto snap = [](double v) { return std::fabs(v) < 1e-9 ? 0.0 : v; };
+    auto h2 = [&](int i) { return snap(H[i] <= HM1 ? 0.0 : H[i]); };
+    auto u2 = [&](int i) { return snap(H[i] <= HM1 ? 0.0 : U[i]); };
+    auto v2 = [&](int i) { return snap(H[i] <= HM1 ? 0.0 : V[i]); };
+    auto z2 = [&](int i) { return snap(H[i] <= HM1 ? d->zbc[i] : Z[i]); };
+    auto w2 = [&](int i) {   // single precision, as the reference prints it
+        float w = 0;
+        if (H[i] > HM1) w = std::sqrt(U[i] * U[i] + V[i] * V[i]);
+        if (std::fabs(w) < 1e-9f) w = 0;
+        return w;
+    };
+    auto fi = [&](int i) { return H[i] > HM1 ? flow_angle(U[i], V[i]) * (double)57.298 : 0.0; };
+
+    frame_header(o->h2u2v2, jt2, kt, d->dt);
+    frame_header(o->zuv, jt2, kt, d->dt);
+    value_block(o->h2u2v2, "H2=", C, h2);
+    o->h2u2v2 << std::endl;
+    value_block(o->h2u2v2, "U2=", C, u2);
+    o->h2u2v2 << std::endl;
+    value_block(o->h2u2v2, "V2=", C, v2);
+    o->h2u2v2 << " " << std::endl;
+    value_block(o->zuv, "Z2=", C, z2);
+    o->zuv << std::endl;
+    value_block(o->zuv, "W2=", C, w2);
+    o->zuv << std::endl;
+    value_block(o->zuv, "FI=", C, fi);
+    o->zuv << " " << std::endl;
+
+    o->timelog << std::fixed << std::setprecision(4) << (double)jt2 / d->ndays << std::endl;
+
+    std::ostream &t = o->tec;
+    t << " VARIABLES = \"X\", \"Y\", \"H2\", \"Z2\",\"U2\",\"V2\",\"W2\"" << std::endl;
+    t << "ZONE N=" << d->nod << ", E=" << C << ", DATAPACKING=BLOCK, ZONETYPE=FEQUADRILATERAL" << std::endl;
+    t << "VARLOCATION=([3-7]=CELLCENTERED)" << std::endl;
+    tec_block(t, d->nod, false, [&](int i) { return d->xp[i] + d->ximin; });
+    t << std::endl;
+    tec_block(t, d->nod, false, [&](int i) { return d->yp[i] + d->yimin; });
+    t << std::endl;
+    tec_block(t, C, true, [&](int i) { return snap(H[i] <= HM1 ? 0.0 : H[i]); });
+    tec_block(t, C, false, z2);
+    t << std::endl;
+    tec_block(t, C, false, u2);
+    t << std::endl;
+    tec_block(t, C, false, v2);
+    t << std::endl;
+    tec_block(t, C, false, w2);
+    t << std::endl;
+    for (int i = 0; i < C; i++) {
+        for (int k = 0; k < 4; k++) t << d->nap[4 * (size_t)i + k] << " ";
+        t << std::endl;
+    }
+    const bool ok = o->side.good() && o->zuv.good() && o->h2u2v2.good() && o->tec.good() && o->timelog.good();
+    return ok ? HB_OK : hb::set_error(HB_E_IO, "hb_output_frame: write failed");
+}
+
+extern "C" int hb_output_close(hb_output *o) {
+    delete o;
+    return HB_OK;
+}
+

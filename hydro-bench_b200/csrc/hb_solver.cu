@@ -1139,3 +1139,42 @@ extern "C" int hb_autotune(hb_handle *h, int32_t steps, void *stream, float *ms_
     if (best) *best = best_c + 1;
     return HB_OK;
 }
+
+// The reference driver's --dump file (cuda_native_impl/benchmark.cu:141-162):
+// int32 CELL; H, U, V, Z [CELL]; SLCOS, SLSIN, SIDE [4*CELL]; FLUX0..3
+// [4*CELL]; every value of the build's Real type (double for HB_FP64 and
+// HB_SPLIT, float for HB_FP32), reference order.  The geometry comes from the
+// caller's mesh description (the arrays the reference reads back from its
+// host mesh); the state and fluxes from scenario s of the handle.
+extern "C" int hb_write_dump(hb_handle *h, int32_t s, const hb_mesh_desc *md, const char *path) {
+    TRY(check_scenario(h, s));
+    if (!md || !path || !md->slcos || !md->slsin || !md->side)
+        return hb::set_error(HB_E_INVALID, "hb_write_dump: null argument");
+    const int C = h->scn[s].cells;
+    if (md->cells != C) return hb::set_error(HB_E_INVALID, "hb_write_dump: mesh has %d cells, scenario %d", md->cells, C);
+    const size_t S = 4 * (size_t)C;
+    std::vector<double> st(5 * (size_t)C), fl(4 * S);
+    TRY(hb_get_state_at(h, s, st.data(), st.data() + C, st.data() + 2 * (size_t)C, st.data() + 3 * (size_t)C, nullptr));
+    TRY(hb_get_flux_at(h, s, fl.data(), fl.data() + S, fl.data() + 2 * S, fl.data() + 3 * S));
+    FILE *f = fopen(path, "wb");
+    if (!f) return hb::set_error(HB_E_IO, "hb_write_dump: cannot open %s", path);
+    const bool f32 = h->opt.precision == HB_FP32;
+    bool ok = fwrite(&C, sizeof(int32_t), 1, f) == 1;
+    auto put = [&](const double *a, size_t n) {
+        if (!ok) return;
+        if (f32) {
+            std::vector<float> b(a, a + n);
+            ok = fwrite(b.data(), sizeof(float), n, f) == n;
+        } else {
+            ok = fwrite(a, sizeof(double), n, f) == n;
+        }
+    };
+    for (int k = 0; k < 4; k++) put(st.data() + (size_t)k * C, C);
+    put(md->slcos, S);
+    put(md->slsin, S);
+    put(md->side, S);
+    for (int k = 0; k < 4; k++) put(fl.data() + (size_t)k * S, S);
+    if (fclose(f) != 0) ok = false;
+    return ok ? HB_OK : hb::set_error(HB_E_IO, "hb_write_dump: write to %s failed", path);
+}
+

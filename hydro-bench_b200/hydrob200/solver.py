@@ -167,6 +167,11 @@ class Solver:
     def sync(self, stream=None) -> None:
         check(lib().hb_sync(self._h, _stream_handle(stream)))
 
+    def write_dump(self, path: str, scenario: int = 0, deck: Deck = None) -> None:
+        """hb_write_dump: the reference driver's --dump file (benchmark.cu:141-162)."""
+        d = deck if deck is not None else (self.deck if hasattr(self, "deck") else self.decks[scenario])
+        check(lib().hb_write_dump(self._h, scenario, C.byref(d.mesh), path.encode()))
+
     def device_errors(self) -> int:
         v = C.c_uint32()
         check(lib().hb_device_errors(self._h, C.byref(v)))

@@ -167,6 +167,11 @@ int hb_graph_launch(hb_handle *h, void *stream);
 int hb_device_state(hb_handle *h, void **H, void **U, void **V, void **Z, void **W, int32_t *stride);
 /* Renumbering: perm[new] = old (cell ids, 0-based). */
 int hb_get_permutation(hb_handle *h, int32_t *perm);
+/* Write scenario s's state and last fluxes as the reference driver's --dump
+ * file (cuda_native_impl/benchmark.cu:141-162): int32 CELL; H, U, V, Z;
+ * SLCOS, SLSIN, SIDE (from `mesh`); FLUX0..3; values of the build's Real
+ * type (float for HB_FP32, double otherwise), reference order. */
+int hb_write_dump(hb_handle *h, int32_t s, const hb_mesh_desc *mesh, const char *path);
 /* Sticky device error word (bit set of hb_status codes seen by kernels). */
 int hb_device_errors(hb_handle *h, uint32_t *bits);
 
@@ -211,6 +216,22 @@ int hb_deck_mesh(const hb_deck *d, hb_mesh_desc *mesh);
 int hb_deck_state(const hb_deck *d, const double **H, const double **U, const double **V,
                   const double **Z, const double **W);
 int hb_deck_free(hb_deck *d);
+
+/* ---- result files in the reference's text formats (mesh.cpp:535-839) ----
+ * hb_output_open creates (truncating) SIDE.OUT, H2U2V2.OUT, ZUV.OUT,
+ * XY-TEC.DAT and TIMELOG.OUT in `dir` for the deck's mesh; hb_output_frame
+ * appends one frame of a state (reference order, fp64 [CELL]) for day jt and
+ * step kt as the reference's outputToFile(jt, kt) does (the first frame,
+ * jt = 0 and kt = 1, also writes the geometry to SIDE.OUT).  The driver loop
+ * writes the initial frame (0, 1), then one after the last step of every
+ * NTOUTPUT-th day and after the last step (benchmark.cu:105-124). */
+typedef struct hb_output hb_output;
+int hb_output_open(const hb_deck *d, const char *dir, hb_output **out);
+int hb_output_frame(hb_output *o, int32_t jt, int32_t kt, const double *H, const double *U, const double *V,
+                    const double *Z);
+int hb_output_close(hb_output *o);
+/* NTOUTPUT of the deck (BINFOR/TIME.DAT). */
+int hb_deck_ntoutput(const hb_deck *d, int32_t *ntoutput);
 
 #ifdef __cplusplus
 }
