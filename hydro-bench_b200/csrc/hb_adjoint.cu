@@ -694,8 +694,10 @@ struct hb_adjoint {
     std::vector<int32_t> gauges_dev;        // gauge cells, device order
     int32_t *d_gcell = nullptr;
     double *d_ckpt = nullptr;               // [T/k + 1][C][4]
-    double *d_seg = nullptr;                // [k + 1][C][4] states of a segment
-    double *d_terms = nullptr;              // [k][4C][4] slot terms of a segment
+    double *d_seg[2] = {nullptr, nullptr};   // [k + 1][C][4] states of a segment (two segments in flight)
+    double *d_terms[2] = {nullptr, nullptr}; // [k][4C][4] slot terms of a segment
+    cudaStream_t recompute = nullptr;        // the recomputation runs ahead of the reverse steps on its own stream
+    cudaEvent_t ev_recomputed[2] = {nullptr, nullptr}, ev_reversed[2] = {nullptr, nullptr};
     double *d_gd = nullptr;                 // [nobs][ng] gauge depths of the forward
     double *d_obs = nullptr;                // [nobs][ng]
     double *d_res = nullptr;                // [nobs][ng]
@@ -708,6 +710,11 @@ struct hb_adjoint {
     bool forward_done = false;
     ~hb_adjoint() {
         if (fwd_graph) cudaGraphExecDestroy(fwd_graph);
+        for (int q = 0; q < 2; q++) {
+            if (ev_recomputed[q]) cudaEventDestroy(ev_recomputed[q]);
+            if (ev_reversed[q]) cudaEventDestroy(ev_reversed[q]);
+        }
+        if (recompute) cudaStreamDestroy(recompute);
         for (void *p : allocs) cudaFree(p);
     }
 };
@@ -841,8 +848,15 @@ extern "C" int hb_adjoint_create(hb_handle *h, const int32_t *gauges, int32_t ng
     am.obs_every = obs_every;
     const int nck = nsteps / checkpoint_every + 1;
     if ((st = adj_alloc(a, &a->d_ckpt, (size_t)nck * 4 * C)) != HB_OK) return fail(st);
-    if ((st = adj_alloc(a, &a->d_seg, (size_t)(checkpoint_every + 1) * 4 * C)) != HB_OK) return fail(st);
-    if ((st = adj_alloc(a, &a->d_terms, (size_t)checkpoint_every * 16 * C)) != HB_OK) return fail(st);
+    for (int q = 0; q < 2; q++) {
+        if ((st = adj_alloc(a, &a->d_seg[q], (size_t)(checkpoint_every + 1) * 4 * C)) != HB_OK) return fail(st);
+        if ((st = adj_alloc(a, &a->d_terms[q], (size_t)checkpoint_every * 16 * C)) != HB_OK) return fail(st);
+        if (cudaEventCreateWithFlags(&a->ev_recomputed[q], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&a->ev_reversed[q], cudaEventDisableTiming) != cudaSuccess)
+            return fail(hb::set_error(HB_E_CUDA, "hb_adjoint_create: cudaEventCreate failed"));
+    }
+    if (cudaStreamCreateWithFlags(&a->recompute, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(hb::set_error(HB_E_CUDA, "hb_adjoint_create: cudaStreamCreate failed"));
     if ((st = adj_alloc(a, &a->d_gd, (size_t)std::max(a->nobs, 1) * ngauges)) != HB_OK) return fail(st);
     if ((st = adj_alloc(a, &a->d_obs, (size_t)std::max(a->nobs, 1) * ngauges)) != HB_OK) return fail(st);
     if ((st = adj_alloc(a, &a->d_z0, C)) != HB_OK) return fail(st);
@@ -985,15 +999,37 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const int nseg = (a->T + a->k - 1) / a->k;
-    for (int sgi = nseg - 1; sgi >= 0; sgi--) {
-        const int t0 = sgi * a->k, t1 = std::min(t0 + a->k, a->T), len = t1 - t0;
-        // recompute the segment: its states and the slot terms of its steps
-        HB_CUDA_RET(cudaMemcpyAsync(a->d_seg, a->d_ckpt + (size_t)sgi * S4, S4 * sizeof(double),
-                                    cudaMemcpyDeviceToDevice, st));
-        hb::adj::set_counter_kernel<<<1, 1, 0, st>>>(h->d_ctr, t0);
+    // Segment sgi's states and slot terms are recomputed on the recompute
+    // stream into buffer sgi & 1, one segment ahead of the reverse steps on
+    // `st`: recompute(sgi - 1) overlaps reverse(sgi).  Events order each
+    // buffer's reuse.  The reverse kernels do not read the step counter or any
+    // other array the forward kernels write besides the segment buffers.
+    cudaStream_t rs = a->recompute;
+    cudaEvent_t start_ev = nullptr;
+    HB_CUDA_RET(cudaEventCreateWithFlags(&start_ev, cudaEventDisableTiming));
+    HB_CUDA_RET(cudaEventRecord(start_ev, st));
+    HB_CUDA_RET(cudaStreamWaitEvent(rs, start_ev, 0));   // after this call's earlier work on st
+    cudaEventDestroy(start_ev);
+    bool reversed_once[2] = {false, false};
+    auto issue_recompute = [&](int sgi) -> int {
+        const int b = sgi & 1;
+        const int t0 = sgi * a->k, len = std::min(t0 + a->k, a->T) - t0;
+        if (reversed_once[b]) HB_CUDA_RET(cudaStreamWaitEvent(rs, a->ev_reversed[b], 0));
+        HB_CUDA_RET(cudaMemcpyAsync(a->d_seg[b], a->d_ckpt + (size_t)sgi * S4, S4 * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, rs));
+        hb::adj::set_counter_kernel<<<1, 1, 0, rs>>>(h->d_ctr, t0);
         for (int i = 0; i < len; i++)
-            TRY(hb_forward_step_into(h, t0, i, a->d_seg + (size_t)i * S4, a->d_seg + (size_t)(i + 1) * S4,
-                                     a->d_terms + (size_t)i * 16 * C, st));
+            TRY(hb_forward_step_into(h, t0, i, a->d_seg[b] + (size_t)i * S4, a->d_seg[b] + (size_t)(i + 1) * S4,
+                                     a->d_terms[b] + (size_t)i * 16 * C, rs));
+        HB_CUDA_RET(cudaEventRecord(a->ev_recomputed[b], rs));
+        return HB_OK;
+    };
+    TRY(issue_recompute(nseg - 1));
+    for (int sgi = nseg - 1; sgi >= 0; sgi--) {
+        const int b = sgi & 1;
+        const int t0 = sgi * a->k, len = std::min(t0 + a->k, a->T) - t0;
+        if (sgi > 0) TRY(issue_recompute(sgi - 1));
+        HB_CUDA_RET(cudaStreamWaitEvent(st, a->ev_recomputed[b], 0));
         for (int i = len - 1; i >= 0; i--) {
             const int t = t0 + i;
             const hb::StepParams p = step_params(h, t);
@@ -1001,10 +1037,12 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
             const hb::adj::AdjStepBufs bufs{a->d_dir[w ^ 1], a->d_so[w ^ 1], a->d_sn[w ^ 1],
                                             a->d_dir[w], a->d_so[w], a->d_sn[w]};
             const int row = (t + 1 < a->T && (t + 1) % a->obs_every == 0) ? (t + 1) / a->obs_every - 1 : -1;
-            const double *xs = a->d_seg + (size_t)i * S4, *ts = a->d_terms + (size_t)i * 16 * C;
+            const double *xs = a->d_seg[b] + (size_t)i * S4, *ts = a->d_terms[b] + (size_t)i * 16 * C;
             HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::adj::adj_step_kernel, h->m64, am, bufs, xs, ts, p,
                                            (int)(t == a->T - 1), row));
         }
+        HB_CUDA_RET(cudaEventRecord(a->ev_reversed[b], st));
+        reversed_once[b] = true;
     }
     // the adjoint of x_0 (step 0 wrote copy 0)
     hb::adj::adj_gather_kernel<<<(4 * C + 127) / 128, 128, 0, st>>>(C, am, a->d_dir[0], a->d_so[0], a->d_sn[0]);
