@@ -1178,3 +1178,94 @@ extern "C" int hb_write_dump(hb_handle *h, int32_t s, const hb_mesh_desc *md, co
     return ok ? HB_OK : hb::set_error(HB_E_IO, "hb_write_dump: write to %s failed", path);
 }
 
+// ---------------------------------------------------------------------------
+// checkpoint / resume
+// ---------------------------------------------------------------------------
+namespace {
+struct CheckpointHeader {
+    char magic[8];                      // "HBCKPT1"
+    int32_t precision, variant, layout, tile_cells, renumber;
+    int32_t cells, nrecords, nscen;
+    int64_t steps_done;
+    uint64_t payload;                   // bytes after the header
+};
+
+// the pieces of device memory a resumed run needs, in checkpoint order
+template <class A>
+std::vector<std::pair<void *, size_t>> checkpoint_pieces(hb_handle *h, hb::DevMesh<A> &m) {
+    using R = typename A::real;
+    const size_t C = (size_t)h->C;
+    const int par = (int)(h->steps_done & 1);
+    return {{m.S[par], 4 * C * sizeof(R)}, {m.W, C * sizeof(R)},       {m.f0, 4 * C * sizeof(R)},
+            {m.f1, 4 * C * sizeof(R)},     {m.f2, 4 * C * sizeof(R)}, {m.f3, 4 * C * sizeof(R)},
+            {m.rmeta, (size_t)m.nrecords}, {h->d_err, sizeof(uint32_t)}};
+}
+}  // namespace
+
+extern "C" int hb_checkpoint_size(hb_handle *h, size_t *bytes) {
+    if (!h || !bytes) return hb::set_error(HB_E_INVALID, "null argument");
+    size_t n = sizeof(CheckpointHeader);
+    h->with_mesh([&](auto &m) {
+        for (auto &p : checkpoint_pieces(h, m)) n += p.second;
+        return HB_OK;
+    });
+    *bytes = n;
+    return HB_OK;
+}
+
+extern "C" int hb_checkpoint_save(hb_handle *h, void *buffer, size_t bytes) {
+    size_t need = 0;
+    TRY(hb_checkpoint_size(h, &need));
+    if (!buffer || bytes < need) return hb::set_error(HB_E_INVALID, "hb_checkpoint_save: buffer of %zu bytes, need %zu", bytes, need);
+    HB_CUDA_RET(cudaDeviceSynchronize());
+    CheckpointHeader hd{};
+    memcpy(hd.magic, "HBCKPT1", 8);
+    hd.precision = h->opt.precision; hd.variant = h->opt.variant; hd.layout = h->opt.layout;
+    hd.tile_cells = h->opt.tile_cells; hd.renumber = h->opt.renumber;
+    hd.cells = h->C; hd.nscen = (int32_t)h->scn.size();
+    hd.steps_done = h->steps_done;
+    hd.payload = need - sizeof hd;
+    char *out = (char *)buffer + sizeof hd;
+    int rc = h->with_mesh([&](auto &m) -> int {
+        hd.nrecords = m.nrecords;
+        for (auto &p : checkpoint_pieces(h, m)) {
+            HB_CUDA_RET(cudaMemcpy(out, p.first, p.second, cudaMemcpyDeviceToHost));
+            out += p.second;
+        }
+        return HB_OK;
+    });
+    if (rc != HB_OK) return rc;
+    memcpy(buffer, &hd, sizeof hd);
+    return HB_OK;
+}
+
+extern "C" int hb_checkpoint_load(hb_handle *h, const void *buffer, size_t bytes) {
+    if (!h || !buffer || bytes < sizeof(CheckpointHeader)) return hb::set_error(HB_E_INVALID, "hb_checkpoint_load: bad argument");
+    CheckpointHeader hd;
+    memcpy(&hd, buffer, sizeof hd);
+    if (memcmp(hd.magic, "HBCKPT1", 8) != 0) return hb::set_error(HB_E_INVALID, "hb_checkpoint_load: not a checkpoint");
+    int nrec = 0;
+    h->with_mesh([&](auto &m) { nrec = m.nrecords; return HB_OK; });
+    if (hd.precision != h->opt.precision || hd.variant != h->opt.variant || hd.layout != h->opt.layout ||
+        hd.tile_cells != h->opt.tile_cells || hd.renumber != h->opt.renumber || hd.cells != h->C ||
+        hd.nscen != (int32_t)h->scn.size() || hd.nrecords != nrec)
+        return hb::set_error(HB_E_INVALID, "hb_checkpoint_load: the checkpoint is of another mesh or other options");
+    if (hd.steps_done < 0 || hd.steps_done > h->step_limit())
+        return hb::set_error(HB_E_INVALID, "hb_checkpoint_load: position %lld beyond the boundary tables", (long long)hd.steps_done);
+    if (bytes < sizeof hd + hd.payload) return hb::set_error(HB_E_INVALID, "hb_checkpoint_load: truncated checkpoint");
+    HB_CUDA_RET(cudaDeviceSynchronize());
+    h->steps_done = hd.steps_done;   // the state goes into buffer (steps_done & 1)
+    const char *in = (const char *)buffer + sizeof hd;
+    int rc = h->with_mesh([&](auto &m) -> int {
+        for (auto &p : checkpoint_pieces(h, m)) {
+            HB_CUDA_RET(cudaMemcpy(p.first, in, p.second, cudaMemcpyHostToDevice));
+            in += p.second;
+        }
+        return HB_OK;
+    });
+    if (rc != HB_OK) return rc;
+    long long v = hd.steps_done;
+    HB_CUDA_RET(cudaMemcpy(h->d_ctr, &v, sizeof v, cudaMemcpyHostToDevice));
+    return HB_OK;
+}
+

@@ -126,6 +126,9 @@ def lib():
         "hb_output_frame": (C.c_int, [vp, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp]),
         "hb_output_close": (C.c_int, [vp]),
         "hb_deck_ntoutput": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+        "hb_checkpoint_size": (C.c_int, [vp, C.POINTER(C.c_size_t)]),
+        "hb_checkpoint_save": (C.c_int, [vp, C.c_void_p, C.c_size_t]),
+        "hb_checkpoint_load": (C.c_int, [vp, C.c_void_p, C.c_size_t]),
         "hb_write_dump": (C.c_int, [vp, C.c_int32, C.POINTER(MeshDesc), C.c_char_p]),
         "hb_adjoint_create": (C.c_int, [vp, _ip, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(vp)]),
         "hb_adjoint_destroy": (C.c_int, [vp]),
@@ -158,6 +161,6 @@ EXPORTED = ["hb_options_default", "hb_tile_configs", "hb_launch_shapes", "hb_cre
             "hb_ref_update_cell_f32", "hb_ref_take_device_errors", "hb_ref_step_static",
             "hb_create_batch", "hb_batch_size", "hb_scenario_cells", "hb_set_state_at", "hb_get_state_at",
             "hb_get_flux_at", "hb_get_klas_at", "hb_get_permutation_at", "hb_set_tile_config", "hb_get_tile_config",
-            "hb_autotune", "hb_write_dump", "hb_output_open", "hb_output_frame", "hb_output_close",
+            "hb_autotune", "hb_checkpoint_size", "hb_checkpoint_save", "hb_checkpoint_load", "hb_write_dump", "hb_output_open", "hb_output_frame", "hb_output_close",
             "hb_deck_ntoutput", "hb_adjoint_create", "hb_adjoint_destroy", "hb_adjoint_set_parameters",
             "hb_adjoint_set_initial", "hb_adjoint_set_observations", "hb_adjoint_forward", "hb_adjoint_backward"]

@@ -167,6 +167,19 @@ class Solver:
     def sync(self, stream=None) -> None:
         check(lib().hb_sync(self._h, _stream_handle(stream)))
 
+    def checkpoint(self) -> bytes:
+        """hb_checkpoint_save: everything needed to continue this run bit for bit."""
+        n = C.c_size_t()
+        check(lib().hb_checkpoint_size(self._h, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        check(lib().hb_checkpoint_save(self._h, buf, n.value))
+        return buf.raw
+
+    def restore(self, blob: bytes) -> None:
+        """hb_checkpoint_load: continue from a checkpoint of the same mesh and options."""
+        buf = C.create_string_buffer(blob, len(blob))
+        check(lib().hb_checkpoint_load(self._h, buf, len(blob)))
+
     def write_dump(self, path: str, scenario: int = 0, deck: Deck = None) -> None:
         """hb_write_dump: the reference driver's --dump file (benchmark.cu:141-162)."""
         d = deck if deck is not None else (self.deck if hasattr(self, "deck") else self.decks[scenario])

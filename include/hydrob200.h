@@ -172,6 +172,16 @@ int hb_get_permutation(hb_handle *h, int32_t *perm);
  * SLCOS, SLSIN, SIDE (from `mesh`); FLUX0..3; values of the build's Real
  * type (float for HB_FP32, double otherwise), reference order. */
 int hb_write_dump(hb_handle *h, int32_t s, const hb_mesh_desc *mesh, const char *path);
+/* Checkpoint / resume (no reference counterpart): everything a run needs to
+ * continue bit for bit -- the current state and W, the fluxes (codes that
+ * leave fluxes unwritten keep the old ones), the per-slot boundary codes
+ * (KLAS 7 slots breach), the device error bits and the step position -- in
+ * one host buffer of hb_checkpoint_size bytes.  A checkpoint loads into a
+ * handle of the same mesh(es) and options (precision, variant, layout,
+ * tile_cells, renumbering); a captured graph stays valid. */
+int hb_checkpoint_size(hb_handle *h, size_t *bytes);
+int hb_checkpoint_save(hb_handle *h, void *buffer, size_t bytes);
+int hb_checkpoint_load(hb_handle *h, const void *buffer, size_t bytes);
 /* Sticky device error word (bit set of hb_status codes seen by kernels). */
 int hb_device_errors(hb_handle *h, uint32_t *bits);
 
