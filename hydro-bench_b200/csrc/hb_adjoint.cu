@@ -910,6 +910,7 @@ extern "C" int hb_adjoint_set_observations(hb_adjoint *a, const double *obs) {
 }
 
 extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_depths, void *stream) {
+    NvtxRange nvtx_("hb_adjoint_forward");
     if (!a) return hb::set_error(HB_E_INVALID, "null adjoint");
     hb_handle *h = a->h;
     cudaStream_t st = (cudaStream_t)stream;
@@ -977,6 +978,7 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
 }
 
 extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_zbc, void *stream) {
+    NvtxRange nvtx_("hb_adjoint_backward");
     if (!a) return hb::set_error(HB_E_INVALID, "null adjoint");
     if (!a->forward_done) return hb::set_error(HB_E_INVALID, "hb_adjoint_backward: run hb_adjoint_forward first");
     hb_handle *h = a->h;

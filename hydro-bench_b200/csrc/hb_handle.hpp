@@ -5,7 +5,15 @@
 #include <climits>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "hb_step.cuh"
+
+// An NVTX range over a host entry point (visible to Nsight tools; free otherwise).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
 
 // ---------------------------------------------------------------------------
 // handle

@@ -910,6 +910,7 @@ extern "C" int hb_get_klas(hb_handle *h, double *klas) {
 }
 
 extern "C" int hb_step(hb_handle *h, int32_t nsteps, void *stream) {
+    NvtxRange nvtx_("hb_step");
     if (!h || nsteps < 0) return hb::set_error(HB_E_INVALID, "hb_step: bad argument");
     TRY(check_range(h, nsteps));
     TRY(enqueue_steps(h, nsteps, (cudaStream_t)stream));
@@ -940,6 +941,7 @@ int step_host_t(hb_handle *h, hb::DevMesh<A> &m, double *H, double *U, double *V
 
 extern "C" int hb_step_host(hb_handle *h, double *H, double *U, double *V, double *Z, double *W, int32_t nsteps,
                             void *stream) {
+    NvtxRange nvtx_("hb_step_host");
     if (!h || !H || !U || !V || !Z || nsteps < 0) return hb::set_error(HB_E_INVALID, "hb_step_host: bad argument");
     if (h->segmented()) return hb::set_error(HB_E_INVALID, "hb_step_host: not available on a batch handle");
     TRY(check_range(h, nsteps));
@@ -993,6 +995,7 @@ extern "C" int hb_set_position(hb_handle *h, int64_t steps_done) {
 }
 
 extern "C" int hb_capture_graph(hb_handle *h, int32_t nsteps, void *stream) {
+    NvtxRange nvtx_("hb_capture_graph");
     if (!h || nsteps <= 0) return hb::set_error(HB_E_INVALID, "hb_capture_graph: bad argument");
     cudaStream_t st = (cudaStream_t)stream;
     cudaStream_t cap = st;
@@ -1013,6 +1016,7 @@ extern "C" int hb_capture_graph(hb_handle *h, int32_t nsteps, void *stream) {
 }
 
 extern "C" int hb_graph_launch(hb_handle *h, void *stream) {
+    NvtxRange nvtx_("hb_graph_launch");
     if (!h || !h->graph_exec) return hb::set_error(HB_E_INVALID, "hb_graph_launch: no graph captured");
     TRY(check_range(h, h->graph_steps));
     HB_CUDA_RET(cudaGraphLaunch(h->graph_exec, (cudaStream_t)stream));
@@ -1070,6 +1074,7 @@ extern "C" int hb_get_tile_config(hb_handle *h, int32_t *tile_config) {
 // fastest shape becomes the handle's (a captured graph is dropped).
 extern "C" int hb_autotune(hb_handle *h, int32_t steps, void *stream, float *ms_per_step, int32_t capacity,
                            int32_t *best) {
+    NvtxRange nvtx_("hb_autotune");
     if (!h || steps <= 0) return hb::set_error(HB_E_INVALID, "hb_autotune: bad argument");
     TRY(check_range(h, (long long)steps + 1));
     cudaStream_t st = (cudaStream_t)stream;
