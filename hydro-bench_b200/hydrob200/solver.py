@@ -236,7 +236,8 @@ class Solver:
         return p
 
     def device_state(self):
-        """Zero-copy torch views of the device state (renumbered order): H, U, V, Z, W."""
+        """Zero-copy torch views of the device state (renumbered order): H, U, V,
+        Z, W (split precision: H, U, V, H_lo, W)."""
         import torch
         ptrs = [C.c_void_p() for _ in range(5)]
         stride = C.c_int32()
@@ -249,8 +250,14 @@ class Solver:
                 self.__cuda_array_interface__ = {"shape": (n,), "typestr": dt, "data": (ptr, False), "version": 3,
                                                  "strides": (st * item,)}
 
-        return {k: torch.as_tensor(_CAI(p.value, self.cells, stride.value if k != "W" else 1), device="cuda")
-                for k, p in zip("HUVZW", ptrs)}
+        # split precision keeps no level: its fourth interleaved entry is the depth's low part ("H_lo")
+        names = "HUVZW" if self.precision != SPLIT else ("H", "U", "V", "H_lo", "W")
+        out = {}
+        for k, p in zip(names, ptrs):
+            if k == "H_lo":
+                p = C.c_void_p(ptrs[0].value + 3 * item)
+            out[k] = torch.as_tensor(_CAI(p.value, self.cells, stride.value if k != "W" else 1), device="cuda")
+        return out
 
 
 class Batch(Solver):

@@ -128,3 +128,20 @@ def test_tile_configs_bit_identical(deck_dir):
         else:
             np.testing.assert_array_equal(h, ref, err_msg=f"tile_config {cfg}")
         s.close()
+
+
+def test_device_state_views(deck_dir):
+    """Zero-copy views of the split state: fp32 H, U, V and the depth's low part;
+    H + H_lo is the depth hb_get_state reports for wet cells."""
+    import torch
+    deck = hb.Deck(deck_dir["f1"])
+    s = hb.Solver(deck, precision="split")
+    s.step(5)
+    s.sync()
+    v = s.device_state()
+    assert set(v) == {"H", "U", "V", "H_lo", "W"}
+    assert v["H"].dtype == torch.float32
+    perm = s.permutation()
+    st = s.get_state()
+    depth = v["H"].cpu().numpy().astype(np.float64) + v["H_lo"].cpu().numpy().astype(np.float64)
+    np.testing.assert_array_equal(depth, st["H"][perm])
