@@ -18,7 +18,7 @@
 //
 // Memory: the state is kept every `checkpoint_every` = k steps; the backward
 // pass recomputes each k-step segment from its checkpoint, keeping that
-// segment's states and slot terms, then runs the segment's reverse steps, one
+// segment's states, then runs the segment's reverse steps, one
 // kernel each (adj_step_kernel, four lanes per cell):
 //   - the state adjoint after the step, gathered from the later step's
 //     direct terms, the cell's own slots' contributions and those of the
@@ -87,15 +87,21 @@ __device__ __forceinline__ OsherFwd osher_fwd(double cl, const double ql[3], con
     o.p6 = any && (k2 == 4 ? k1 <= 2 : k1 >= 3);
     o.s6 = k2 != 4 ? -1.0 : 1.0;
     o.p7 = any && k1 >= 3;
-    o.us = A::divk(fil, 3.0);
-    o.hs = A::divk(A::mul(o.us, o.us), 9.81);
+    // the dividing pieces only where the case takes them (osher() does the same)
     o.ua35 = A::mul(A::add(fil, o.fir), A::c(0.5));
     o.fil3 = A::sub(fil, o.ua35);
-    o.ha3 = A::divk(A::mul(o.fil3, o.fil3), 39.24);
     o.fir5 = A::sub(o.fir, o.ua35);
-    o.ha5 = A::divk(A::mul(o.fir5, o.fir5), 39.24);
-    o.us6 = A::divk(o.p5 ? o.fir5 : o.fir, 3.0);
-    o.hs6 = A::divk(A::mul(o.us6, o.us6), 9.81);
+    o.us = o.hs = o.ha3 = o.ha5 = o.us6 = o.hs6 = 0.0;
+    if (o.p2) {
+        o.us = A::divk(fil, 3.0);
+        o.hs = A::divk(A::mul(o.us, o.us), 9.81);
+    }
+    if (o.p3) o.ha3 = A::divk(A::mul(o.fil3, o.fil3), 39.24);
+    if (o.p5) o.ha5 = A::divk(A::mul(o.fir5, o.fir5), 39.24);
+    if (o.p6) {
+        o.us6 = A::divk(o.p5 ? o.fir5 : o.fir, 3.0);
+        o.hs6 = A::divk(A::mul(o.us6, o.us6), 9.81);
+    }
     // FLUX3 as qf_acc_if sums it: out3 += +-4.905 h * h over the active pieces in order
     double o3 = 0.0;
     auto acc = [&](bool on, double sign, double h) {
@@ -483,14 +489,23 @@ __device__ __forceinline__ void gather4(const AdjMesh &a, const double *dir, con
     }
 }
 
-// One reverse step t, four lanes per cell.  x: the state before the step;
-// terms: the forward's slot terms of the step.  The adjoint of the state after
-// the step is gathered first from step t + 1's contributions (`first`: it is
-// the seed a.lam instead), with the loss term of row `obs_row` when step t + 1
-// ends on an observation.  Lane 0 reverses the cell update and shares the
-// adjoints of the slot sums; lane j then reverses slot j.
-__global__ void __launch_bounds__(128, 5) adj_step_kernel(DevMesh<A> m, AdjMesh a, AdjStepBufs b,
-                                                          const double *__restrict__ x, const double *__restrict__ terms,
+// One reverse step t, four lanes per cell.  x: the state before the step; xn:
+// the state after it.  The adjoint of the state after the step is gathered
+// first from step t + 1's contributions (`first`: it is the seed a.lam
+// instead), with the loss term of row `obs_row` when step t + 1 ends on an
+// observation.  Lane 0 reverses the cell update and shares the adjoints of the
+// slot sums; lane j then reverses slot j.
+//
+// The update's forward values come from xn rather than from the slot sums:
+// H2 = max(H + QLUA - DTA WH, HM1) is xn's depth, so H2 > HM1 exactly when the
+// unclamped depth is; and where H2 > HM2 the velocity U2 is xn's U whenever
+// |U2| < 15, the only case in which its adjoint passes (at the clamp, xn holds
+// +-15 and the adjoint is cut).
+//
+// Seven CTAs per SM (72 registers, some spilled to L1): the kernel waits on
+// L2 gathers, and more resident warps hide them better than fewer spills do.
+__global__ void __launch_bounds__(128, 7) adj_step_kernel(DevMesh<A> m, AdjMesh a, AdjStepBufs b,
+                                                          const double *__restrict__ x, const double *__restrict__ xn,
                                                           StepParams p, int first, int obs_row) {
     // launched with programmatic dependent launch: wait for the previous kernel's results
     cudaGridDependencySynchronize();
@@ -510,19 +525,9 @@ __global__ void __launch_bounds__(128, 5) adj_step_kernel(DevMesh<A> m, AdjMesh 
     double whb = 0.0, wub = 0.0, wvb = 0.0;
     if (j == 0) {
         // ---- the update (UpdateCellKernel, functors.cu:717-784, variant H): forward values, then its reverse
-        double wh = 0.0, wu = 0.0, wv = 0.0;
-        const unsigned mask = m.cmask[c];
-        for (int q = 0; q < 4; q++) {
-            if (!(mask & (1u << q))) continue;
-            const double *t = terms + 16 * (size_t)c + 4 * q;
-            wh = A::madd(t[3], t[0], wh, M_WH);
-            wu = A::add(wu, t[1]);
-            wv = A::add(wv, t[2]);
-        }
         const double HM1 = p.hm1, HM2 = p.hm2, DT = p.dt;
         const double dta = m.dta[c], fnc = m.fnc[c];
-        const double h2raw = A::add(A::madd(-dta, wh, hv, M_H2), A::c(K::QLUA));
-        const double h2 = A::fmax(h2raw, HM1);
+        const double h2 = xn[4 * (size_t)c], u2 = xn[4 * (size_t)c + 1], v2 = xn[4 * (size_t)c + 2];
         double h2b = l[0] + l[3];   // Z2 = H2 + ZBC
         double hb = 0.0, ub = 0.0, vb = 0.0, fncb = 0.0;
         if (h2 > HM2) {
@@ -531,8 +536,6 @@ __global__ void __launch_bounds__(128, 5) adj_step_kernel(DevMesh<A> m, AdjMesh 
             const double hp = A::pow(hv, A::c(0.33333));
             const double wsf = A::div(A::mul(fnc, sq), hp);
             const double dtw = A::mul(DT, wsf);
-            const double u2 = A::div(A::madd(-dtw, uv, A::dot(hv, uv, -dta, wu, M_U2A), M_U2B), h2);
-            const double v2 = A::div(A::madd(-dtw, vv, A::dot(hv, vv, -dta, wv, M_U2A), M_U2B), h2);
             const double ih2 = 1.0 / h2, ihp = 1.0 / hp;
             const double ue = fabs(u2) < 15.0 ? l[1] : 0.0;
             const double ve = fabs(v2) < 15.0 ? l[2] : 0.0;
@@ -553,7 +556,7 @@ __global__ void __launch_bounds__(128, 5) adj_step_kernel(DevMesh<A> m, AdjMesh 
             if (fabs(uv) < K::VMIN) ub += l[1];
             if (fabs(vv) < K::VMIN) vb += l[2];
         }
-        if (h2raw > HM1) { hb += h2b; whb -= h2b * dta; }
+        if (h2 > HM1) { hb += h2b; whb -= h2b * dta; }
         if (valid) {
             double *d = b.dir_out + 4 * (size_t)c;
             d[0] = hb; d[1] = ub; d[2] = vb; d[3] = 0.0;
@@ -695,7 +698,7 @@ struct hb_adjoint {
     int32_t *d_gcell = nullptr;
     double *d_ckpt = nullptr;               // [T/k + 1][C][4]
     double *d_seg[2] = {nullptr, nullptr};   // [k + 1][C][4] states of a segment (two segments in flight)
-    double *d_terms[2] = {nullptr, nullptr}; // [k][4C][4] slot terms of a segment
+    double *d_terms = nullptr;              // [4C][4] slot terms of the step being recomputed
     cudaStream_t recompute = nullptr;        // the recomputation runs ahead of the reverse steps on its own stream
     cudaEvent_t ev_recomputed[2] = {nullptr, nullptr}, ev_reversed[2] = {nullptr, nullptr};
     double *d_gd = nullptr;                 // [nobs][ng] gauge depths of the forward
@@ -848,9 +851,9 @@ extern "C" int hb_adjoint_create(hb_handle *h, const int32_t *gauges, int32_t ng
     am.obs_every = obs_every;
     const int nck = nsteps / checkpoint_every + 1;
     if ((st = adj_alloc(a, &a->d_ckpt, (size_t)nck * 4 * C)) != HB_OK) return fail(st);
+    if ((st = adj_alloc(a, &a->d_terms, 16 * (size_t)C)) != HB_OK) return fail(st);
     for (int q = 0; q < 2; q++) {
         if ((st = adj_alloc(a, &a->d_seg[q], (size_t)(checkpoint_every + 1) * 4 * C)) != HB_OK) return fail(st);
-        if ((st = adj_alloc(a, &a->d_terms[q], (size_t)checkpoint_every * 16 * C)) != HB_OK) return fail(st);
         if (cudaEventCreateWithFlags(&a->ev_recomputed[q], cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&a->ev_reversed[q], cudaEventDisableTiming) != cudaSuccess)
             return fail(hb::set_error(HB_E_CUDA, "hb_adjoint_create: cudaEventCreate failed"));
@@ -1001,10 +1004,10 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const int nseg = (a->T + a->k - 1) / a->k;
-    // Segment sgi's states and slot terms are recomputed on the recompute
-    // stream into buffer sgi & 1, one segment ahead of the reverse steps on
-    // `st`: recompute(sgi - 1) overlaps reverse(sgi).  Events order each
-    // buffer's reuse.  The reverse kernels do not read the step counter or any
+    // Segment sgi's states are recomputed on the recompute stream into buffer
+    // sgi & 1, one segment ahead of the reverse steps on `st`: recompute(sgi -
+    // 1) overlaps reverse(sgi).  Each step's slot terms only pass through
+    // d_terms on the recompute stream.  Events order each buffer's reuse.  The reverse kernels do not read the step counter or any
     // other array the forward kernels write besides the segment buffers.
     cudaStream_t rs = a->recompute;
     cudaEvent_t start_ev = nullptr;
@@ -1022,7 +1025,7 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
         hb::adj::set_counter_kernel<<<1, 1, 0, rs>>>(h->d_ctr, t0);
         for (int i = 0; i < len; i++)
             TRY(hb_forward_step_into(h, t0, i, a->d_seg[b] + (size_t)i * S4, a->d_seg[b] + (size_t)(i + 1) * S4,
-                                     a->d_terms[b] + (size_t)i * 16 * C, rs));
+                                     a->d_terms, rs));
         HB_CUDA_RET(cudaEventRecord(a->ev_recomputed[b], rs));
         return HB_OK;
     };
@@ -1039,8 +1042,8 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
             const hb::adj::AdjStepBufs bufs{a->d_dir[w ^ 1], a->d_so[w ^ 1], a->d_sn[w ^ 1],
                                             a->d_dir[w], a->d_so[w], a->d_sn[w]};
             const int row = (t + 1 < a->T && (t + 1) % a->obs_every == 0) ? (t + 1) / a->obs_every - 1 : -1;
-            const double *xs = a->d_seg[b] + (size_t)i * S4, *ts = a->d_terms[b] + (size_t)i * 16 * C;
-            HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::adj::adj_step_kernel, h->m64, am, bufs, xs, ts, p,
+            const double *xs = a->d_seg[b] + (size_t)i * S4, *xn = xs + S4;
+            HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::adj::adj_step_kernel, h->m64, am, bufs, xs, xn, p,
                                            (int)(t == a->T - 1), row));
         }
         HB_CUDA_RET(cudaEventRecord(a->ev_reversed[b], st));

@@ -283,6 +283,12 @@ __device__ __forceinline__ void qf_acc_if(typename A::real out[4], bool on, bool
     }
 }
 
+// A piece that is not taken: traced as inactive (osher_f2 skips it).
+template <class A, class TR>
+__device__ __forceinline__ void qf_skip(TR *tr, int piece) {
+    if constexpr (!std::is_same<TR, void>::value) tr->f0[piece] = typename A::real(0);
+}
+
 // FLUX2 of a traced Osher evaluation re-summed with tangents ql2 / qr2, in the
 // same order and with the same fused sums as qf_acc_if.
 template <class A>
@@ -307,10 +313,11 @@ __device__ __forceinline__ typename A::real osher_f2(const OsherTrace<typename A
 // The reference's 16 (K1, K2) cases each add a signed subset of the pieces
 // 1 (left state), 2 (left sonic point), 3 (intermediate state, left),
 // 5 (intermediate state, right), 6 (right sonic point), 7 (right state), and
-// every case lists its pieces in increasing order.  Here all six pieces are
-// evaluated in that order and each is added when its case coefficient is
-// non-zero: the same sums in the same order, without the per-case branches
-// that would serialise a warp whose lanes fall into different cases.
+// every case lists its pieces in increasing order.  Here the six pieces are
+// taken in that order and each is added when its case coefficient is
+// non-zero: the same sums in the same order, without one branch per case.
+// Pieces without a division are formed on every lane and selected; those
+// with one are formed only by the lanes that take them.
 // Piece 3 updates FIL and piece 5 updates FIR (QS<3>, QS<5>); no case has
 // both, and piece 6 sees the FIR that piece 5 left.
 template <class A, class TR = void>
@@ -345,30 +352,40 @@ __device__ __forceinline__ void osher(typename A::real cl, const typename A::rea
     const bool p7 = any && k1 >= 3;
     // piece 1: QF(QL)
     qf_acc_if<A>(out, p1, false, ql[0], ql[1], ql[2], tr, 0);
+    // Pieces 2, 3, 5 and 6 divide; each is evaluated only where its case
+    // takes it (subcritical flow mostly takes 3 or 5 alone).
     // piece 2: US = FIL/3, HS = US^2/9.81
-    {
+    if (p2) {
         R us = A::divk(fil, 3.0);
         R hs = A::divk(A::mul(us, us), 9.81);
-        qf_acc_if<A>(out, p2, n2, hs, us, ql[2], tr, 1);
+        qf_acc_if<A>(out, true, n2, hs, us, ql[2], tr, 1);
+    } else {
+        qf_skip<A>(tr, 1);
     }
     // pieces 3 and 5 share UA = (FIL + FIR)/2
     const R ua35 = A::mul(A::add(fil, fir), A::c(0.5));
-    {
+    if (p3) {
         R fil3 = A::sub(fil, ua35);
         R ha = A::divk(A::mul(fil3, fil3), 39.24);
-        qf_acc_if<A>(out, p3, false, ha, ua35, ql[2], tr, 2);
+        qf_acc_if<A>(out, true, false, ha, ua35, ql[2], tr, 2);
+    } else {
+        qf_skip<A>(tr, 2);
     }
     R fir5 = A::sub(fir, ua35);
-    {
+    if (p5) {
         R ha = A::divk(A::mul(fir5, fir5), 39.24);
-        qf_acc_if<A>(out, p5, false, ha, ua35, qr[2], tr, 3);
+        qf_acc_if<A>(out, true, false, ha, ua35, qr[2], tr, 3);
+    } else {
+        qf_skip<A>(tr, 3);
     }
     // piece 6: US = FIR/3 with FIR as piece 5 left it
-    {
+    if (p6) {
         R f6 = p5 ? fir5 : fir;
         R us = A::divk(f6, 3.0);
         R hs = A::divk(A::mul(us, us), 9.81);
-        qf_acc_if<A>(out, p6, n6, hs, us, qr[2], tr, 4);
+        qf_acc_if<A>(out, true, n6, hs, us, qr[2], tr, 4);
+    } else {
+        qf_skip<A>(tr, 4);
     }
     // piece 7: QF(QR)
     qf_acc_if<A>(out, p7, false, qr[0], qr[1], qr[2], tr, 5);
