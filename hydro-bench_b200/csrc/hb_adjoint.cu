@@ -43,6 +43,20 @@ using A = F64Exact;
 // adjoint of one cell's slot inputs {h, u, v, z, zbc}
 struct Adj5 { double h, u, v, z, b; };
 
+// A slot's Adj5 contribution in memory: six doubles (the last one padding),
+// moved as three aligned 16-byte accesses.
+constexpr int ADJ_REC = 6;
+__device__ __forceinline__ void ld_rec(const double *p, double q[5]) {
+    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+    const double2 c = reinterpret_cast<const double2 *>(p)[2];
+    q[0] = a.x; q[1] = a.y; q[2] = b.x; q[3] = b.y; q[4] = c.x;
+}
+__device__ __forceinline__ void st_rec(double *p, const Adj5 &g) {
+    reinterpret_cast<double2 *>(p)[0] = make_double2(g.h, g.u);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(g.v, g.z);
+    reinterpret_cast<double2 *>(p)[2] = make_double2(g.b, 0.0);
+}
+
 // QF(h, u, v) = (h u, h u^2, h u v, 4.905 h^2) times `sign`, reversed with
 // output adjoint ob (functors.cu:505-511)
 __device__ __forceinline__ void qf_rev(double h, double u, double v, double sign, const double ob[4], double &hb,
@@ -473,10 +487,13 @@ __device__ __forceinline__ void gather4(const AdjMesh &a, const double *dir, con
                                         int c, int j, int obs_row, double l[4], double &zg) {
     const size_t s = 4 * (size_t)c + j;
     double part[5];
-    for (int q = 0; q < 5; q++) part[q] = so[5 * s + q];
+    ld_rec(so + ADJ_REC * s, part);
     const int mj = a.mirror4[s];
-    if (mj >= 0)
-        for (int q = 0; q < 5; q++) part[q] += sn[5 * (size_t)mj + q];
+    if (mj >= 0) {
+        double q5[5];
+        ld_rec(sn + ADJ_REC * (size_t)mj, q5);
+        for (int q = 0; q < 5; q++) part[q] += q5[q];
+    }
     for (int q = 0; q < 5; q++) {
         part[q] += __shfl_xor_sync(0xffffffffu, part[q], 1);
         part[q] += __shfl_xor_sync(0xffffffffu, part[q], 2);
@@ -520,7 +537,8 @@ __global__ void __launch_bounds__(128, 7) adj_step_kernel(DevMesh<A> m, AdjMesh 
     } else {
         gather4(a, b.dir_in, b.so_in, b.sn_in, c, j, obs_row, l, zg);
     }
-    const double hv = x[4 * (size_t)c], uv = x[4 * (size_t)c + 1], vv = x[4 * (size_t)c + 2];
+    const Vec4<double> xc = ld4(x + 4 * (size_t)c);
+    const double hv = xc.x, uv = xc.y, vv = xc.z;
     const double zbc = m.zbc[c];
     double whb = 0.0, wub = 0.0, wvb = 0.0;
     if (j == 0) {
@@ -570,10 +588,11 @@ __global__ void __launch_bounds__(128, 7) adj_step_kernel(DevMesh<A> m, AdjMesh 
     if (!valid) return;
     // ---- lane j: slot 4c+j
     const size_t s = 4 * (size_t)c + j;
-    double *so = b.so_out + 5 * s, *sno = b.sn_out + 5 * s;
+    double *so = b.so_out + ADJ_REC * s, *sno = b.sn_out + ADJ_REC * s;
     const uint8_t meta = a.meta4[s];
     if (meta == 0xFF) {
-        for (int q = 0; q < 5; q++) { so[q] = 0.0; sno[q] = 0.0; }
+        st_rec(so, Adj5{0, 0, 0, 0, 0});
+        st_rec(sno, Adj5{0, 0, 0, 0, 0});
         return;
     }
     const double cs = a.cs4[s], sn = a.sn4[s], side = a.side4[s];
@@ -584,14 +603,15 @@ __global__ void __launch_bounds__(128, 7) adj_step_kernel(DevMesh<A> m, AdjMesh 
     fb[2] = -slsin * wub + slcos * wvb;
     fb[3] = fb[1];
     SlotInA<A> in;
-    in.own = CellStateA<A>{hv, uv, vv, x[4 * (size_t)c + 3], zbc};
+    in.own = CellStateA<A>{hv, uv, vv, xc.w, zbc};
     in.code = (int8_t)(meta & META_CODE);
     in.own_first = meta & META_OWN_FIRST;
     in.has_nb = meta & META_HAS_NB;
     const int nb = a.nbr4[s];
-    if (in.has_nb)
-        in.nb = CellStateA<A>{x[4 * (size_t)nb], x[4 * (size_t)nb + 1], x[4 * (size_t)nb + 2], x[4 * (size_t)nb + 3],
-                              m.zbc[nb]};
+    if (in.has_nb) {
+        const Vec4<double> xn4 = ld4(x + 4 * (size_t)nb);
+        in.nb = CellStateA<A>{xn4.x, xn4.y, xn4.z, xn4.w, m.zbc[nb]};
+    }
     else
         in.nb = CellStateA<A>{0, 0, 0, 0, 0};
     in.cosj = cs; in.sinj = sn; in.side = side;
@@ -612,8 +632,8 @@ __global__ void __launch_bounds__(128, 7) adj_step_kernel(DevMesh<A> m, AdjMesh 
     };
     Adj5 go{0, 0, 0, 0, 0}, gn{0, 0, 0, 0, 0};
     slot_rev(in, p, fetch, fb, go, gn, m.err);
-    so[0] = go.h; so[1] = go.u; so[2] = go.v; so[3] = go.z; so[4] = go.b;
-    sno[0] = gn.h; sno[1] = gn.u; sno[2] = gn.v; sno[3] = gn.z; sno[4] = gn.b;
+    st_rec(so, go);
+    st_rec(sno, gn);
 }
 
 // The adjoint of x_0 from step 0's contributions, into a.lam, with their bed terms.
@@ -706,8 +726,8 @@ struct hb_adjoint {
     double *d_res = nullptr;                // [nobs][ng]
     double *d_z0 = nullptr, *d_u0 = nullptr, *d_v0 = nullptr;   // initial level and velocities (device order)
     double *d_dir[2] = {nullptr, nullptr};  // [C][4] the update's direct terms, by step parity
-    double *d_so[2] = {nullptr, nullptr};   // [4C][5] slots' contributions to their own cells
-    double *d_sn[2] = {nullptr, nullptr};   // [4C][5] slots' contributions to their neighbours
+    double *d_so[2] = {nullptr, nullptr};   // [4C][ADJ_REC] slots' contributions to their own cells
+    double *d_sn[2] = {nullptr, nullptr};   // [4C][ADJ_REC] slots' contributions to their neighbours
     hb::adj::AdjMesh am{};
     cudaGraphExec_t fwd_graph = nullptr;    // k forward steps with checkpoint and gauge kernels
     bool forward_done = false;
@@ -839,8 +859,8 @@ extern "C" int hb_adjoint_create(hb_handle *h, const int32_t *gauges, int32_t ng
     if ((st = adj_upload(a, &a->d_gcell, a->gauges_dev)) != HB_OK) return fail(st);
     for (int q = 0; q < 2; q++) {
         if ((st = adj_alloc(a, &a->d_dir[q], 4 * (size_t)C)) != HB_OK) return fail(st);
-        if ((st = adj_alloc(a, &a->d_so[q], 20 * (size_t)C)) != HB_OK) return fail(st);
-        if ((st = adj_alloc(a, &a->d_sn[q], 20 * (size_t)C)) != HB_OK) return fail(st);
+        if ((st = adj_alloc(a, &a->d_so[q], 4 * hb::adj::ADJ_REC * (size_t)C)) != HB_OK) return fail(st);
+        if ((st = adj_alloc(a, &a->d_sn[q], 4 * hb::adj::ADJ_REC * (size_t)C)) != HB_OK) return fail(st);
     }
     if ((st = adj_alloc(a, &am.fnc_g, C)) != HB_OK) return fail(st);
     if ((st = adj_alloc(a, &am.zbc_g, C)) != HB_OK) return fail(st);
