@@ -18,13 +18,15 @@
 //
 // Memory: the state is kept every `checkpoint_every` = k steps; the backward
 // pass recomputes each k-step segment from its checkpoint, keeping that
-// segment's states, then runs the segment's reverse steps, one
+// segment's states and the update coefficients of its steps (written by
+// the recomputed update kernels), then runs the segment's reverse steps, one
 // kernel each (adj_step_kernel, four lanes per cell):
 //   - the state adjoint after the step, gathered from the later step's
 //     direct terms, the cell's own slots' contributions and those of the
 //     neighbours' slots that face it (fixed order, no atomics: the gradient
 //     is deterministic);
-//   - lane 0: the cell update's reverse, shared with the other lanes;
+//   - lane 0: the cell update's reverse (from the stored coefficients),
+//     shared with the other lanes;
 //   - lane j: slot j's flux reverse, leaving its contributions to its own
 //     cell and its neighbour for the next (earlier) step.
 // The forward rollout is replayed from a CUDA graph of k steps whose
@@ -506,12 +508,23 @@ __device__ __forceinline__ void gather4(const AdjMesh &a, const double *dir, con
     }
 }
 
+// The update coefficients of a step (update_cell with COEF, written by the
+// recomputed step's update kernel) for the reverse of the cell update.
+struct UpdateCoef { double dtw, ih2, d_fnc, d_h, d_s; };
+__device__ __forceinline__ UpdateCoef ld_coef(const double *p) {
+    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+    const double2 c = reinterpret_cast<const double2 *>(p)[2];
+    return {a.x, a.y, b.x, b.y, c.x};
+}
+
 // One reverse step t, four lanes per cell.  x: the state before the step; xn:
 // the state after it.  The adjoint of the state after the step is gathered
 // first from step t + 1's contributions (`first`: it is the seed a.lam
 // instead), with the loss term of row `obs_row` when step t + 1 ends on an
 // observation.  Lane 0 reverses the cell update and shares the adjoints of the
 // slot sums; lane j then reverses slot j.
+//
+// coef: the step's update coefficients (written with the recomputed step).
 //
 // The update's forward values come from xn rather than from the slot sums:
 // H2 = max(H + QLUA - DTA WH, HM1) is xn's depth, so H2 > HM1 exactly when the
@@ -523,7 +536,8 @@ __device__ __forceinline__ void gather4(const AdjMesh &a, const double *dir, con
 // L2 gathers, and more resident warps hide them better than fewer spills do.
 __global__ void __launch_bounds__(128, 7) adj_step_kernel(DevMesh<A> m, AdjMesh a, AdjStepBufs b,
                                                           const double *__restrict__ x, const double *__restrict__ xn,
-                                                          StepParams p, int first, int obs_row) {
+                                                          const double *__restrict__ coef, StepParams p, int first,
+                                                          int obs_row) {
     // launched with programmatic dependent launch: wait for the previous kernel's results
     cudaGridDependencySynchronize();
     cudaTriggerProgrammaticLaunchCompletion();
@@ -543,33 +557,28 @@ __global__ void __launch_bounds__(128, 7) adj_step_kernel(DevMesh<A> m, AdjMesh 
     double whb = 0.0, wub = 0.0, wvb = 0.0;
     if (j == 0) {
         // ---- the update (UpdateCellKernel, functors.cu:717-784, variant H): forward values, then its reverse
-        const double HM1 = p.hm1, HM2 = p.hm2, DT = p.dt;
-        const double dta = m.dta[c], fnc = m.fnc[c];
-        const double h2 = xn[4 * (size_t)c], u2 = xn[4 * (size_t)c + 1], v2 = xn[4 * (size_t)c + 2];
+        const double HM1 = p.hm1, HM2 = p.hm2;
+        const double dta = m.dta[c];
+        const Vec4<double> xn4 = ld4(xn + 4 * (size_t)c);
+        const double h2 = xn4.x, u2 = xn4.y, v2 = xn4.z;
         double h2b = l[0] + l[3];   // Z2 = H2 + ZBC
         double hb = 0.0, ub = 0.0, vb = 0.0, fncb = 0.0;
         if (h2 > HM2) {
-            const double s2 = A::dot(uv, uv, vv, vv, M_SQ1);
-            const double sq = A::sqrt(s2);
-            const double hp = A::pow(hv, A::c(0.33333));
-            const double wsf = A::div(A::mul(fnc, sq), hp);
-            const double dtw = A::mul(DT, wsf);
-            const double ih2 = 1.0 / h2, ihp = 1.0 / hp;
+            const UpdateCoef k = ld_coef(coef + UPDATE_COEF * (size_t)c);
             const double ue = fabs(u2) < 15.0 ? l[1] : 0.0;
             const double ve = fabs(v2) < 15.0 ? l[2] : 0.0;
-            const double nub = ue * ih2, nvb = ve * ih2;
-            h2b -= (ue * u2 + ve * v2) * ih2;
+            const double nub = ue * k.ih2, nvb = ve * k.ih2;
+            h2b -= (ue * u2 + ve * v2) * k.ih2;
             hb += nub * uv + nvb * vv;
-            ub += nub * (hv - dtw);
-            vb += nvb * (hv - dtw);
+            ub += nub * (hv - k.dtw);
+            vb += nvb * (hv - k.dtw);
             wub -= nub * dta;
             wvb -= nvb * dta;
             const double dtwb = -(nub * uv + nvb * vv);
-            // dtw = DT fnc s / h^p
-            fncb += dtwb * DT * sq * ihp;
-            const double sb = dtwb * DT * fnc * ihp;
-            hb += dtwb * DT * fnc * sq * (-0.33333) * ihp / hv;
-            if (sq > 0.0) { const double is = 1.0 / sq; ub += sb * uv * is; vb += sb * vv * is; }
+            fncb += dtwb * k.d_fnc;
+            hb += dtwb * k.d_h;
+            ub += dtwb * k.d_s * uv;
+            vb += dtwb * k.d_s * vv;
         } else if (h2 > HM1) {
             if (fabs(uv) < K::VMIN) ub += l[1];
             if (fabs(vv) < K::VMIN) vb += l[2];
@@ -683,9 +692,15 @@ __global__ void adj_init_rev_kernel(int C, AdjMesh a, const double *__restrict__
 
 __global__ void set_counter_kernel(long long *ctr, long long v) { *ctr = v; }
 
+// The checkpoint and gauge kernels sit between step sequences of the forward
+// and are chained to them by programmatic dependent launch: each waits for
+// the previous kernel's results and lets the next one launch at once.
+
 // the state before step t = *ctr into checkpoint t / k (when t is a multiple of k)
 __global__ void ckpt_kernel(const double *S0, const double *S1, double *ckpt, const long long *ctr, int k,
                             size_t n) {
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
     const long long t = *ctr;
     if (t % k != 0) return;
     const double *src = (t & 1) ? S1 : S0;
@@ -697,6 +712,8 @@ __global__ void ckpt_kernel(const double *S0, const double *S1, double *ckpt, co
 // after t = *ctr steps, when t ends on an observation: the gauge depths into row t / obs_every - 1
 __global__ void gauge_ctr_kernel(const double *S0, const double *S1, const int32_t *__restrict__ gcell, int ng,
                                  double *gd, const long long *ctr, int obs_every) {
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
     const long long t = *ctr;
     if (t == 0 || t % obs_every != 0) return;
     const double *S = (t & 1) ? S1 : S0;
@@ -719,6 +736,7 @@ struct hb_adjoint {
     double *d_ckpt = nullptr;               // [T/k + 1][C][4]
     double *d_seg[2] = {nullptr, nullptr};   // [k + 1][C][4] states of a segment (two segments in flight)
     double *d_terms = nullptr;              // [4C][4] slot terms of the step being recomputed
+    double *d_coef[2] = {nullptr, nullptr}; // [k][C][UPDATE_COEF] update coefficients of a segment
     cudaStream_t recompute = nullptr;        // the recomputation runs ahead of the reverse steps on its own stream
     cudaEvent_t ev_recomputed[2] = {nullptr, nullptr}, ev_reversed[2] = {nullptr, nullptr};
     double *d_gd = nullptr;                 // [nobs][ng] gauge depths of the forward
@@ -874,6 +892,8 @@ extern "C" int hb_adjoint_create(hb_handle *h, const int32_t *gauges, int32_t ng
     if ((st = adj_alloc(a, &a->d_terms, 16 * (size_t)C)) != HB_OK) return fail(st);
     for (int q = 0; q < 2; q++) {
         if ((st = adj_alloc(a, &a->d_seg[q], (size_t)(checkpoint_every + 1) * 4 * C)) != HB_OK) return fail(st);
+        if ((st = adj_alloc(a, &a->d_coef[q], (size_t)checkpoint_every * hb::UPDATE_COEF * C)) != HB_OK)
+            return fail(st);
         if (cudaEventCreateWithFlags(&a->ev_recomputed[q], cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&a->ev_reversed[q], cudaEventDisableTiming) != cudaSuccess)
             return fail(hb::set_error(HB_E_CUDA, "hb_adjoint_create: cudaEventCreate failed"));
@@ -948,10 +968,22 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
     // forward steps t0 .. t0+n-1: checkpoint at the segment's start, gauge
     // depths after every step that ends on an observation (positions fixed
     // when k is a multiple of obs_every, otherwise after every step)
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
     auto enqueue = [&](int t0, int n, cudaStream_t s) -> int {
         const double *S0 = h->m64.S[0], *S1 = h->m64.S[1];
-        hb::adj::ckpt_kernel<<<64, 256, 0, s>>>(S0, S1, a->d_ckpt, h->d_ctr, a->k, S4);
-        HB_CUDA_RET(cudaGetLastError());
+        cudaLaunchConfig_t ck{};
+        ck.gridDim = dim3(64);
+        ck.blockDim = dim3(256);
+        ck.stream = s;
+        ck.attrs = attr;
+        ck.numAttrs = 1;
+        cudaLaunchConfig_t gk = ck;
+        gk.gridDim = dim3((unsigned)((a->ng + 127) / 128));
+        gk.blockDim = dim3(128);
+        HB_CUDA_RET(cudaLaunchKernelEx(&ck, hb::adj::ckpt_kernel, S0, S1, a->d_ckpt, (const long long *)h->d_ctr, a->k,
+                                       S4));
         // runs of steps up to each observation: one multi-step launch sequence each
         for (int i = 0; i < n;) {
             int m = n - i;
@@ -959,9 +991,8 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
             else m = 1;
             TRY(hb_enqueue_steps(h, m, s));
             i += m;
-            hb::adj::gauge_ctr_kernel<<<(a->ng + 127) / 128, 128, 0, s>>>(S0, S1, a->d_gcell, a->ng, a->d_gd,
-                                                                          h->d_ctr, a->obs_every);
-            HB_CUDA_RET(cudaGetLastError());
+            HB_CUDA_RET(cudaLaunchKernelEx(&gk, hb::adj::gauge_ctr_kernel, S0, S1, (const int32_t *)a->d_gcell, a->ng,
+                                           a->d_gd, (const long long *)h->d_ctr, a->obs_every));
         }
         return HB_OK;
     };
@@ -1024,11 +1055,13 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const int nseg = (a->T + a->k - 1) / a->k;
-    // Segment sgi's states are recomputed on the recompute stream into buffer
-    // sgi & 1, one segment ahead of the reverse steps on `st`: recompute(sgi -
-    // 1) overlaps reverse(sgi).  Each step's slot terms only pass through
-    // d_terms on the recompute stream.  Events order each buffer's reuse.  The reverse kernels do not read the step counter or any
-    // other array the forward kernels write besides the segment buffers.
+    // Segment sgi's states and update coefficients are recomputed on the
+    // recompute stream into buffer sgi & 1, one segment ahead of the reverse
+    // steps on `st`: recompute(sgi - 1) overlaps reverse(sgi).  Each step's
+    // slot terms only pass through d_terms on the recompute stream.  Events
+    // order each buffer's reuse.  The reverse kernels do not read the step
+    // counter or any other array the forward kernels write besides the
+    // segment buffers.
     cudaStream_t rs = a->recompute;
     cudaEvent_t start_ev = nullptr;
     HB_CUDA_RET(cudaEventCreateWithFlags(&start_ev, cudaEventDisableTiming));
@@ -1045,7 +1078,7 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
         hb::adj::set_counter_kernel<<<1, 1, 0, rs>>>(h->d_ctr, t0);
         for (int i = 0; i < len; i++)
             TRY(hb_forward_step_into(h, t0, i, a->d_seg[b] + (size_t)i * S4, a->d_seg[b] + (size_t)(i + 1) * S4,
-                                     a->d_terms, rs));
+                                     a->d_terms, a->d_coef[b] + (size_t)i * hb::UPDATE_COEF * C, rs));
         HB_CUDA_RET(cudaEventRecord(a->ev_recomputed[b], rs));
         return HB_OK;
     };
@@ -1063,7 +1096,8 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
                                             a->d_dir[w], a->d_so[w], a->d_sn[w]};
             const int row = (t + 1 < a->T && (t + 1) % a->obs_every == 0) ? (t + 1) / a->obs_every - 1 : -1;
             const double *xs = a->d_seg[b] + (size_t)i * S4, *xn = xs + S4;
-            HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::adj::adj_step_kernel, h->m64, am, bufs, xs, xn, p,
+            const double *cf = a->d_coef[b] + (size_t)i * hb::UPDATE_COEF * C;
+            HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::adj::adj_step_kernel, h->m64, am, bufs, xs, xn, cf, p,
                                            (int)(t == a->T - 1), row));
         }
         HB_CUDA_RET(cudaEventRecord(a->ev_reversed[b], st));

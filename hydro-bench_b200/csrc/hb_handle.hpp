@@ -118,6 +118,8 @@ int hb_enqueue_steps(hb_handle *h, int n, cudaStream_t st);
 int hb_check_range(hb_handle *h, long long n);
 // One fp64 edge-layout step t0 + k (the device step counter must hold t0)
 // from state `in` to state `out` ([C][4] each), keeping the slots' terms of
-// the cell sums in `terms` ([4C][4]); the handle's W is overwritten, the fluxes are not.
+// the cell sums in `terms` ([4C][4]) and the update coefficients of the wet
+// cells in `coef` ([C][UPDATE_COEF]); the handle's W is overwritten, the
+// fluxes are not.
 int hb_forward_step_into(hb_handle *h, long long t0, int k, const double *in, double *out, double *terms,
-                         cudaStream_t st);
+                         double *coef, cudaStream_t st);

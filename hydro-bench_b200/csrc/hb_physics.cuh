@@ -830,10 +830,18 @@ __device__ __forceinline__ void wsum_add(typename A::real &wh, typename A::real 
     wv = A::add(wv, A::dot(slsin, fr1, slcos, fr2, M_WV));
 }
 
-template <class A, int VARIANT>
+// Coefficients of a wet cell's velocity update for the reverse sweep (COEF):
+// U2 = (H U - DTA WU - DTW U) / H2, DTW = DT FNC S / H^0.33333, S = |(U, V)|
+// (functors.cu:766-772).  Six doubles per cell:
+//   {DTW, 1/H2, dDTW/dFNC, dDTW/dH, (dDTW/dS)/S (0 when S = 0), 0}.
+constexpr int UPDATE_COEF = 6;
+
+// COEF: also write the cell's update coefficients to `coef` when the cell is
+// wet after the step (H2 > HM2; fp64 only).
+template <class A, int VARIANT, bool COEF = false>
 __device__ __forceinline__ CellUpdateOut<typename A::real, typename A::level>
 update_cell(const CellUpdateIn<typename A::real, typename A::level> &c, typename A::real wh, typename A::real wu,
-            typename A::real wv, const StepParams &p) {
+            typename A::real wv, const StepParams &p, double *coef = nullptr) {
     using R = typename A::real;
     const R HM1 = A::c(p.hm1), HM2 = A::c(p.hm2), DT = A::c(p.dt);
     R dta;
@@ -870,12 +878,22 @@ update_cell(const CellUpdateIn<typename A::real, typename A::level> &c, typename
         o.u = A::copysign(A::fmin(A::c(K::VMIN), A::fabs(c.u)), c.u);
         o.v = A::copysign(A::fmin(A::c(K::VMIN), A::fabs(c.v)), c.v);
     } else {
-        R wsf = A::div(A::mul(c.fnc, A::sqrt(A::dot(c.u, c.u, c.v, c.v, M_SQ1))), A::pow(c.h, A::c(0.33333)));
+        const R sq = A::sqrt(A::dot(c.u, c.u, c.v, c.v, M_SQ1));
+        const R hp = A::pow(c.h, A::c(0.33333));
+        R wsf = A::div(A::mul(c.fnc, sq), hp);
         R dtw = A::mul(DT, wsf);
         R u2 = A::div(A::madd(-dtw, c.u, A::dot(c.h, c.u, -dta, wu, M_U2A), M_U2B), o.h);
         R v2 = A::div(A::madd(-dtw, c.v, A::dot(c.h, c.v, -dta, wv, M_U2A), M_U2B), o.h);
         o.u = A::copysign(A::fmin(A::fabs(u2), cap), u2);
         o.v = A::copysign(A::fmin(A::fabs(v2), cap), v2);
+        if constexpr (COEF) {
+            static_assert(std::is_same<R, double>::value, "update coefficients are fp64");
+            const double ihp = 1.0 / hp;
+            double2 *q = reinterpret_cast<double2 *>(coef);
+            q[0] = make_double2(dtw, 1.0 / o.h);
+            q[1] = make_double2(DT * sq * ihp, DT * c.fnc * sq * (-0.33333) * ihp / c.h);
+            q[2] = make_double2(sq > 0.0 ? DT * c.fnc * ihp / sq : 0.0, 0.0);
+        }
     }
     o.w = A::sqrt(A::dot(o.u, o.u, o.v, o.v, M_SQ2));
     return o;

@@ -553,6 +553,22 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *mds, int n, hb::DevMesh<
     return HB_OK;
 }
 
+// The counter tick after a step sequence, chained to it by programmatic
+// dependent launch.
+int launch_tick(hb_handle *h, int n, cudaStream_t st) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(1);
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::tick_kernel, h->d_ctr, n));
+    return HB_OK;
+}
+
 template <class A, int VARIANT, bool SEG>
 int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     // Programmatic dependent launch: each kernel may start while its predecessor
@@ -594,9 +610,7 @@ int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     default: return hb::set_error(HB_E_INVALID, "launch shape %d is not an edge-layout shape", h->launch_config + 1);
     }
     if (rc != HB_OK) return rc;
-    hb::tick_kernel<<<1, 1, 0, st>>>(h->d_ctr, n);
-    HB_CUDA_RET(cudaGetLastError());
-    return HB_OK;
+    return launch_tick(h, n, st);
 }
 
 size_t tile_smem_bytes(int max_cells, int max_pairs, size_t real_size) {
@@ -634,9 +648,7 @@ int launch_tiles_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
         return HB_OK;
     });
     if (rc != HB_OK) return rc;
-    hb::tick_kernel<<<1, 1, 0, st>>>(h->d_ctr, n);
-    HB_CUDA_RET(cudaGetLastError());
-    return HB_OK;
+    return launch_tick(h, n, st);
 }
 
 // Lets every tile kernel of the handle's policy use the shared memory its
@@ -693,12 +705,13 @@ int hb_enqueue_steps(hb_handle *h, int n, cudaStream_t st) { return enqueue_step
 int hb_check_range(hb_handle *h, long long n) { return check_range(h, n); }
 
 int hb_forward_step_into(hb_handle *h, long long t0, int k, const double *in, double *out, double *terms,
-                         cudaStream_t st) {
+                         double *coef, cudaStream_t st) {
     hb::DevMesh<hb::F64Exact> m = h->m64;
     const int par = (int)((t0 + k) & 1);
     m.S[par] = const_cast<double *>(in);
     m.S[par ^ 1] = out;
     m.slotw = terms;
+    m.ucoef = coef;
     // programmatic dependent launch, as in the step sequence (launch_steps_t)
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -712,7 +725,7 @@ int hb_forward_step_into(hb_handle *h, long long t0, int k, const double *in, do
     HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::flux_kernel<hb::F64Exact, 0, 128, 6, false>, m, k, 0));
     cfg.gridDim = dim3((unsigned)((m.C + hb::UPDATE_THREADS - 1) / hb::UPDATE_THREADS));
     cfg.blockDim = dim3(hb::UPDATE_THREADS);
-    HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::update_kernel<hb::F64Exact, 0, 6, false>, m, k, 0));
+    HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::update_kernel<hb::F64Exact, 0, 6, false, true>, m, k, 0));
     return HB_OK;
 }
 

@@ -70,6 +70,7 @@ struct DevMesh {
     const int32_t *bcell;      // [C] row of the boundary tables, -1 = none
     const uint8_t *cmask;      // [C] bit j: slot j is a real slot
     R *slotw;                  // [4C][4] per-slot terms of the cell sums {F0, dWU, dWV, SIDE}
+    double *ucoef;             // [C][UPDATE_COEF] update coefficients (update kernels with COEF only)
     // records [nrecords]
     const int4 *rix;           // {a, b, sa, sb}: cell of the slot, its neighbour (-1 = none),
                                // slot 4*a+j, and for a pair the slot of b (-1 otherwise)
@@ -356,7 +357,7 @@ __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k
 // Sums and update of one cell (UpdateCellKernel, functors.cu:717-784).  The
 // zero-length fourth slot of a triangle is evaluated here without pow
 // (flux_slot's ZERO_LEN), exactly when fluxes are written out.
-template <class A, int VARIANT>
+template <class A, int VARIANT, bool COEF = false>
 __device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const StepIndex &si, const StepParams &p,
                                            int write_flux, const typename A::real *terms) {
     using R = typename A::real;
@@ -404,7 +405,8 @@ __device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const Ste
     ci.fnc = fnc;
     ci.dta_or_area = dta;
     ci.sidex = sidex;
-    CellUpdateOut<R, L> o = update_cell<A, VARIANT>(ci, wh, wu, wv, p);
+    CellUpdateOut<R, L> o =
+        update_cell<A, VARIANT, COEF>(ci, wh, wu, wv, p, COEF ? m.ucoef + UPDATE_COEF * (size_t)c : nullptr);
     const int np = si.par ^ 1;
     if constexpr (is_split<A>::value) st4(m.S[np] + 4 * (size_t)c, o.h, o.u, o.v, o.hlo);
     else st4(m.S[np] + 4 * (size_t)c, o.h, o.u, o.v, o.z);
@@ -413,8 +415,9 @@ __device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const Ste
 }
 
 // Every cell of one step.  Single mesh: a grid-stride loop over the cells.
-// Batch: CTA b takes the scenario and cell range of useg[b].
-template <class A, int VARIANT, int UMINB, bool SEG>
+// Batch: CTA b takes the scenario and cell range of useg[b].  COEF: also the
+// update coefficients of the wet cells into m.ucoef.
+template <class A, int VARIANT, int UMINB, bool SEG, bool COEF = false>
 __global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<A> m, int k, int write_flux) {
     if constexpr (SEG) {
         const int4 d = m.useg[blockIdx.x];
@@ -424,14 +427,14 @@ __global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<A
         const StepIndex si = step_index(m, k, sp.per_day, sp.ndays);
         const StepParams p{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
         const int c = d.y + (int)threadIdx.x;
-        if ((int)threadIdx.x < d.z) update_one<A, VARIANT>(m, c, si, p, write_flux, m.slotw + 16 * (size_t)c);
+        if ((int)threadIdx.x < d.z) update_one<A, VARIANT, COEF>(m, c, si, p, write_flux, m.slotw + 16 * (size_t)c);
     } else {
         cudaGridDependencySynchronize();
         cudaTriggerProgrammaticLaunchCompletion();
         const StepIndex si = step_index(m, k, m.per_day, m.ndays);
         const StepParams p{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
         for (int c = blockIdx.x * UPDATE_THREADS + threadIdx.x; c < m.C; c += gridDim.x * UPDATE_THREADS)
-            update_one<A, VARIANT>(m, c, si, p, write_flux, m.slotw + 16 * (size_t)c);
+            update_one<A, VARIANT, COEF>(m, c, si, p, write_flux, m.slotw + 16 * (size_t)c);
     }
 }
 
@@ -469,7 +472,14 @@ __global__ void __launch_bounds__(THREADS, MINB) tile_kernel(DevMesh<A> m, int k
         update_one<A, VARIANT>(m, td.cell0 + c, si, p, write_flux, terms + 16 * c);
 }
 
-static __global__ void tick_kernel(long long *ctr, int n) { *ctr += n; }
+// Advances the step counter after a step sequence.  Launched with
+// programmatic dependent launch like the step kernels: it waits for the last
+// step's results and lets the next kernel launch at once.
+static __global__ void tick_kernel(long long *ctr, int n) {
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
+    *ctr += n;
+}
 
 // Split precision state <-> the reference's (H, Z) of one cell.  The depth is
 // kept as the fp32 pair (h, hlo) with h + hlo = H; a cell at or below the dry
