@@ -721,6 +721,14 @@ __global__ void gauge_ctr_kernel(const double *S0, const double *S1, const int32
     if (g < ng) gd[(size_t)(t / obs_every - 1) * ng + g] = S[4 * (size_t)gcell[g]];
 }
 
+// the gauge depths of state S (after a step that ends on an observation) into row `row`
+__global__ void gauge_state_kernel(const double *S, const int32_t *__restrict__ gcell, int ng, double *gd, int row) {
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < ng) gd[(size_t)row * ng + g] = S[4 * (size_t)gcell[g]];
+}
+
 }  // namespace adj
 }  // namespace hb
 
@@ -737,6 +745,7 @@ struct hb_adjoint {
     double *d_seg[2] = {nullptr, nullptr};   // [k + 1][C][4] states of a segment (two segments in flight)
     double *d_terms = nullptr;              // [4C][4] slot terms of the step being recomputed
     double *d_coef[2] = {nullptr, nullptr}; // [k][C][UPDATE_COEF] update coefficients of a segment
+    int recorded_seg = -1;                  // segment whose states the forward left in d_seg (-1: none)
     cudaStream_t recompute = nullptr;        // the recomputation runs ahead of the reverse steps on its own stream
     cudaEvent_t ev_recomputed[2] = {nullptr, nullptr}, ev_reversed[2] = {nullptr, nullptr};
     double *d_gd = nullptr;                 // [nobs][ng] gauge depths of the forward
@@ -965,6 +974,7 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
     hb::adj::set_counter_kernel<<<1, 1, 0, st>>>(h->d_ctr, 0);
     HB_CUDA_RET(cudaMemsetAsync(h->d_err, 0, sizeof(uint32_t), st));
     h->steps_done = 0;
+    a->recorded_seg = -1;
     // forward steps t0 .. t0+n-1: checkpoint at the segment's start, gauge
     // depths after every step that ends on an observation (positions fixed
     // when k is a multiple of obs_every, otherwise after every step)
@@ -996,8 +1006,13 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
         }
         return HB_OK;
     };
-    const int nfull = a->T / a->k;
-    if (nfull > 0 && !a->fwd_graph) {
+    // Segments 0 .. nseg-2 replay the k-step graph; the last one (k steps or
+    // the remainder) is stepped into the segment buffer with its update
+    // coefficients, as the backward pass would recompute it, so the backward
+    // starts reversing at once.
+    const int nseg = (a->T + a->k - 1) / a->k;
+    const int ngraph = nseg - 1;
+    if (ngraph > 0 && !a->fwd_graph) {
         cudaStream_t cap;
         HB_CUDA_RET(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
         HB_CUDA_RET(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
@@ -1011,8 +1026,38 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
         cudaGraphDestroy(g);
         if (ei != cudaSuccess) { a->fwd_graph = nullptr; return hb::set_error(HB_E_CUDA, "adjoint forward graph: %s", cudaGetErrorString(ei)); }
     }
-    for (int sgi = 0; sgi < nfull; sgi++) HB_CUDA_RET(cudaGraphLaunch(a->fwd_graph, st));
-    if (a->T % a->k) TRY(enqueue(nfull * a->k, a->T % a->k, st));
+    for (int sgi = 0; sgi < ngraph; sgi++) HB_CUDA_RET(cudaGraphLaunch(a->fwd_graph, st));
+    {
+        const int sgi = nseg - 1, t0 = sgi * a->k, len = a->T - t0, b = sgi & 1;
+        cudaLaunchConfig_t ck{};
+        ck.gridDim = dim3(64);
+        ck.blockDim = dim3(256);
+        ck.stream = st;
+        ck.attrs = attr;
+        ck.numAttrs = 1;
+        cudaLaunchConfig_t gk = ck;
+        gk.gridDim = dim3((unsigned)((a->ng + 127) / 128));
+        gk.blockDim = dim3(128);
+        HB_CUDA_RET(cudaLaunchKernelEx(&ck, hb::adj::ckpt_kernel, (const double *)h->m64.S[0],
+                                       (const double *)h->m64.S[1], a->d_ckpt, (const long long *)h->d_ctr, a->k,
+                                       S4));
+        for (int i = 0; i < len; i++) {
+            const double *in = i == 0 ? h->m64.S[t0 & 1] : a->d_seg[b] + (size_t)i * S4;
+            double *out = a->d_seg[b] + (size_t)(i + 1) * S4;
+            TRY(hb_forward_step_into(h, t0, i, in, out, a->d_terms, a->d_coef[b] + (size_t)i * hb::UPDATE_COEF * C,
+                                     (int)(i == len - 1), st));
+            const int t = t0 + i + 1;
+            if (t % a->obs_every == 0)
+                HB_CUDA_RET(cudaLaunchKernelEx(&gk, hb::adj::gauge_state_kernel, (const double *)out,
+                                               (const int32_t *)a->d_gcell, a->ng, a->d_gd, t / a->obs_every - 1));
+        }
+        // the handle's state and counter after the rollout
+        HB_CUDA_RET(cudaMemcpyAsync(h->m64.S[a->T & 1], a->d_seg[b] + (size_t)len * S4, S4 * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, st));
+        hb::adj::set_counter_kernel<<<1, 1, 0, st>>>(h->d_ctr, a->T);
+        HB_CUDA_RET(cudaGetLastError());
+        a->recorded_seg = sgi;
+    }
     h->steps_done = a->T;
     HB_CUDA_RET(cudaStreamSynchronize(st));
     uint32_t bits = 0;
@@ -1069,25 +1114,29 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
     HB_CUDA_RET(cudaStreamWaitEvent(rs, start_ev, 0));   // after this call's earlier work on st
     cudaEventDestroy(start_ev);
     bool reversed_once[2] = {false, false};
+    // state i of segment sgi: its checkpoint, then the segment buffer
+    auto seg_state = [&](int sgi, int i) -> const double * {
+        return i == 0 ? a->d_ckpt + (size_t)sgi * S4 : a->d_seg[sgi & 1] + (size_t)i * S4;
+    };
+    // the forward left the last segment's states and coefficients in place
+    const bool have_last = a->recorded_seg == nseg - 1;
     auto issue_recompute = [&](int sgi) -> int {
         const int b = sgi & 1;
         const int t0 = sgi * a->k, len = std::min(t0 + a->k, a->T) - t0;
         if (reversed_once[b]) HB_CUDA_RET(cudaStreamWaitEvent(rs, a->ev_reversed[b], 0));
-        HB_CUDA_RET(cudaMemcpyAsync(a->d_seg[b], a->d_ckpt + (size_t)sgi * S4, S4 * sizeof(double),
-                                    cudaMemcpyDeviceToDevice, rs));
         hb::adj::set_counter_kernel<<<1, 1, 0, rs>>>(h->d_ctr, t0);
         for (int i = 0; i < len; i++)
-            TRY(hb_forward_step_into(h, t0, i, a->d_seg[b] + (size_t)i * S4, a->d_seg[b] + (size_t)(i + 1) * S4,
-                                     a->d_terms, a->d_coef[b] + (size_t)i * hb::UPDATE_COEF * C, rs));
+            TRY(hb_forward_step_into(h, t0, i, seg_state(sgi, i), a->d_seg[b] + (size_t)(i + 1) * S4, a->d_terms,
+                                     a->d_coef[b] + (size_t)i * hb::UPDATE_COEF * C, 0, rs));
         HB_CUDA_RET(cudaEventRecord(a->ev_recomputed[b], rs));
         return HB_OK;
     };
-    TRY(issue_recompute(nseg - 1));
+    if (!have_last) TRY(issue_recompute(nseg - 1));
     for (int sgi = nseg - 1; sgi >= 0; sgi--) {
         const int b = sgi & 1;
         const int t0 = sgi * a->k, len = std::min(t0 + a->k, a->T) - t0;
         if (sgi > 0) TRY(issue_recompute(sgi - 1));
-        HB_CUDA_RET(cudaStreamWaitEvent(st, a->ev_recomputed[b], 0));
+        if (sgi != nseg - 1 || !have_last) HB_CUDA_RET(cudaStreamWaitEvent(st, a->ev_recomputed[b], 0));
         for (int i = len - 1; i >= 0; i--) {
             const int t = t0 + i;
             const hb::StepParams p = step_params(h, t);
@@ -1095,7 +1144,7 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
             const hb::adj::AdjStepBufs bufs{a->d_dir[w ^ 1], a->d_so[w ^ 1], a->d_sn[w ^ 1],
                                             a->d_dir[w], a->d_so[w], a->d_sn[w]};
             const int row = (t + 1 < a->T && (t + 1) % a->obs_every == 0) ? (t + 1) / a->obs_every - 1 : -1;
-            const double *xs = a->d_seg[b] + (size_t)i * S4, *xn = xs + S4;
+            const double *xs = seg_state(sgi, i), *xn = a->d_seg[b] + (size_t)(i + 1) * S4;
             const double *cf = a->d_coef[b] + (size_t)i * hb::UPDATE_COEF * C;
             HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::adj::adj_step_kernel, h->m64, am, bufs, xs, xn, cf, p,
                                            (int)(t == a->T - 1), row));
@@ -1110,6 +1159,7 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
     HB_CUDA_RET(cudaGetLastError());
     // leave the handle's counter where the forward left it
     hb::adj::set_counter_kernel<<<1, 1, 0, st>>>(h->d_ctr, a->T);
+    a->recorded_seg = -1;   // the segment buffers were reused
     HB_CUDA_RET(cudaStreamSynchronize(st));
     uint32_t bits = 0;
     HB_CUDA_RET(cudaMemcpy(&bits, h->d_err, sizeof bits, cudaMemcpyDeviceToHost));

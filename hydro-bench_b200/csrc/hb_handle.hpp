@@ -119,7 +119,7 @@ int hb_check_range(hb_handle *h, long long n);
 // One fp64 edge-layout step t0 + k (the device step counter must hold t0)
 // from state `in` to state `out` ([C][4] each), keeping the slots' terms of
 // the cell sums in `terms` ([4C][4]) and the update coefficients of the wet
-// cells in `coef` ([C][UPDATE_COEF]); the handle's W is overwritten, the
-// fluxes are not.
+// cells in `coef` ([C][UPDATE_COEF]); the handle's W is overwritten, its
+// fluxes only when `write_flux` is set.
 int hb_forward_step_into(hb_handle *h, long long t0, int k, const double *in, double *out, double *terms,
-                         double *coef, cudaStream_t st);
+                         double *coef, int write_flux, cudaStream_t st);

@@ -705,7 +705,7 @@ int hb_enqueue_steps(hb_handle *h, int n, cudaStream_t st) { return enqueue_step
 int hb_check_range(hb_handle *h, long long n) { return check_range(h, n); }
 
 int hb_forward_step_into(hb_handle *h, long long t0, int k, const double *in, double *out, double *terms,
-                         double *coef, cudaStream_t st) {
+                         double *coef, int write_flux, cudaStream_t st) {
     hb::DevMesh<hb::F64Exact> m = h->m64;
     const int par = (int)((t0 + k) & 1);
     m.S[par] = const_cast<double *>(in);
@@ -722,10 +722,10 @@ int hb_forward_step_into(hb_handle *h, long long t0, int k, const double *in, do
     cfg.numAttrs = 1;
     cfg.gridDim = dim3((unsigned)((m.nrecords + 127) / 128));
     cfg.blockDim = dim3(128);
-    HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::flux_kernel<hb::F64Exact, 0, 128, 6, false>, m, k, 0));
+    HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::flux_kernel<hb::F64Exact, 0, 128, 6, false>, m, k, write_flux));
     cfg.gridDim = dim3((unsigned)((m.C + hb::UPDATE_THREADS - 1) / hb::UPDATE_THREADS));
     cfg.blockDim = dim3(hb::UPDATE_THREADS);
-    HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::update_kernel<hb::F64Exact, 0, 6, false, true>, m, k, 0));
+    HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::update_kernel<hb::F64Exact, 0, 6, false, true>, m, k, write_flux));
     return HB_OK;
 }
 

@@ -9,6 +9,8 @@ against observations from a run with perturbed Manning coefficients.
     equal the complex-step reference's to 1e-8 (relative) and fourth-order
     central differences of the GPU rollout itself to 1e-6;
   * the gradient does not depend on the checkpoint interval (bit for bit);
+  * the handle holds the plain rollout's final state after the forward, and a
+    second backward gives the same gradient;
   * torch.autograd reaches the same gradient through GaugeLoss.
 """
 import numpy as np
@@ -94,6 +96,34 @@ def test_gradient_independent_of_checkpoint_interval(setup):
     for gn, gz in grads[1:]:
         np.testing.assert_array_equal(gn, grads[0][0])
         np.testing.assert_array_equal(gz, grads[0][1])
+
+
+def test_final_state_and_repeated_backward(setup):
+    """The forward steps its last segment into the segment buffers (outside
+    the k-step graph) and leaves the rollout's final state in the handle: the
+    same bits as a plain rollout of the handle from the same initial state,
+    whether that segment is the whole run (k = 40), a full segment after graph
+    replays (k = 10) or a remainder (k = 7).  A second backward without a new
+    forward recomputes that segment and gives the same gradient."""
+    s = setup
+    st = s["deck"].state()
+    hm1 = CS.ComplexDeck(s["deck"]).hm1
+    H0, U0, V0, Z0 = (np.real(x) for x in CS.initial_state(st["Z"], st["U"], st["V"], s["zbc"], hm1))
+    for k in (40, 10, 7):
+        a, _ = _adjoint(s, k)
+        a.forward()
+        after = a.solver.get_state()
+        g1 = a.backward()
+        g2 = a.backward()
+        np.testing.assert_array_equal(g1[0], g2[0])
+        np.testing.assert_array_equal(g1[1], g2[1])
+        a.solver.set_state(H0, U0, V0, Z0)
+        a.solver.set_position(0)
+        a.solver.step(NSTEPS)
+        plain = a.solver.get_state()
+        for f in "HUVZ":
+            np.testing.assert_array_equal(after[f], plain[f], err_msg=f"{f}, k = {k}")
+        a.close()
 
 
 def test_autograd_function(setup):
