@@ -757,9 +757,11 @@ struct hb_adjoint {
     double *d_sn[2] = {nullptr, nullptr};   // [4C][ADJ_REC] slots' contributions to their neighbours
     hb::adj::AdjMesh am{};
     cudaGraphExec_t fwd_graph = nullptr;    // k forward steps with checkpoint and gauge kernels
+    cudaGraphExec_t fwd_graph_multi = nullptr;   // 100 / k such segments
     bool forward_done = false;
     ~hb_adjoint() {
         if (fwd_graph) cudaGraphExecDestroy(fwd_graph);
+        if (fwd_graph_multi) cudaGraphExecDestroy(fwd_graph_multi);
         for (int q = 0; q < 2; q++) {
             if (ev_recomputed[q]) cudaEventDestroy(ev_recomputed[q]);
             if (ev_reversed[q]) cudaEventDestroy(ev_reversed[q]);
@@ -975,13 +977,14 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
     HB_CUDA_RET(cudaMemsetAsync(h->d_err, 0, sizeof(uint32_t), st));
     h->steps_done = 0;
     a->recorded_seg = -1;
-    // forward steps t0 .. t0+n-1: checkpoint at the segment's start, gauge
-    // depths after every step that ends on an observation (positions fixed
-    // when k is a multiple of obs_every, otherwise after every step)
+    // forward segments: checkpoint at each segment's start, gauge depths
+    // after every step that ends on an observation (positions fixed when k is
+    // a multiple of obs_every, otherwise after every step)
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
-    auto enqueue = [&](int t0, int n, cudaStream_t s) -> int {
+    // nsegs k-step segments from a step that is a multiple of k
+    auto enqueue = [&](int nsegs, cudaStream_t s) -> int {
         const double *S0 = h->m64.S[0], *S1 = h->m64.S[1];
         cudaLaunchConfig_t ck{};
         ck.gridDim = dim3(64);
@@ -992,41 +995,57 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
         cudaLaunchConfig_t gk = ck;
         gk.gridDim = dim3((unsigned)((a->ng + 127) / 128));
         gk.blockDim = dim3(128);
-        HB_CUDA_RET(cudaLaunchKernelEx(&ck, hb::adj::ckpt_kernel, S0, S1, a->d_ckpt, (const long long *)h->d_ctr, a->k,
-                                       S4));
-        // runs of steps up to each observation: one multi-step launch sequence each
-        for (int i = 0; i < n;) {
-            int m = n - i;
-            if (a->k % a->obs_every == 0) m = std::min(m, a->obs_every - (t0 + i) % a->obs_every);
-            else m = 1;
-            TRY(hb_enqueue_steps(h, m, s));
-            i += m;
-            HB_CUDA_RET(cudaLaunchKernelEx(&gk, hb::adj::gauge_ctr_kernel, S0, S1, (const int32_t *)a->d_gcell, a->ng,
-                                           a->d_gd, (const long long *)h->d_ctr, a->obs_every));
+        for (int q = 0; q < nsegs; q++) {
+            HB_CUDA_RET(cudaLaunchKernelEx(&ck, hb::adj::ckpt_kernel, S0, S1, a->d_ckpt, (const long long *)h->d_ctr,
+                                           a->k, S4));
+            // runs of steps up to each observation: one multi-step launch sequence each
+            for (int i = 0; i < a->k;) {
+                int m = a->k - i;
+                if (a->k % a->obs_every == 0) m = std::min(m, a->obs_every - i % a->obs_every);
+                else m = 1;
+                TRY(hb_enqueue_steps(h, m, s));
+                i += m;
+                HB_CUDA_RET(cudaLaunchKernelEx(&gk, hb::adj::gauge_ctr_kernel, S0, S1, (const int32_t *)a->d_gcell,
+                                               a->ng, a->d_gd, (const long long *)h->d_ctr, a->obs_every));
+            }
         }
         return HB_OK;
     };
-    // Segments 0 .. nseg-2 replay the k-step graph; the last one (k steps or
-    // the remainder) is stepped into the segment buffer with its update
-    // coefficients, as the backward pass would recompute it, so the backward
-    // starts reversing at once.
-    const int nseg = (a->T + a->k - 1) / a->k;
-    const int ngraph = nseg - 1;
-    if (ngraph > 0 && !a->fwd_graph) {
+    auto capture = [&](int nsegs, cudaGraphExec_t *exec) -> int {
         cudaStream_t cap;
         HB_CUDA_RET(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
         HB_CUDA_RET(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-        const int rc = enqueue(0, a->k, cap);
+        const int rc = enqueue(nsegs, cap);
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(cap, &g);
         cudaStreamDestroy(cap);
         if (rc != HB_OK) { if (g) cudaGraphDestroy(g); return rc; }
         if (e != cudaSuccess) return hb::set_error(HB_E_CUDA, "adjoint forward capture: %s", cudaGetErrorString(e));
-        const cudaError_t ei = cudaGraphInstantiate(&a->fwd_graph, g, 0);
+        const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
         cudaGraphDestroy(g);
-        if (ei != cudaSuccess) { a->fwd_graph = nullptr; return hb::set_error(HB_E_CUDA, "adjoint forward graph: %s", cudaGetErrorString(ei)); }
+        if (ei != cudaSuccess) {
+            *exec = nullptr;
+            return hb::set_error(HB_E_CUDA, "adjoint forward graph: %s", cudaGetErrorString(ei));
+        }
+        return HB_OK;
+    };
+    // Segments 0 .. nseg-2 replay captured graphs: one of G = 100 / k
+    // segments (about 100 steps) where it fits, one segment otherwise.  The
+    // last segment (k steps or the remainder) is stepped into the segment
+    // buffer with its update coefficients, as the backward pass would
+    // recompute it, so the backward starts reversing at once.
+    const int nseg = (a->T + a->k - 1) / a->k;
+    const int ngraph = nseg - 1;
+    const int G = std::max(1, 100 / a->k);
+    int done = 0;
+    if (G > 1 && ngraph >= G) {
+        if (!a->fwd_graph_multi) TRY(capture(G, &a->fwd_graph_multi));
+        for (; done + G <= ngraph; done += G) HB_CUDA_RET(cudaGraphLaunch(a->fwd_graph_multi, st));
     }
-    for (int sgi = 0; sgi < ngraph; sgi++) HB_CUDA_RET(cudaGraphLaunch(a->fwd_graph, st));
+    if (done < ngraph) {
+        if (!a->fwd_graph) TRY(capture(1, &a->fwd_graph));
+        for (; done < ngraph; done++) HB_CUDA_RET(cudaGraphLaunch(a->fwd_graph, st));
+    }
     {
         const int sgi = nseg - 1, t0 = sgi * a->k, len = a->T - t0, b = sgi & 1;
         cudaLaunchConfig_t ck{};

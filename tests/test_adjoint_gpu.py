@@ -98,6 +98,33 @@ def test_gradient_independent_of_checkpoint_interval(setup):
         np.testing.assert_array_equal(gz, grads[0][1])
 
 
+def test_multi_segment_graphs(tmp_path):
+    """120 steps: with k = 10 the forward replays one captured graph of ten
+    segments and one of a single segment, with k = 7 one of fourteen segments
+    and three single ones, with k = 60 single segments only.  The loss, the
+    gradient and the final state agree bit for bit."""
+    root = str(tmp_path / "deck")
+    D.write_deck(D.config_f1(steps=130), root)
+    deck = hb.Deck(root)
+    gauges = np.random.default_rng(3).choice(deck.cells, 8, replace=False)
+    out = []
+    for k in (10, 7, 60):
+        a = Adjoint(deck, gauges, OBS_EVERY, 120, checkpoint_every=k)
+        _, obs = a.forward()
+        a.set_observations(obs + 0.01)
+        L, _ = a.forward()
+        gn, gz = a.backward()
+        out.append((L, gn, gz, a.solver.get_state()))
+        a.close()
+    L0, gn0, gz0, st0 = out[0]
+    for L, gn, gz, st in out[1:]:
+        assert L == L0
+        np.testing.assert_array_equal(gn, gn0)
+        np.testing.assert_array_equal(gz, gz0)
+        for f in "HUVZ":
+            np.testing.assert_array_equal(st[f], st0[f])
+
+
 def test_final_state_and_repeated_backward(setup):
     """The forward steps its last segment into the segment buffers (outside
     the k-step graph) and leaves the rollout's final state in the handle: the
