@@ -56,6 +56,8 @@ struct hb_handle {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_steps = 0;
     int launch_config = 0;           // index into LAUNCH_CONFIGS
+    struct HaloList { int32_t *cells; int32_t n; };
+    std::vector<HaloList> halo_lists;   // hb_halo_define: device cell indices (memory in allocs)
     bool segmented() const { return scn.size() > 1; }
     long long step_limit() const {
         long long l = LLONG_MAX;

@@ -21,11 +21,13 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <numeric>
 #include <queue>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "hb_common.cuh"
@@ -1287,3 +1289,87 @@ extern "C" int hb_checkpoint_load(hb_handle *h, const void *buffer, size_t bytes
     return HB_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// halo exchange of a mesh split across handles
+// ---------------------------------------------------------------------------
+namespace {
+
+// buf[i] = the state record of cell cells[i] (pack) or the reverse (unpack);
+// a record is the four state components of one cell.
+template <class R>
+__global__ void halo_pack_kernel(const R *__restrict__ S, const int32_t *__restrict__ cells, int n,
+                                 R *__restrict__ buf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const hb::Vec4<R> v = hb::ld4(S + 4 * (size_t)cells[i]);
+    hb::st4(buf + 4 * (size_t)i, v.x, v.y, v.z, v.w);
+}
+template <class R>
+__global__ void halo_unpack_kernel(R *__restrict__ S, const int32_t *__restrict__ cells, int n,
+                                   const R *__restrict__ buf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const hb::Vec4<R> v = hb::ld4(buf + 4 * (size_t)i);
+    hb::st4(S + 4 * (size_t)cells[i], v.x, v.y, v.z, v.w);
+}
+
+int halo_args(hb_handle *h, int32_t list, const void *buf, const char *who) {
+    if (!h || !buf) return hb::set_error(HB_E_INVALID, "%s: null argument", who);
+    if (list < 0 || list >= (int32_t)h->halo_lists.size())
+        return hb::set_error(HB_E_INVALID, "%s: no halo list %d", who, list);
+    if ((uintptr_t)buf % 16 != 0) return hb::set_error(HB_E_INVALID, "%s: buffer not 16-byte aligned", who);
+    return HB_OK;
+}
+
+}  // namespace
+
+extern "C" int hb_state_record_bytes(const hb_handle *h, int32_t *bytes) {
+    if (!h || !bytes) return hb::set_error(HB_E_INVALID, "null argument");
+    *bytes = h->opt.precision == HB_FP64 ? 32 : 16;
+    return HB_OK;
+}
+
+extern "C" int hb_halo_define(hb_handle *h, const int32_t *cells, int32_t n, int32_t *list) {
+    if (!h || !list || n < 0 || (n > 0 && !cells)) return hb::set_error(HB_E_INVALID, "hb_halo_define: bad argument");
+    if (h->segmented()) return hb::set_error(HB_E_INVALID, "hb_halo_define: a batch handle has no single mesh to split");
+    const hb::Scenario &sc = h->scn[0];
+    std::vector<int32_t> dev(std::max(n, 1), 0);
+    for (int32_t i = 0; i < n; i++) {
+        if (cells[i] < 0 || cells[i] >= sc.cells)
+            return hb::set_error(HB_E_INVALID, "hb_halo_define: cell %d outside 0..%d", cells[i], sc.cells - 1);
+        dev[i] = sc.cell0 + sc.inv[cells[i]];
+    }
+    int32_t *d = nullptr;
+    TRY(dev_upload(h, &d, dev));
+    h->halo_lists.push_back({d, n});
+    *list = (int32_t)h->halo_lists.size() - 1;
+    return HB_OK;
+}
+
+extern "C" int hb_halo_pack(hb_handle *h, int32_t list, void *buf, void *stream) {
+    TRY(halo_args(h, list, buf, "hb_halo_pack"));
+    const auto L = h->halo_lists[list];
+    if (L.n == 0) return HB_OK;
+    const int par = (int)(h->steps_done & 1);
+    return h->with_mesh([&](auto &m) -> int {
+        using R = std::remove_pointer_t<std::decay_t<decltype(m.S[0])>>;
+        halo_pack_kernel<R><<<(L.n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(m.S[par], L.cells, L.n, (R *)buf);
+        HB_CUDA_RET(cudaGetLastError());
+        return HB_OK;
+    });
+}
+
+extern "C" int hb_halo_unpack(hb_handle *h, int32_t list, const void *buf, void *stream) {
+    TRY(halo_args(h, list, buf, "hb_halo_unpack"));
+    const auto L = h->halo_lists[list];
+    if (L.n == 0) return HB_OK;
+    const int par = (int)(h->steps_done & 1);
+    return h->with_mesh([&](auto &m) -> int {
+        using R = std::remove_pointer_t<std::decay_t<decltype(m.S[0])>>;
+        halo_unpack_kernel<R><<<(L.n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(m.S[par], L.cells, L.n,
+                                                                                     (const R *)buf);
+        HB_CUDA_RET(cudaGetLastError());
+        return HB_OK;
+    });
+}

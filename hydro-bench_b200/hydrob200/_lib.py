@@ -129,6 +129,10 @@ def lib():
         "hb_checkpoint_size": (C.c_int, [vp, C.POINTER(C.c_size_t)]),
         "hb_checkpoint_save": (C.c_int, [vp, C.c_void_p, C.c_size_t]),
         "hb_checkpoint_load": (C.c_int, [vp, C.c_void_p, C.c_size_t]),
+        "hb_state_record_bytes": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+        "hb_halo_define": (C.c_int, [vp, _ip, C.c_int32, C.POINTER(C.c_int32)]),
+        "hb_halo_pack": (C.c_int, [vp, C.c_int32, C.c_void_p, vp]),
+        "hb_halo_unpack": (C.c_int, [vp, C.c_int32, C.c_void_p, vp]),
         "hb_write_dump": (C.c_int, [vp, C.c_int32, C.POINTER(MeshDesc), C.c_char_p]),
         "hb_adjoint_create": (C.c_int, [vp, _ip, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(vp)]),
         "hb_adjoint_destroy": (C.c_int, [vp]),
@@ -163,4 +167,5 @@ EXPORTED = ["hb_options_default", "hb_tile_configs", "hb_launch_shapes", "hb_cre
             "hb_get_flux_at", "hb_get_klas_at", "hb_get_permutation_at", "hb_set_tile_config", "hb_get_tile_config",
             "hb_autotune", "hb_checkpoint_size", "hb_checkpoint_save", "hb_checkpoint_load", "hb_write_dump", "hb_output_open", "hb_output_frame", "hb_output_close",
             "hb_deck_ntoutput", "hb_adjoint_create", "hb_adjoint_destroy", "hb_adjoint_set_parameters",
-            "hb_adjoint_set_initial", "hb_adjoint_set_observations", "hb_adjoint_forward", "hb_adjoint_backward"]
+            "hb_adjoint_set_initial", "hb_adjoint_set_observations", "hb_adjoint_forward", "hb_adjoint_backward",
+            "hb_state_record_bytes", "hb_halo_define", "hb_halo_pack", "hb_halo_unpack"]

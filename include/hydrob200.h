@@ -182,6 +182,21 @@ int hb_write_dump(hb_handle *h, int32_t s, const hb_mesh_desc *mesh, const char 
 int hb_checkpoint_size(hb_handle *h, size_t *bytes);
 int hb_checkpoint_save(hb_handle *h, void *buffer, size_t bytes);
 int hb_checkpoint_load(hb_handle *h, const void *buffer, size_t bytes);
+
+/* Halo exchange (no reference counterpart; the reference steps one mesh on
+ * one GPU).  A mesh too large for one GPU is split into parts, each stepped
+ * by its own handle over its cells plus a one-ring halo of its neighbours'
+ * cells; after every step each halo cell takes the state its owner computed.
+ * hb_halo_define registers a list of this handle's cells (reference order,
+ * host memory) and returns its id.  hb_halo_pack copies the current state
+ * record of every cell of a list, in list order, into `buf`; hb_halo_unpack
+ * writes such records into the current state.  `buf` is device memory,
+ * 16-byte aligned, of n * hb_state_record_bytes bytes; both calls are ordered
+ * on `stream` after the handle's steps.  Single-mesh handles only. */
+int hb_state_record_bytes(const hb_handle *h, int32_t *bytes);
+int hb_halo_define(hb_handle *h, const int32_t *cells, int32_t n, int32_t *list);
+int hb_halo_pack(hb_handle *h, int32_t list, void *buf, void *stream);
+int hb_halo_unpack(hb_handle *h, int32_t list, const void *buf, void *stream);
 /* Sticky device error word (bit set of hb_status codes seen by kernels). */
 int hb_device_errors(hb_handle *h, uint32_t *bits);
 
