@@ -6,12 +6,13 @@ kernels of the edge layout, chained by programmatic dependent launch),
 replayed from a captured CUDA graph.  Prints ONE JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--extras all|none|ensemble|adjoint|split]
+                    [--extras all|none|ensemble|adjoint|split|fp32|dambreak]
 
-On one GPU the line also carries the three additions, each with its error
+On one GPU the line also carries these additions, each with its error
 against fp64 (``--extras`` chooses which; ``--only-extras`` skips the main
 measurement, for profiling one of them):
   split_207k  split precision, tile layout, on the same 207K mesh;
+  fp32_207k   plain fp32 (the reference's fp32 tree), tile layout, same mesh;
   ensemble    64 independent channel scenarios in one launch per step
               (fp64 edge layout vs split precision tile layout, autotuned),
               1000 steps each, with the split form's depth error;
@@ -19,7 +20,10 @@ measurement, for profiling one of them):
               1000 steps for checkpoint intervals 10, 50, 100: its time over
               the plain forward's;
   dambreak    2,000,000-cell dam break on a fractal bed, 2000 steps: split
-              precision against fp64 every 100 steps, and both speeds.
+              precision and fp32 against fp64 every 100 steps, and the speeds
+              of all three (HBM-bound: the working set is several L2s).
+Each reduced-precision and dam-break speed carries its algorithmic GB/s and
+the fraction of the measured copy bandwidth.
 
 Multi-GPU: one process per GPU (torchrun); each rank runs its own replica of
 the scenario (the path has no exchange step between independent meshes), the
@@ -102,6 +106,23 @@ def alg_bytes_per_cell_step(cells: int, edges: int, w: int) -> float:
     per-cell constants (AREA, ZBC, FNC); per unique edge two int32 cell ids,
     a 1-byte code and SIDE, COSF, SINF."""
     return 12 * w + (edges / cells) * (8 + 1 + 3 * w)
+
+
+def alg_bytes_for(precision: str, cells: int, edges: int) -> float:
+    """alg_bytes_per_cell_step for a precision: fp64 with w = 8, fp32 with
+    w = 4, split = fp32 plus the fp32 depth compensation term in and out."""
+    if precision == "fp64":
+        return alg_bytes_per_cell_step(cells, edges, 8)
+    return alg_bytes_per_cell_step(cells, edges, 4) + (8 if precision == "split" else 0)
+
+
+def hbm_point(precision: str, cells: int, edges: int, us: float) -> dict:
+    """Algorithmic GB/s of a step time and its fraction of the measured copy bandwidth."""
+    b = alg_bytes_for(precision, cells, edges)
+    peak, kind = load_peaks()
+    gbs = b * cells / (us * 1e-6) / 1e9
+    return {"alg_bytes_per_cell_step": b, "hbm_gbs_alg": gbs, "frac": gbs / peak, "peak": peak,
+            "peak_source": f"{kind} hbm_gbs"}
 
 
 class ClockSampler:
@@ -368,15 +389,18 @@ def adjoint_leg(local, steps=1000, ks=(10, 50, 100)):
     return out
 
 
-def split_leg(deck, local, steps=900):
+def split_leg(deck, local, steps=900, precision="split"):
+    """The reduced-precision step on the 207K mesh (tile layout, autotuned):
+    time from 100-step graph replays, and its depths after `steps` steps
+    against the fp64 step's."""
     import torch
     import hydrob200 as hb
     from hydrob200.accuracy import depth_error
-    sp = hb.Solver(deck, precision="split", layout="tile", tile_cells=512, device=local)
+    sp = hb.Solver(deck, precision=precision, layout="tile", tile_cells=512, device=local)
     best, _ = sp.autotune(steps=10)
     us = _time_graph(sp, steps, 100, torch)
     sp.close()
-    a, b = hb.Solver(deck, device=local), hb.Solver(deck, precision="split", layout="tile", tile_cells=512,
+    a, b = hb.Solver(deck, device=local), hb.Solver(deck, precision=precision, layout="tile", tile_cells=512,
                                                      device=local)
     a.step(steps)
     b.step(steps)
@@ -384,7 +408,8 @@ def split_leg(deck, local, steps=900):
     b.sync()
     e = depth_error(b.get_state()["H"], a.get_state()["H"], deck.mesh.hm2, deck.array("area"))
     return {"us_per_step": us, "value": deck.cells / (us * 1e-6), "unit": METRIC, "layout": "tile",
-            "tile_cells": 512, "tile_config": best, "error_vs_fp64": dict(e, after_steps=steps)}
+            "tile_cells": 512, "tile_config": best, "error_vs_fp64": dict(e, after_steps=steps),
+            "roofline": hbm_point(precision, deck.cells, unique_edges(deck), us)}
 
 
 
@@ -451,8 +476,11 @@ def dambreak_leg(local, steps=2000, every=100, ncells=2_000_000):
     out["error_vs_fp64"] = rows["split"]
     out["fp32_error_vs_fp64"] = rows["fp32"]
     n = every * (steps // every)
+    edges = unique_edges(deck)
     for name in runs:
         out[f"{name}_us_per_step"] = times[name] * 1e3 / n
+        # the mesh's working set is several times the L2: these are HBM-bound points
+        out[f"{name}_roofline"] = hbm_point(name, C, edges, out[f"{name}_us_per_step"])
     out["split_vs_fp64"] = times["fp64"] / times["split"]
     out["value_split"] = C / (out["split_us_per_step"] * 1e-6)
     out["unit"] = METRIC
@@ -471,7 +499,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--extras", default="all", choices=["all", "none", "ensemble", "adjoint", "split", "dambreak"])
+    ap.add_argument("--extras", default="all",
+                    choices=["all", "none", "ensemble", "adjoint", "split", "fp32", "dambreak"])
     ap.add_argument("--only-extras", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=1000)
     ap.add_argument("--ensemble-steps", type=int, default=1000)
@@ -509,7 +538,7 @@ def main():
     b_alg = alg_bytes_per_cell_step(C, edges, w)
 
     if args.only_extras:   # one or more of the additions alone (profiling); not a bench line
-        legs = {"split": lambda: split_leg(deck, local),
+        legs = {"split": lambda: split_leg(deck, local), "fp32": lambda: split_leg(deck, local, precision="fp32"),
                 "ensemble": lambda: ensemble_leg(local, args.ensemble_steps, rank=rank, world=world),
                 "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
                 "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells)}
@@ -619,13 +648,14 @@ def main():
 
     extras = {}
     if world == 1 and rank == 0 and args.extras != "none":
-        legs = {"split": lambda: split_leg(deck, local), "ensemble": lambda: ensemble_leg(local, args.ensemble_steps),
+        legs = {"split": lambda: split_leg(deck, local), "fp32": lambda: split_leg(deck, local, precision="fp32"),
+                "ensemble": lambda: ensemble_leg(local, args.ensemble_steps),
                 "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
                 "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells)}
         for name, fn in legs.items():
             if args.extras in ("all", name):
                 try:
-                    extras[name if name != "split" else "split_207k"] = fn()
+                    extras[{"split": "split_207k", "fp32": "fp32_207k"}.get(name, name)] = fn()
                 except Exception as ex:   # the bench line still prints
                     extras[name] = {"error": f"{type(ex).__name__}: {ex}"[:300]}
     elif world > 1 and args.extras in ("all", "ensemble"):
