@@ -369,9 +369,11 @@ __device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const Ste
     else st.z = raw.w;
     const unsigned mask = m.cmask[c];
     const R fnc = m.fnc[c], dta = m.dta[c], sidex = VARIANT == 1 ? m.sidex[c] : R(0);
+    // only the real slots' terms are read (a triangle's zero-length fourth
+    // slot is evaluated below and has none)
     Vec4<R> t[4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) t[j] = ld4(terms + 4 * j);
+    for (int j = 0; j < 4; j++) t[j] = (mask & (1u << j)) ? ld4(terms + 4 * j) : Vec4<R>{R(0), R(0), R(0), R(0)};
     R wh = R(0), wu = R(0), wv = R(0);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
