@@ -155,21 +155,26 @@ __device__ __forceinline__ CellStateA<A> load_cell(const DevMesh<A> &m, int par,
 // Where a step keeps the slots' terms of the cell sums between the flux and
 // the update: slot s at p + 4 * (s - slot0).  Global memory (m.slotw, slot0 =
 // 0) between the two kernels of the edge layout; shared memory (slot0 = the
-// tile's first slot) inside the tile kernel.
-template <class R>
-struct Terms { R *p; int slot0; };
+// tile's first slot) inside the tile kernel (SMEM).
+template <class R, bool SMEM = false>
+struct Terms {
+    R *p;
+    int slot0;
+    static constexpr bool smem = SMEM;
+};
 
 // the slot's terms of the cell sums (functors.cu:733-741): F0 and SIDE for
 // WH = fma(SIDE, F0, WH), and the complete WU / WV increments
-template <class A>
-__device__ __forceinline__ void store_terms(const Terms<typename A::real> &t, int s, const typename A::real f[4],
+template <class A, class T>
+__device__ __forceinline__ void store_terms(const T &t, int s, const typename A::real f[4],
                                             typename A::real side, typename A::real cs, typename A::real sn) {
     using R = typename A::real;
     const R fr1 = A::add(f[1], f[3]);
     const R slcos = A::mul(side, cs), slsin = A::mul(side, sn);
     const R dwu = A::dot(slcos, fr1, -slsin, f[2], M_WU);
     const R dwv = A::dot(slsin, fr1, slcos, f[2], M_WV);
-    st4(t.p + 4 * (size_t)(s - t.slot0), f[0], dwu, dwv, side);
+    if constexpr (T::smem) st4(t.p + 4 * (size_t)(s - t.slot0), f[0], dwu, dwv, side);
+    else stg4(t.p + 4 * (size_t)(s - t.slot0), f[0], dwu, dwv, side);
 }
 
 template <class A>
@@ -178,9 +183,9 @@ __device__ __forceinline__ void store_flux(const DevMesh<A> &m, int s, const typ
 }
 
 // One slot on its own: flux_slot with its boundary tables (functors.cu:47-202).
-template <class A, int VARIANT>
+template <class A, int VARIANT, class T>
 __device__ __forceinline__ void single_record(const DevMesh<A> &m, int r, const StepIndex &si,
-                                              const StepParams &p, int write_flux, const Terms<typename A::real> &tout) {
+                                              const StepParams &p, int write_flux, const T &tout) {
     using R = typename A::real;
     const int4 ix = m.rix[r];
     const int a = ix.x, b = ix.y, sa = ix.z;
@@ -226,9 +231,9 @@ __device__ __forceinline__ void single_record(const DevMesh<A> &m, int r, const 
 
 // The mirrored Osher of a pair computed on its own (when its inputs differ
 // from the direct route's in the normal velocity).
-template <class A>
+template <class A, class T>
 __device__ __forceinline__ void pair_mirror(const DevMesh<A> &m, int r, const StepIndex &si,
-                                            const StepParams &p, int write_flux, const Terms<typename A::real> &tout) {
+                                            const StepParams &p, int write_flux, const T &tout) {
     using R = typename A::real;
     const int4 ix = m.rix[r];
     const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
@@ -260,9 +265,9 @@ __device__ __forceinline__ bool same_bits(R a, R b) {
 // the b side's FLUX2 is re-summed with its own tangent if only that differs;
 // otherwise the pair goes to the CTA's queue, whose mirrored Osher
 // evaluations run together after the main pass (pair_mirror).
-template <class A, int VARIANT>
+template <class A, int VARIANT, class T>
 __device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const StepIndex &si, const StepParams &p,
-                                            int write_flux, const Terms<typename A::real> &tout, int *queue, int *qn) {
+                                            int write_flux, const T &tout, int *queue, int *qn) {
     using R = typename A::real;
     const int4 ix = m.rix[r];
     const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
@@ -479,7 +484,7 @@ __global__ void __launch_bounds__(THREADS, MINB) tile_kernel(DevMesh<A> m, int k
     cudaTriggerProgrammaticLaunchCompletion();
     const StepIndex si = step_index(m, k, sp.per_day, sp.ndays);
     const StepParams p{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
-    const Terms<R> tout{terms, 4 * td.cell0};
+    const Terms<R, true> tout{terms, 4 * td.cell0};
     __syncthreads();
     const int nrec = td.npairs + td.nsingles;
     for (int i = threadIdx.x; i < nrec; i += THREADS) {
