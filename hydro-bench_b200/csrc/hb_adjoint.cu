@@ -46,7 +46,9 @@ using A = F64Exact;
 struct Adj5 { double h, u, v, z, b; };
 
 // A slot's Adj5 contribution in memory: six doubles (the last one padding),
-// moved as three aligned 16-byte accesses.
+// moved as three aligned 16-byte accesses.  (Eight doubles moved as two
+// 256-bit accesses measured slower: the extra bytes cost more than the
+// saved instruction.)
 constexpr int ADJ_REC = 6;
 __device__ __forceinline__ void ld_rec(const double *p, double q[5]) {
     const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
@@ -500,7 +502,8 @@ __device__ __forceinline__ void gather4(const AdjMesh &a, const double *dir, con
         part[q] += __shfl_xor_sync(0xffffffffu, part[q], 1);
         part[q] += __shfl_xor_sync(0xffffffffu, part[q], 2);
     }
-    for (int q = 0; q < 4; q++) l[q] = dir[4 * (size_t)c + q] + part[q];
+    const Vec4<double> d = ldg4(dir + 4 * (size_t)c);
+    l[0] = d.x + part[0]; l[1] = d.y + part[1]; l[2] = d.z + part[2]; l[3] = d.w + part[3];
     zg = part[4];
     if (obs_row >= 0) {
         const int g = a.gauge_of[c];
@@ -512,9 +515,8 @@ __device__ __forceinline__ void gather4(const AdjMesh &a, const double *dir, con
 // recomputed step's update kernel) for the reverse of the cell update.
 struct UpdateCoef { double dtw, ih2, d_fnc, d_h, d_s; };
 __device__ __forceinline__ UpdateCoef ld_coef(const double *p) {
-    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
-    const double2 c = reinterpret_cast<const double2 *>(p)[2];
-    return {a.x, a.y, b.x, b.y, c.x};
+    const Vec4<double> a = ldg4(p), b = ldg4(p + 4);
+    return {a.x, a.y, a.z, a.w, b.x};
 }
 
 // One reverse step t, four lanes per cell.  x: the state before the step; xn:
@@ -551,7 +553,7 @@ __global__ void __launch_bounds__(128, 7) adj_step_kernel(DevMesh<A> m, AdjMesh 
     } else {
         gather4(a, b.dir_in, b.so_in, b.sn_in, c, j, obs_row, l, zg);
     }
-    const Vec4<double> xc = ld4(x + 4 * (size_t)c);
+    const Vec4<double> xc = ldg4(x + 4 * (size_t)c);
     const double hv = xc.x, uv = xc.y, vv = xc.z;
     const double zbc = m.zbc[c];
     double whb = 0.0, wub = 0.0, wvb = 0.0;
@@ -559,7 +561,7 @@ __global__ void __launch_bounds__(128, 7) adj_step_kernel(DevMesh<A> m, AdjMesh 
         // ---- the update (UpdateCellKernel, functors.cu:717-784, variant H): forward values, then its reverse
         const double HM1 = p.hm1, HM2 = p.hm2;
         const double dta = m.dta[c];
-        const Vec4<double> xn4 = ld4(xn + 4 * (size_t)c);
+        const Vec4<double> xn4 = ldg4(xn + 4 * (size_t)c);
         const double h2 = xn4.x, u2 = xn4.y, v2 = xn4.z;
         double h2b = l[0] + l[3];   // Z2 = H2 + ZBC
         double hb = 0.0, ub = 0.0, vb = 0.0, fncb = 0.0;
@@ -585,8 +587,7 @@ __global__ void __launch_bounds__(128, 7) adj_step_kernel(DevMesh<A> m, AdjMesh 
         }
         if (h2 > HM1) { hb += h2b; whb -= h2b * dta; }
         if (valid) {
-            double *d = b.dir_out + 4 * (size_t)c;
-            d[0] = hb; d[1] = ub; d[2] = vb; d[3] = 0.0;
+            stg4(b.dir_out + 4 * (size_t)c, hb, ub, vb, 0.0);
             a.fnc_g[c] += fncb;
             a.zbc_g[c] += l[3] + zg;
         }
@@ -618,7 +619,7 @@ __global__ void __launch_bounds__(128, 7) adj_step_kernel(DevMesh<A> m, AdjMesh 
     in.has_nb = meta & META_HAS_NB;
     const int nb = a.nbr4[s];
     if (in.has_nb) {
-        const Vec4<double> xn4 = ld4(x + 4 * (size_t)nb);
+        const Vec4<double> xn4 = ldg4(x + 4 * (size_t)nb);
         in.nb = CellStateA<A>{xn4.x, xn4.y, xn4.z, xn4.w, m.zbc[nb]};
     }
     else

@@ -832,9 +832,14 @@ __device__ __forceinline__ void wsum_add(typename A::real &wh, typename A::real 
 
 // Coefficients of a wet cell's velocity update for the reverse sweep (COEF):
 // U2 = (H U - DTA WU - DTW U) / H2, DTW = DT FNC S / H^0.33333, S = |(U, V)|
-// (functors.cu:766-772).  Six doubles per cell:
-//   {DTW, 1/H2, dDTW/dFNC, dDTW/dH, (dDTW/dS)/S (0 when S = 0), 0}.
-constexpr int UPDATE_COEF = 6;
+// (functors.cu:766-772).  Eight doubles per cell (two 32-byte halves):
+//   {DTW, 1/H2, dDTW/dFNC, dDTW/dH, (dDTW/dS)/S (0 when S = 0), 0, 0, 0}.
+constexpr int UPDATE_COEF = 8;
+
+// One 256-bit store of four doubles to global memory (32-byte aligned).
+__device__ __forceinline__ void st_global_f64x4(double *p, double x, double y, double z, double w) {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" :: "l"(p), "d"(x), "d"(y), "d"(z), "d"(w) : "memory");
+}
 
 // COEF: also write the cell's update coefficients to `coef` when the cell is
 // wet after the step (H2 > HM2; fp64 only).
@@ -889,10 +894,8 @@ update_cell(const CellUpdateIn<typename A::real, typename A::level> &c, typename
         if constexpr (COEF) {
             static_assert(std::is_same<R, double>::value, "update coefficients are fp64");
             const double ihp = 1.0 / hp;
-            double2 *q = reinterpret_cast<double2 *>(coef);
-            q[0] = make_double2(dtw, 1.0 / o.h);
-            q[1] = make_double2(DT * sq * ihp, DT * c.fnc * sq * (-0.33333) * ihp / c.h);
-            q[2] = make_double2(sq > 0.0 ? DT * c.fnc * ihp / sq : 0.0, 0.0);
+            st_global_f64x4(coef, dtw, 1.0 / o.h, DT * sq * ihp, DT * c.fnc * sq * (-0.33333) * ihp / c.h);
+            st_global_f64x4(coef + 4, sq > 0.0 ? DT * c.fnc * ihp / sq : 0.0, 0.0, 0.0, 0.0);
         }
     }
     o.w = A::sqrt(A::dot(o.u, o.u, o.v, o.v, M_SQ2));

@@ -140,7 +140,7 @@ __device__ __forceinline__ Vec4<double> ldg4(const double *p) {
 }
 __device__ __forceinline__ Vec4<float> ldg4(const float *p) { return ld4(p); }
 __device__ __forceinline__ void stg4(double *p, double x, double y, double z, double w) {
-    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" :: "l"(p), "d"(x), "d"(y), "d"(z), "d"(w) : "memory");
+    st_global_f64x4(p, x, y, z, w);
 }
 __device__ __forceinline__ void stg4(float *p, float x, float y, float z, float w) { st4(p, x, y, z, w); }
 
