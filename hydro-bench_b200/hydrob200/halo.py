@@ -21,7 +21,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
-from typing import Callable, Dict, List, Optional, Sequence
+from typing import Callable, Dict, List, Optional
 
 import numpy as np
 
