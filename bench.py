@@ -6,7 +6,7 @@ kernels of the edge layout, chained by programmatic dependent launch),
 replayed from a captured CUDA graph.  Prints ONE JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--extras all|none|ensemble|adjoint|split|fp32|dambreak]
+                    [--extras all|none|ensemble|adjoint|split|fp32|dambreak|halo]
 
 On one GPU the line also carries these additions, each with its error
 against fp64 (``--extras`` chooses which; ``--only-extras`` skips the main
@@ -19,6 +19,9 @@ measurement, for profiling one of them):
   adjoint     gradient of the gauge loss on the 24,020-cell channel over
               1000 steps for checkpoint intervals 10, 50, 100: its time over
               the plain forward's;
+  halo        the dam-break mesh split into 2 and 4 parts with a halo exchanged
+              after every step, against the whole mesh (on several GPUs, with
+              --extras halo: one part per GPU over NCCL);
   dambreak    2,000,000-cell dam break on a fractal bed, 2000 steps: split
               precision and fp32 against fp64 every 100 steps, and the speeds
               of all three (HBM-bound: the working set is several L2s).
@@ -413,6 +416,77 @@ def split_leg(deck, local, steps=900, precision="split"):
 
 
 
+def _dambreak_root(ncells: int, steps: int) -> str:
+    from hydrob200 import deck as D
+    root = os.path.join(tempfile.gettempdir(), f"hb_dambreak_{ncells}_{steps}")
+    if not os.path.exists(os.path.join(root, "BINFOR", "TIME.DAT")):
+        tmp = root + f".tmp{os.getpid()}"
+        D.write_deck(D.dam_break_deck(ncells=ncells, steps=steps), tmp)
+        shutil.rmtree(root, ignore_errors=True)
+        os.replace(tmp, root)
+    return root
+
+
+def halo_leg(local, ncells=2_000_000, steps=200, parts=(2, 4), rank=0, world=1):
+    """The dam-break mesh split into parts with a one-ring halo exchanged after
+    every step (hydrob200.halo), against the whole mesh on one handle, both
+    stepped one step per call (no graphs; each call also writes the step's
+    FLUX0..3, which the API keeps after every call), fp64.  One process: every part on
+    this GPU (the cost of splitting and exchanging).  Several ranks: one part
+    per rank, NCCL between them, time = max over ranks.  The gathered state
+    is compared with the whole mesh's bit for bit."""
+    import numpy as np
+    import torch
+    import hydrob200 as hb
+    from hydrob200 import halo
+    root = _dambreak_root(ncells, 2000)
+    deck = hb.Deck(root)
+    st = torch.cuda.current_stream()
+
+    def timed(fn):
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms * 1e3 / steps
+
+    out = {"cells": deck.cells, "steps": steps, "precision": "fp64", "ranks": world,
+           "partition": "reverse Cuthill-McKee order cut into equal contiguous ranges"}
+    whole = None
+    if rank == 0:
+        whole = hb.Solver(deck, device=local)
+        if world == 1:
+            out["whole_us_per_step"] = timed(lambda: [whole.step(1, st) for _ in range(steps)])
+        else:
+            whole.step(steps, st)   # the reference for the comparison only
+        ref = whole.get_state()
+    for n in ((world,) if world > 1 else parts):
+        run = halo.split_deck(deck, n, rank=rank if world > 1 else 0, world=world, device=local)
+        us = timed(lambda: run.step(steps))
+        got = run.gather()
+        entry = {"us_per_step": us, "value": deck.cells / (us * 1e-6), "unit": METRIC,
+                 "halo_cells": int(sum(len(p.halo) for p in run.parts)),
+                 "owned_max": int(max(len(p.owned) for p in run.parts))}
+        if rank == 0:
+            entry["bit_identical_to_whole"] = bool(all(np.array_equal(got[k], ref[k]) for k in "HUVZ"))
+        out[f"parts_{n}"] = entry
+        run.close()
+    if whole is not None:
+        whole.close()
+    return out if rank == 0 else None
+
+
 def dambreak_leg(local, steps=2000, every=100, ncells=2_000_000):
     """The wetting/drying configuration: split precision (tile layout) and
     fp64 (edge layout) stepped side by side, depths compared every `every`
@@ -421,14 +495,8 @@ def dambreak_leg(local, steps=2000, every=100, ncells=2_000_000):
     import numpy as np
     import torch
     import hydrob200 as hb
-    from hydrob200 import deck as D
     from hydrob200.accuracy import depth_error
-    root = os.path.join(tempfile.gettempdir(), f"hb_dambreak_{ncells}_{steps}")
-    if not os.path.exists(os.path.join(root, "BINFOR", "TIME.DAT")):
-        tmp = root + f".tmp{os.getpid()}"
-        D.write_deck(D.dam_break_deck(ncells=ncells, steps=steps), tmp)
-        shutil.rmtree(root, ignore_errors=True)
-        os.replace(tmp, root)
+    root = _dambreak_root(ncells, steps)
     deck = hb.Deck(root)
     C = deck.cells
     area = deck.array("area")
@@ -502,7 +570,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--extras", default="all",
-                    choices=["all", "none", "ensemble", "adjoint", "split", "fp32", "dambreak"])
+                    choices=["all", "none", "ensemble", "adjoint", "split", "fp32", "dambreak", "halo"])
     ap.add_argument("--only-extras", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=1000)
     ap.add_argument("--ensemble-steps", type=int, default=1000)
@@ -543,9 +611,10 @@ def main():
         legs = {"split": lambda: split_leg(deck, local), "fp32": lambda: split_leg(deck, local, precision="fp32"),
                 "ensemble": lambda: ensemble_leg(local, args.ensemble_steps, rank=rank, world=world),
                 "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
-                "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells)}
-        if world > 1 and args.extras != "ensemble":
-            raise SystemExit("--only-extras on several GPUs runs the ensemble only (--extras ensemble)")
+                "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells),
+                "halo": lambda: halo_leg(local, ncells=args.dambreak_cells, rank=rank, world=world)}
+        if world > 1 and args.extras not in ("ensemble", "halo"):
+            raise SystemExit("--only-extras on several GPUs runs the ensemble or the halo leg (--extras ensemble|halo)")
         out = {k: fn() for k, fn in legs.items() if args.extras in ("all", k)}
         if rank == 0:
             print(json.dumps(out), flush=True)
@@ -653,7 +722,8 @@ def main():
         legs = {"split": lambda: split_leg(deck, local), "fp32": lambda: split_leg(deck, local, precision="fp32"),
                 "ensemble": lambda: ensemble_leg(local, args.ensemble_steps),
                 "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
-                "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells)}
+                "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells),
+                "halo": lambda: halo_leg(local, ncells=args.dambreak_cells)}
         for name, fn in legs.items():
             if args.extras in ("all", name):
                 try:
@@ -665,6 +735,11 @@ def main():
         ens = ensemble_leg(local, args.ensemble_steps, rank=rank, world=world)
         if rank == 0:
             extras["ensemble"] = ens
+    elif world > 1 and args.extras == "halo":
+        # one mesh in one part per GPU, halo over NCCL (asked for explicitly)
+        hal = halo_leg(local, ncells=args.dambreak_cells, rank=rank, world=world)
+        if rank == 0:
+            extras["halo"] = hal
 
     if rank == 0:
         line = {
