@@ -12,7 +12,7 @@ the seeded decks of :mod:`hydrob200.deck`, runs the reference dump driver
 
 Usage::
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out /tmp/golden
 """
 from __future__ import annotations
 
