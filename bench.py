@@ -6,7 +6,7 @@ kernels of the edge layout, chained by programmatic dependent launch),
 replayed from a captured CUDA graph.  Prints ONE JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--extras all|none|ensemble|adjoint|split|fp32|dambreak|halo]
+                    [--extras all|none|ensemble|adjoint|split|fp32|dambreak|halo|persistent]
 
 On one GPU the line also carries these additions, each with its error
 against fp64 (``--extras`` chooses which; ``--only-extras`` skips the main
@@ -24,7 +24,11 @@ measurement, for profiling one of them):
               --extras halo: one part per GPU over NCCL);
   dambreak    2,000,000-cell dam break on a fractal bed, 2000 steps: split
               precision and fp32 against fp64 every 100 steps, and the speeds
-              of all three (HBM-bound: the working set is several L2s).
+              of all three (HBM-bound: the working set is several L2s);
+  persistent  the fp64 step as one cooperative launch per step sequence
+              (grid barriers between flux and cell phases) next to the
+              two-kernel sequence, on the 207K and the dam-break meshes,
+              with a bit-for-bit comparison of the two.
 Each reduced-precision and dam-break speed carries its algorithmic GB/s and
 the fraction of the measured copy bandwidth.
 
@@ -416,6 +420,43 @@ def split_leg(deck, local, steps=900, precision="split"):
 
 
 
+def persistent_leg(deck, local, steps=900, graph=100, dambreak_cells=0):
+    """The plain fp64 step with the whole sequence as one cooperative launch
+    (hb_options.persistent: flux records, grid barrier, cells, grid barrier)
+    next to the two-kernel sequence (flux and cell kernels chained by
+    programmatic dependent launch), both replayed from `graph`-step CUDA graphs
+    and timed the same way (warm, no L2 flush), then compared bit for bit
+    after the same steps.  With dambreak_cells, the same on the dam-break mesh
+    (HBM-bound) for 200 steps."""
+    import numpy as np
+    import torch
+    import hydrob200 as hb
+
+    def pair(dk, n, g):
+        two, one = hb.Solver(dk, device=local), hb.Solver(dk, device=local, persistent=True)
+        for s in (two, one):
+            s.step(10)
+            s.sync()
+        us_two = _time_graph(two, n, g, torch)
+        us_one = _time_graph(one, n, g, torch)
+        a, b = two.get_state(), one.get_state()
+        same = all(np.array_equal(a[k].view(np.uint64), b[k].view(np.uint64)) for k in "HUVZW")
+        edges = unique_edges(dk)
+        out = {"cells": dk.cells, "steps": n, "graph_steps": g, "us_per_step_two_kernel": us_two,
+               "us_per_step_persistent": us_one, "value_persistent": dk.cells / (us_one * 1e-6),
+               "value_two_kernel": dk.cells / (us_two * 1e-6), "unit": METRIC, "bit_identical": same,
+               "roofline_persistent": hbm_point("fp64", dk.cells, edges, us_one),
+               "roofline_two_kernel": hbm_point("fp64", dk.cells, edges, us_two)}
+        two.close()
+        one.close()
+        return out
+
+    out = {"c207k": pair(deck, steps, graph)}
+    if dambreak_cells:
+        out["dambreak"] = pair(hb.Deck(_dambreak_root(dambreak_cells, 2000)), 200, 50)
+    return out
+
+
 def _dambreak_root(ncells: int, steps: int) -> str:
     from hydrob200 import deck as D
     root = os.path.join(tempfile.gettempdir(), f"hb_dambreak_{ncells}_{steps}")
@@ -570,7 +611,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--extras", default="all",
-                    choices=["all", "none", "ensemble", "adjoint", "split", "fp32", "dambreak", "halo"])
+                    choices=["all", "none", "ensemble", "adjoint", "split", "fp32", "dambreak", "halo", "persistent"])
     ap.add_argument("--only-extras", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=1000)
     ap.add_argument("--ensemble-steps", type=int, default=1000)
@@ -612,7 +653,8 @@ def main():
                 "ensemble": lambda: ensemble_leg(local, args.ensemble_steps, rank=rank, world=world),
                 "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
                 "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells),
-                "halo": lambda: halo_leg(local, ncells=args.dambreak_cells, rank=rank, world=world)}
+                "halo": lambda: halo_leg(local, ncells=args.dambreak_cells, rank=rank, world=world),
+                "persistent": lambda: persistent_leg(deck, local, dambreak_cells=args.dambreak_cells)}
         if world > 1 and args.extras not in ("ensemble", "halo"):
             raise SystemExit("--only-extras on several GPUs runs the ensemble or the halo leg (--extras ensemble|halo)")
         out = {k: fn() for k, fn in legs.items() if args.extras in ("all", k)}
@@ -673,13 +715,19 @@ def main():
 
     # end to end through the public API: host state in and out every step (page-locked buffers)
     st = solver.get_state()
-    host = {k: torch.from_numpy(st[k]).pin_memory() for k in "HUVZW"}
+    block = torch.empty((4, C), dtype=torch.float64).pin_memory()   # rows H, U, V, Z: one copy each way
+    host = {}
+    for i, k in enumerate("HUVZ"):
+        block[i].copy_(torch.from_numpy(st[k]))
+        host[k] = block[i]
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.e2e_steps):
-        solver.step_host(host["H"], host["U"], host["V"], host["Z"], host["W"], 1, stream)
+        # the step's result is the new state H, U, V, Z (what the reference driver dumps,
+        # benchmark.cu:141-162); W = |(U, V)| stays on the device (hb_step_host takes W = NULL)
+        solver.step_host(host["H"], host["U"], host["V"], host["Z"], None, 1, stream)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
@@ -723,7 +771,8 @@ def main():
                 "ensemble": lambda: ensemble_leg(local, args.ensemble_steps),
                 "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
                 "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells),
-                "halo": lambda: halo_leg(local, ncells=args.dambreak_cells)}
+                "halo": lambda: halo_leg(local, ncells=args.dambreak_cells),
+                "persistent": lambda: persistent_leg(deck, local, dambreak_cells=args.dambreak_cells)}
         for name, fn in legs.items():
             if args.extras in ("all", name):
                 try:
@@ -757,7 +806,8 @@ def main():
             "error": err,
             "clocks": clocks,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 4 * 8 * C,
-                    "d2h_bytes_per_step": 5 * 8 * C, "api": "hb_step_host, one step per call, page-locked buffers"},
+                    "d2h_bytes_per_step": 4 * 8 * C,
+                    "api": "hb_step_host, one step per call, page-locked buffers, state H, U, V, Z in and out"},
             "gpu_launches": launches,
             "gpu_launches_e2e": launches_e2e,
             "cpu_baseline": cpu,

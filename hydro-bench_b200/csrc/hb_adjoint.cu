@@ -811,8 +811,9 @@ extern "C" int hb_adjoint_create(hb_handle *h, const int32_t *gauges, int32_t ng
         return hb::set_error(HB_E_INVALID, "hb_adjoint_create: bad argument");
     *out = nullptr;
     if (h->opt.precision != HB_FP64 || h->opt.variant != HB_VARIANT_H || h->opt.layout != HB_LAYOUT_EDGE ||
-        h->scn.size() != 1)
-        return hb::set_error(HB_E_INVALID, "hb_adjoint_create: needs a single-mesh fp64 variant-H edge-layout handle");
+        h->opt.persistent || h->scn.size() != 1)
+        return hb::set_error(HB_E_INVALID,
+                             "hb_adjoint_create: needs a single-mesh fp64 variant-H edge-layout handle (not persistent)");
     if (nsteps > h->step_limit()) return hb::set_error(HB_E_INVALID, "hb_adjoint_create: %d steps beyond the boundary tables", nsteps);
     const hb::Scenario &sc = h->scn[0];
     const int C = sc.cells;

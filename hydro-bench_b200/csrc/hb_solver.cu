@@ -532,6 +532,7 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *mds, int n, hb::DevMesh<
     }
     m.fseg = h->d_fseg[1];
     m.useg = h->d_useg;
+    m.rev_update = 1;
     {
         std::vector<hb::TileDesc> tiles;
         m.max_tile_cells = 1;
@@ -615,6 +616,49 @@ int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     return launch_tick(h, n, st);
 }
 
+// Persistent handles: the whole sequence as cooperative launches of the
+// default edge shape (128 threads, 6 CTAs per SM), as many CTAs as are
+// resident at once, each launch preceded by zeroing its barrier counter.
+// Sequences of more than PERSIST_MAX_STEPS steps take several launches (the
+// arrival count stays within 32 bits); the extra flux writes at the end of
+// each launch leave the same final fluxes.
+constexpr int PERSIST_THREADS = 128, PERSIST_MINB = 6, PERSIST_MAX_STEPS = 1 << 20;
+
+template <class A, int VARIANT, bool SEG>
+int launch_persistent_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
+    auto kernel = hb::persistent_kernel<A, VARIANT, PERSIST_THREADS, PERSIST_MINB, SEG>;
+    const int ts = thread_slot(PERSIST_THREADS);
+    m.fseg = h->d_fseg[ts];
+    const int nflux = SEG ? h->nfseg[ts] : (m.nrecords + PERSIST_THREADS - 1) / PERSIST_THREADS;
+    const int ncell = SEG ? h->nuseg : (h->C + hb::UPDATE_THREADS - 1) / hb::UPDATE_THREADS;
+    if (h->persist_blocks == 0) {
+        int per_sm = 0, sms = 0;
+        HB_CUDA_RET(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, PERSIST_THREADS, 0));
+        HB_CUDA_RET(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->opt.device));
+        if (per_sm < 1) return hb::set_error(HB_E_CUDA, "persistent kernel: no CTA fits on an SM");
+        h->persist_blocks = per_sm * sms;
+    }
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)std::max(1, std::min(h->persist_blocks, std::max(nflux, ncell))));
+    cfg.blockDim = dim3(PERSIST_THREADS);
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    for (int done = 0; done < n;) {
+        const int k = std::min(n - done, PERSIST_MAX_STEPS);
+        HB_CUDA_RET(cudaMemsetAsync(h->d_bar, 0, sizeof(unsigned), st));
+        HB_CUDA_RET(cudaLaunchKernelEx(&cfg, kernel, m, k, nflux, ncell, h->d_bar, h->barrier_phantom,
+                                       h->barrier_limit_ns));
+        // the step counter advances per launch: the next launch's steps follow on
+        TRY(launch_tick(h, k, st));
+        done += k;
+    }
+    return HB_OK;
+}
+
 size_t tile_smem_bytes(int max_cells, int max_pairs, size_t real_size) {
     return 16 * real_size * (size_t)max_cells + sizeof(int) * (size_t)max_pairs;
 }
@@ -677,6 +721,10 @@ int enqueue_steps(hb_handle *h, int n, cudaStream_t st) {
     return h->with_mesh([&](auto &m) {
         using A = typename std::remove_reference<decltype(m)>::type::Policy;
         if (tiles) return f ? launch_tiles_t<A, 1>(h, m, n, st) : launch_tiles_t<A, 0>(h, m, n, st);
+        if (h->opt.persistent) {
+            if (seg) return f ? launch_persistent_t<A, 1, true>(h, m, n, st) : launch_persistent_t<A, 0, true>(h, m, n, st);
+            return f ? launch_persistent_t<A, 1, false>(h, m, n, st) : launch_persistent_t<A, 0, false>(h, m, n, st);
+        }
         if (seg) return f ? launch_steps_t<A, 1, true>(h, m, n, st) : launch_steps_t<A, 0, true>(h, m, n, st);
         return f ? launch_steps_t<A, 1, false>(h, m, n, st) : launch_steps_t<A, 0, false>(h, m, n, st);
     });
@@ -772,6 +820,10 @@ extern "C" int hb_create_batch(const hb_mesh_desc *meshes, int32_t n, const hb_o
         return hb::set_error(HB_E_INVALID, "hb_create: tile_cells %d outside 0..1024", opt.tile_cells);
     if (config_for(opt.layout, opt.tile_config) < 0)
         return hb::set_error(HB_E_INVALID, "hb_create: tile_config %d is no shape of layout %d", opt.tile_config, opt.layout);
+    if (opt.persistent != 0 && opt.persistent != 1)
+        return hb::set_error(HB_E_INVALID, "hb_create: persistent %d", opt.persistent);
+    if (opt.persistent && (opt.layout != HB_LAYOUT_EDGE || config_for(opt.layout, opt.tile_config) != hb::DEFAULT_EDGE_CONFIG))
+        return hb::set_error(HB_E_INVALID, "hb_create: a persistent handle takes the edge layout's default launch shape");
     long long total = 0;
     for (int s = 0; s < n; s++) total += std::max(meshes[s].cells, 0);
     if (total > (1 << 29)) return hb::set_error(HB_E_TOO_LARGE, "hb_create: %lld cells", total);
@@ -780,7 +832,8 @@ extern "C" int hb_create_batch(const hb_mesh_desc *meshes, int32_t n, const hb_o
     h->opt = opt;
     h->launch_config = config_for(opt.layout, opt.tile_config);
     int st;
-    if ((st = dev_alloc(h, &h->d_err, 1)) != HB_OK || (st = dev_alloc(h, &h->d_ctr, 1)) != HB_OK) {
+    if ((st = dev_alloc(h, &h->d_err, 1)) != HB_OK || (st = dev_alloc(h, &h->d_ctr, 1)) != HB_OK ||
+        (st = dev_alloc(h, &h->d_bar, 1)) != HB_OK) {
         delete h;
         return st;
     }
@@ -941,15 +994,28 @@ int step_host_t(hb_handle *h, hb::DevMesh<A> &m, double *H, double *U, double *V
     const int C = sc.cells;
     const size_t b = (size_t)C * sizeof(double);
     double *io[5] = {H, U, V, Z, W};
-    for (int k = 0; k < 4; k++) HB_CUDA_RET(cudaMemcpyAsync(h->d_stage + (size_t)k * C, io[k], b, cudaMemcpyHostToDevice, st));
+    // arrays that follow one another in host memory (H, U, V, Z, W rows of one
+    // [5][CELL] block) move as one copy, like the staging rows on the device
+    auto copies = [&](int nk, cudaMemcpyKind kind) -> int {
+        for (int k = 0; k < nk;) {
+            if (!io[k]) { k++; continue; }
+            int e = k + 1;
+            while (e < nk && io[e] == io[e - 1] + C) e++;
+            double *dev = h->d_stage + (size_t)k * C;
+            if (kind == cudaMemcpyHostToDevice) HB_CUDA_RET(cudaMemcpyAsync(dev, io[k], b * (e - k), kind, st));
+            else HB_CUDA_RET(cudaMemcpyAsync(io[k], dev, b * (e - k), kind, st));
+            k = e;
+        }
+        return HB_OK;
+    };
+    TRY(copies(4, cudaMemcpyHostToDevice));
     const int blocks = (C + 255) / 256;
     hb::stage_in_kernel<A><<<blocks, 256, 0, st>>>(m, 0, C, sc.hm1, h->d_perm, h->d_stage);
     HB_CUDA_RET(cudaGetLastError());
     TRY(enqueue_steps(h, n, st));
     hb::stage_out_kernel<A><<<blocks, 256, 0, st>>>(m, 0, C, sc.hm1, h->d_perm, h->d_stage);
     HB_CUDA_RET(cudaGetLastError());
-    for (int k = 0; k < 5; k++)
-        if (io[k]) HB_CUDA_RET(cudaMemcpyAsync(io[k], h->d_stage + (size_t)k * C, b, cudaMemcpyDeviceToHost, st));
+    TRY(copies(5, cudaMemcpyDeviceToHost));
     return HB_OK;
 }
 }  // namespace
@@ -971,9 +1037,20 @@ extern "C" int hb_sync(hb_handle *h, void *stream) {
     HB_CUDA_RET(cudaStreamSynchronize((cudaStream_t)stream));
     uint32_t bits = 0;
     HB_CUDA_RET(cudaMemcpy(&bits, h->d_err, sizeof bits, cudaMemcpyDeviceToHost));
+    if (bits & hb::ERRBIT_BARRIER) return hb::set_error(HB_E_BARRIER_TIMEOUT, "a grid barrier of the persistent kernel gave up waiting");
     if (bits & hb::ERRBIT_NONFINITE) return hb::set_error(HB_E_NONFINITE, "a step produced a non-finite state");
     if (bits & hb::ERRBIT_UNDEFINED) return hb::set_error(HB_E_UNDEFINED_REF, "a slot without neighbour reached the mirrored Osher branch");
     if (bits & hb::ERRBIT_TABLE_RANGE) return hb::set_error(HB_E_INVALID, "a step ran beyond the boundary tables");
+    return HB_OK;
+}
+
+extern "C" int hb_set_barrier_limit(hb_handle *h, int64_t timeout_ns, int32_t phantom_arrivals) {
+    if (!h || timeout_ns <= 0 || timeout_ns > 10000000000ll || phantom_arrivals < 0 || phantom_arrivals > (1 << 20))
+        return hb::set_error(HB_E_INVALID, "hb_set_barrier_limit: bad argument");
+    if ((unsigned long long)timeout_ns != h->barrier_limit_ns || (unsigned)phantom_arrivals != h->barrier_phantom)
+        h->drop_graph();   // both are launch arguments captured by a graph
+    h->barrier_limit_ns = (unsigned long long)timeout_ns;
+    h->barrier_phantom = (unsigned)phantom_arrivals;
     return HB_OK;
 }
 
@@ -1071,6 +1148,8 @@ extern "C" int hb_set_tile_config(hb_handle *h, int32_t tile_config) {
     if (!h) return hb::set_error(HB_E_INVALID, "null handle");
     const int c = config_for(h->opt.layout, tile_config);
     if (c < 0) return hb::set_error(HB_E_INVALID, "tile_config %d is no shape of this handle's layout", tile_config);
+    if (h->opt.persistent && c != hb::DEFAULT_EDGE_CONFIG)
+        return hb::set_error(HB_E_INVALID, "a persistent handle keeps the default launch shape");
     if (c != h->launch_config) h->drop_graph();
     h->launch_config = c;
     return HB_OK;
@@ -1091,6 +1170,7 @@ extern "C" int hb_autotune(hb_handle *h, int32_t steps, void *stream, float *ms_
                            int32_t *best) {
     NvtxRange nvtx_("hb_autotune");
     if (!h || steps <= 0) return hb::set_error(HB_E_INVALID, "hb_autotune: bad argument");
+    if (h->opt.persistent) return hb::set_error(HB_E_INVALID, "hb_autotune: a persistent handle has one launch shape");
     TRY(check_range(h, (long long)steps + 1));
     cudaStream_t st = (cudaStream_t)stream;
     HB_CUDA_RET(cudaDeviceSynchronize());

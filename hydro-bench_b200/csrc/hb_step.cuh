@@ -90,6 +90,10 @@ struct DevMesh {
     const ScnParams *scn;      // [nscen]
     const int4 *fseg;          // flux CTAs {scenario, first record, records, 1 = mirror pairs}
     const int4 *useg;          // update CTAs {scenario, first cell, cells, 0}
+    // edge layout: the cell kernel takes its CTAs' cell ranges in reverse order
+    // (last range first), so it starts on the slot terms the flux kernel wrote
+    // last, which are still in L2 when the mesh's terms exceed it
+    int rev_update;
     // tile layout
     const TileDesc *tiles;     // [ntiles]
     int ntiles, max_tile_cells, max_tile_pairs;
@@ -445,8 +449,9 @@ __device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const Ste
 // update coefficients of the wet cells into m.ucoef.
 template <class A, int VARIANT, int UMINB, bool SEG, bool COEF = false>
 __global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<A> m, int k, int write_flux) {
+    const int blk = m.rev_update ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
     if constexpr (SEG) {
-        const int4 d = m.useg[blockIdx.x];
+        const int4 d = m.useg[blk];
         const ScnParams sp = m.scn[d.x];
         cudaGridDependencySynchronize();
         cudaTriggerProgrammaticLaunchCompletion();
@@ -459,7 +464,7 @@ __global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<A
         cudaTriggerProgrammaticLaunchCompletion();
         const StepIndex si = step_index(m, k, m.per_day, m.ndays);
         const StepParams p{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
-        for (int c = blockIdx.x * UPDATE_THREADS + threadIdx.x; c < m.C; c += gridDim.x * UPDATE_THREADS)
+        for (int c = blk * UPDATE_THREADS + threadIdx.x; c < m.C; c += gridDim.x * UPDATE_THREADS)
             update_one<A, VARIANT, COEF>(m, c, si, p, write_flux, m.slotw + 16 * (size_t)c);
     }
 }
@@ -496,6 +501,138 @@ __global__ void __launch_bounds__(THREADS, MINB) tile_kernel(DevMesh<A> m, int k
     __syncthreads();
     for (int c = threadIdx.x; c < td.cells; c += THREADS)
         update_one<A, VARIANT, false, true>(m, td.cell0 + c, si, p, write_flux, terms + 16 * c);
+}
+
+// ---------------------------------------------------------------------------
+// persistent step sequence (edge layout, hb_options.persistent)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Backstop of a barrier wait when the global timer does not advance: each
+// poll is an L2 round trip (>= 0.3 us), so this many polls last >= 10 s.
+constexpr unsigned BARRIER_MAX_POLLS = 1u << 25;
+
+// Grid-wide barrier of a cooperative launch.  *bar counts CTA arrivals since
+// the launch began (the host zeroes it before each launch); a barrier returns
+// once `target` arrivals are counted.  The wait is bounded: after limit_ns of
+// the global timer (or BARRIER_MAX_POLLS polls), or as soon as another CTA has
+// given up, it sets ERRBIT_BARRIER and returns false, and the caller's CTA
+// leaves the kernel, so a barrier that cannot complete ends the launch with a
+// status instead of a hang.  Ordering is the grid-sync pattern: the CTA's
+// writes are ordered before thread 0's arrival by __syncthreads and a device
+// fence, and thread 0's fence after it saw the count orders the CTA's later
+// reads after every arrived CTA's writes.
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned target, uint32_t *err,
+                                             unsigned long long limit_ns) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int good = 1;
+        __threadfence();
+        unsigned seen = atomicAdd(bar, 1u) + 1u;
+        if (seen < target) {
+            const unsigned long long t0 = global_ns();
+            for (unsigned polls = 1;; polls++) {
+                __nanosleep(32);
+                seen = *(volatile unsigned *)bar;
+                if (seen >= target) break;
+                if ((polls & 15u) == 0) {
+                    const bool other_gave_up = (*(volatile uint32_t *)err & ERRBIT_BARRIER) != 0;
+                    if (other_gave_up || global_ns() - t0 > limit_ns || polls >= BARRIER_MAX_POLLS) {
+                        atomicOr(err, ERRBIT_BARRIER);
+                        good = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// All n steps of a sequence in one cooperative launch whose CTAs are all
+// resident: per step, the flux records in chunks of THREADS (batch: the flux
+// segment table's entries) over the CTAs, a grid barrier, the cells in chunks
+// of UPDATE_THREADS (batch: the cell segment table's entries), and a grid
+// barrier before the next step.  Each chunk runs exactly as one CTA of
+// flux_kernel / update_kernel does, so the results are those of the two-kernel
+// sequence bit for bit.  `phantom` adds arrivals that never come to every
+// barrier (0 in use; > 0 only to exercise the bounded wait).
+template <class A, int VARIANT, int THREADS, int MINB, bool SEG>
+__global__ void __launch_bounds__(THREADS, MINB)
+    persistent_kernel(DevMesh<A> m, int n, int nflux, int ncell, unsigned *bar, unsigned phantom,
+                      unsigned long long limit_ns) {
+    __shared__ int queue[THREADS];
+    __shared__ int qn;
+    const Terms<typename A::real> tout{m.slotw, 0};
+    unsigned arrivals = 0;
+    for (int k = 0; k < n; k++) {
+        const int wf = k == n - 1;
+        for (int b = blockIdx.x; b < nflux; b += gridDim.x) {
+            int r0, cnt;
+            bool seg_pairs = false;
+            StepIndex si;
+            StepParams p;
+            if constexpr (SEG) {
+                const int4 d = m.fseg[b];
+                const ScnParams sp = m.scn[d.x];
+                si = step_index(m, k, sp.per_day, sp.ndays);
+                p = StepParams{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
+                r0 = d.y;
+                cnt = d.z;
+                seg_pairs = d.w != 0;
+            } else {
+                si = step_index(m, k, m.per_day, m.ndays);
+                p = StepParams{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
+                r0 = b * THREADS;
+                cnt = min(THREADS, m.nrecords - r0);
+            }
+            if (threadIdx.x == 0) qn = 0;
+            __syncthreads();
+            if ((int)threadIdx.x < cnt) {
+                const int r = r0 + (int)threadIdx.x;
+                const bool pair = SEG ? seg_pairs : r < m.npairs;
+                if (pair) pair_record<A, VARIANT>(m, r, si, p, wf, tout, queue, &qn);
+                else single_record<A, VARIANT>(m, r, si, p, wf, tout);
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < qn; i += THREADS) pair_mirror<A>(m, queue[i], si, p, wf, tout);
+            __syncthreads();   // the queue is reused by the next chunk
+        }
+        arrivals += gridDim.x;
+        if (!grid_barrier(bar, arrivals + phantom, m.err, limit_ns)) return;
+        for (int b = blockIdx.x; b < ncell; b += gridDim.x) {
+            int c0, cnt;
+            StepIndex si;
+            StepParams p;
+            if constexpr (SEG) {
+                const int4 d = m.useg[b];
+                const ScnParams sp = m.scn[d.x];
+                si = step_index(m, k, sp.per_day, sp.ndays);
+                p = StepParams{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
+                c0 = d.y;
+                cnt = d.z;
+            } else {
+                si = step_index(m, k, m.per_day, m.ndays);
+                p = StepParams{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
+                c0 = b * UPDATE_THREADS;
+                cnt = min(UPDATE_THREADS, m.C - c0);
+            }
+            for (int i = threadIdx.x; i < cnt; i += THREADS)
+                update_one<A, VARIANT>(m, c0 + i, si, p, wf, m.slotw + 16 * (size_t)(c0 + i));
+        }
+        if (k + 1 < n) {
+            arrivals += gridDim.x;
+            if (!grid_barrier(bar, arrivals + phantom, m.err, limit_ns)) return;
+        }
+    }
 }
 
 // Advances the step counter after a step sequence.  Launched with

@@ -38,7 +38,7 @@ class MeshDesc(C.Structure):
 class Options(C.Structure):
     _fields_ = [("variant", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32), ("renumber", C.c_int32),
                 ("tile_config", C.c_int32), ("layout", C.c_int32), ("tile_cells", C.c_int32),
-                ("reserved", C.c_int32 * 1)]
+                ("persistent", C.c_int32)]
 
 
 def _view_types(real):
@@ -109,6 +109,7 @@ def lib():
         "hb_device_state": (C.c_int, [vp] + [C.POINTER(vp)] * 5 + [C.POINTER(C.c_int32)]),
         "hb_get_permutation": (C.c_int, [vp, _ip]),
         "hb_device_errors": (C.c_int, [vp, C.POINTER(C.c_uint32)]),
+        "hb_set_barrier_limit": (C.c_int, [vp, C.c_int64, C.c_int32]),
         "hb_last_error": (C.c_int, []),
         "hb_last_error_string": (C.c_char_p, []),
         "hb_status_string": (C.c_char_p, [C.c_int]),
@@ -159,7 +160,7 @@ def check(status: int) -> None:
 # every symbol the C headers declare (checked by the CPU tests)
 EXPORTED = ["hb_options_default", "hb_tile_configs", "hb_launch_shapes", "hb_create", "hb_destroy", "hb_set_state", "hb_get_state", "hb_get_flux",
             "hb_get_klas", "hb_step", "hb_sync", "hb_position", "hb_set_position", "hb_step_host", "hb_capture_graph",
-            "hb_graph_launch", "hb_device_state", "hb_get_permutation", "hb_device_errors", "hb_last_error",
+            "hb_graph_launch", "hb_device_state", "hb_get_permutation", "hb_device_errors", "hb_set_barrier_limit", "hb_last_error",
             "hb_last_error_string", "hb_status_string", "hb_deck_load", "hb_deck_mesh", "hb_deck_state",
             "hb_deck_free", "hb_ref_calculate_flux", "hb_ref_update_cell", "hb_ref_calculate_flux_f32",
             "hb_ref_update_cell_f32", "hb_ref_take_device_errors", "hb_ref_step_static",

@@ -32,7 +32,7 @@ def launch_shapes():
             for i in range(n)}
 
 
-def _options(variant, precision, device, renumber, tile_config, layout, tile_cells):
+def _options(variant, precision, device, renumber, tile_config, layout, tile_cells, persistent=False):
     opt = _lib.Options()
     lib().hb_options_default(C.byref(opt))
     opt.variant = _VARIANTS[variant]
@@ -42,6 +42,7 @@ def _options(variant, precision, device, renumber, tile_config, layout, tile_cel
     opt.tile_config = int(tile_config)
     opt.layout = _LAYOUTS[layout]
     opt.tile_cells = int(tile_cells)
+    opt.persistent = 1 if persistent else 0
     return opt
 
 CELL_ARRAYS = ("zbc", "zb1", "area", "fnc", "bfeat")
@@ -103,9 +104,10 @@ class Solver:
     """
 
     def __init__(self, deck: Deck, variant="H", precision="fp64", device: int = 0, renumber: bool = True,
-                 init_state: bool = True, tile_config: int = 0, layout="edge", tile_cells: int = 0):
+                 init_state: bool = True, tile_config: int = 0, layout="edge", tile_cells: int = 0,
+                 persistent: bool = False):
         self.deck = deck   # keeps the host arrays alive
-        opt = _options(variant, precision, device, renumber, tile_config, layout, tile_cells)
+        opt = _options(variant, precision, device, renumber, tile_config, layout, tile_cells, persistent)
         self.layout = opt.layout
         self.variant = opt.variant
         self.precision = opt.precision
@@ -190,6 +192,10 @@ class Solver:
         check(lib().hb_device_errors(self._h, C.byref(v)))
         return v.value
 
+    def set_barrier_limit(self, timeout_ns: int, phantom_arrivals: int = 0) -> None:
+        """hb_set_barrier_limit: bound of the persistent kernel's grid-barrier waits."""
+        check(lib().hb_set_barrier_limit(self._h, int(timeout_ns), int(phantom_arrivals)))
+
     @property
     def position(self):
         s, kt, jt = C.c_int64(), C.c_int32(), C.c_int32()
@@ -270,9 +276,9 @@ class Batch(Solver):
 
     def __init__(self, decks: Sequence[Deck], variant="H", precision="fp64", device: int = 0,
                  renumber: bool = True, init_state: bool = True, tile_config: int = 0, layout="edge",
-                 tile_cells: int = 0):
+                 tile_cells: int = 0, persistent: bool = False):
         self.decks = list(decks)   # keeps the host arrays alive
-        opt = _options(variant, precision, device, renumber, tile_config, layout, tile_cells)
+        opt = _options(variant, precision, device, renumber, tile_config, layout, tile_cells, persistent)
         self.layout = opt.layout
         self.variant = opt.variant
         self.precision = opt.precision

@@ -80,7 +80,11 @@ typedef struct hb_options {
     int32_t tile_config;      /* launch shape: 0 = the layout's default, k > 0 = entry k-1 of hb_launch_shapes() */
     int32_t layout;           /* hb_layout */
     int32_t tile_cells;       /* HB_LAYOUT_TILE: cells per tile, <= 1024 (0 = 256); tiles hold up to 5*tile_cells/4 */
-    int32_t reserved[1];
+    int32_t persistent;       /* HB_LAYOUT_EDGE with the default launch shape only.  1: a step sequence
+                               * (hb_step, a captured graph) is one cooperative launch of resident CTAs that
+                               * runs every step, flux records then cells, separated by grid barriers whose
+                               * waits are bounded (hb_set_barrier_limit); 0: two launches per step.  Same
+                               * bits either way.  Not for hb_autotune. */
 } hb_options;
 
 /* The compiled launch shapes: the layout each runs, threads per CTA, and
@@ -150,7 +154,9 @@ int hb_set_position(hb_handle *h, int64_t steps_done);
 /* End-to-end call with host buffers, for callers whose state lives on the
  * host (the reference driver keeps it in MeshData, benchmark.cu:66-84):
  * copies H, U, V, Z (reference order, [CELL] fp64) to the device, advances
- * nsteps steps, and copies H, U, V, Z, W back into the same buffers.  The
+ * nsteps steps, and copies H, U, V, Z, W back into the same buffers (W may be
+ * NULL; arrays that follow one another in host memory, e.g. the rows of one
+ * [4][CELL] or [5][CELL] block, move as one copy).  The
  * copies are asynchronous on `stream` (page-locked buffers make them truly
  * so); call hb_sync before reading the results. */
 int hb_step_host(hb_handle *h, double *H, double *U, double *V, double *Z, double *W, int32_t nsteps, void *stream);
@@ -197,6 +203,14 @@ int hb_state_record_bytes(const hb_handle *h, int32_t *bytes);
 int hb_halo_define(hb_handle *h, const int32_t *cells, int32_t n, int32_t *list);
 int hb_halo_pack(hb_handle *h, int32_t list, void *buf, void *stream);
 int hb_halo_unpack(hb_handle *h, int32_t list, const void *buf, void *stream);
+/* Bound of every grid-barrier wait of a persistent handle (default 1 s of the
+ * GPU's global timer, at most 10 s).  A wait that runs out sets the device
+ * error bit of HB_E_BARRIER_TIMEOUT (hb_sync returns it) and every CTA leaves
+ * the launch; the state is then partly stepped.  phantom_arrivals > 0 makes
+ * every barrier also wait for that many arrivals that never come, so that the
+ * bounded wait can be exercised without a fault; use 0. */
+int hb_set_barrier_limit(hb_handle *h, int64_t timeout_ns, int32_t phantom_arrivals);
+
 /* Sticky device error word (bit set of hb_status codes seen by kernels). */
 int hb_device_errors(hb_handle *h, uint32_t *bits);
 
@@ -214,8 +228,8 @@ const char *hb_status_string(int status);
  * mesh.cpp:350-361).  Branch choices (wet/dry, Osher's wave case, clamps,
  * fixed-point iteration counts) are those of the forward state.  The state is
  * checkpointed every checkpoint_every steps and each segment recomputed in
- * the backward pass.  Needs a single-mesh fp64 variant-H edge-layout handle
- * whose boundary codes are among KLAS 0, 1, 4, 10.  The rollout runs on the
+ * the backward pass.  Needs a single-mesh fp64 variant-H edge-layout handle,
+ * not persistent, whose boundary codes are among KLAS 0, 1, 4, 10.  The rollout runs on the
  * handle's own mesh and state (its state is the rollout's end afterwards). */
 typedef struct hb_adjoint hb_adjoint;
 int hb_adjoint_create(hb_handle *h, const int32_t *gauges, int32_t ngauges, int32_t obs_every, int32_t nsteps,

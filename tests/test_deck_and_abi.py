@@ -97,6 +97,18 @@ def test_library_exports_reference_signatures():
         assert sym in out, sym
 
 
+def test_persistent_option_is_checked_before_any_device_work(deck_dir):
+    """A persistent handle takes the edge layout's default launch shape only;
+    other combinations are refused by hb_create before it touches a device."""
+    import hydrob200 as hb
+    deck = hb.Deck(deck_dir["stress_a"])
+    for kw in (dict(layout="tile"), dict(tile_config=2), dict(tile_config=9, layout="tile")):
+        with pytest.raises(hb.HydroError) as e:
+            hb.Solver(deck, persistent=True, **kw)
+        assert e.value.status == 1, kw
+    assert _lib.lib().hb_set_barrier_limit(None, 1_000_000, 0) == 1
+
+
 def test_status_strings():
     l = _lib.lib()
     for code in range(10):
