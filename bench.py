@@ -6,7 +6,7 @@ kernels of the edge layout, chained by programmatic dependent launch),
 replayed from a captured CUDA graph.  Prints ONE JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--extras all|none|ensemble|adjoint|split|fp32|dambreak|halo|persistent]
+                    [--extras all|none|ensemble|adjoint|split|fp32|dambreak|halo|persistent|refgpu]
 
 On one GPU the line also carries these additions, each with its error
 against fp64 (``--extras`` chooses which; ``--only-extras`` skips the main
@@ -28,9 +28,13 @@ measurement, for profiling one of them):
   persistent  the fp64 step as one cooperative launch per step sequence
               (grid barriers between flux and cell phases) next to the
               two-kernel sequence, on the 207K and the dam-break meshes,
-              with a bit-for-bit comparison of the two.
+              with a bit-for-bit comparison of the two;
+  refgpu      the reference's own fp64 CUDA kernels (cuda_native_impl, built
+              for sm_100a) on the same 207K deck, timed by the reference
+              driver's sync / async / graph loops.
 Each reduced-precision and dam-break speed carries its algorithmic GB/s and
-the fraction of the measured copy bandwidth.
+the fraction of the measured copy bandwidth.  A `summary` object ahead of the
+additions' full records carries the headline figure of each.
 
 Multi-GPU: one process per GPU (torchrun); each rank runs its own replica of
 the scenario (the path has no exchange step between independent meshes), the
@@ -58,6 +62,7 @@ METRIC = "cell-steps/s"
 WORKLOAD = "plain fp64 step, 207,234-cell Delaunay channel 40 km x 8 km (1 m bumps, 400 m^3/s Gaussian hydrograph), CUDA-graph replay"
 FALLBACK_HBM_GBS = 6650.0
 L2_FLUSH_BYTES = 256 << 20
+EXTRA_STEPS_207K = 900   # steps the split / fp32 / persistent additions take on the 207K deck
 
 
 def _env_int(k, d):
@@ -183,15 +188,15 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference CPU solver (hydro-cal-fortan/calculate.cpp)
 # ---------------------------------------------------------------------------
-def _calc_deck(deck, steps: int, workdir: str) -> None:
+def _calc_deck(deck, steps: int, workdir: str, open_boundaries: bool) -> None:
     from hydrob200 import deck as D
     root = os.path.join(workdir, f"s{steps}", "origin", "changjiangkou")
     if not os.path.exists(os.path.join(root, "TIME.DAT")):
-        D.write_cpu_solver_deck(deck, root, steps=steps)
+        D.write_cpu_solver_deck(deck, root, steps=steps, open_boundaries=open_boundaries)
 
 
-def _calc_run(binary: str, deck, steps: int, workdir: str) -> float:
-    _calc_deck(deck, steps, workdir)
+def _calc_run(binary: str, deck, steps: int, workdir: str, open_boundaries: bool) -> float:
+    _calc_deck(deck, steps, workdir, open_boundaries)
     t0 = time.perf_counter()
     subprocess.run([binary], cwd=os.path.join(workdir, f"s{steps}"), check=True, stdout=subprocess.DEVNULL,
                    stderr=subprocess.DEVNULL, timeout=900)
@@ -201,17 +206,22 @@ def _calc_run(binary: str, deck, steps: int, workdir: str) -> float:
 def cpu_reference_rate(deck, sample_steps: int, replicas: int):
     """Cell-steps/s of the reference CPU solver, `replicas` concurrent
     single-threaded processes (one per core); returns (value, cores, kind, sample)."""
-    binary = os.path.join(ROOT, "oracle", "_ref", "calculate")
+    # the solver with the minimal open-boundary patch runs the deck as it is;
+    # the unpatched one runs it with its open boundaries as walls
+    binary = os.path.join(ROOT, "oracle", "_ref", "calculate_open")
+    open_b = os.path.exists(binary)
+    if not open_b:
+        binary = os.path.join(ROOT, "oracle", "_ref", "calculate")
     work = tempfile.mkdtemp(prefix="hb_cpu_")
     try:
         if os.path.exists(binary):
-            t1 = _calc_run(binary, deck, 1, work)           # start-up and deck reading
-            _calc_deck(deck, sample_steps, work)
+            t1 = _calc_run(binary, deck, 1, work, open_b)           # start-up and deck reading
+            _calc_deck(deck, sample_steps, work, open_b)
             times = []
             lock = threading.Lock()
 
             def one():
-                t = _calc_run(binary, deck, sample_steps, work)
+                t = _calc_run(binary, deck, sample_steps, work, open_b)
                 with lock:
                     times.append(t)
             th = [threading.Thread(target=one) for _ in range(replicas)]
@@ -221,9 +231,11 @@ def cpu_reference_rate(deck, sample_steps: int, replicas: int):
                 t.join()
             per = [max(t - t1, 1e-9) / (sample_steps - 1) for t in times]
             value = sum(deck.cells / p for p in per)
+            how = ("open boundaries and tables as in the GPU deck; solver built with the minimal patch "
+                   "oracle/calc_patch.sed" if open_b else "open boundaries as walls; unpatched solver")
             return value, replicas, "reference", (f"hydro-cal-fortan/calculate.cpp (g++ -O3), {replicas} concurrent "
                                                   f"single-threaded processes x {sample_steps} steps of the {deck.cells}-cell "
-                                                  f"mesh (open boundaries as walls), start-up time subtracted")
+                                                  f"mesh ({how}), start-up time subtracted")
         # no reference build: the oracle port, all host threads
         sys.path.insert(0, ROOT)
         from oracle.oracle import OracleDeck
@@ -396,7 +408,7 @@ def adjoint_leg(local, steps=1000, ks=(10, 50, 100)):
     return out
 
 
-def split_leg(deck, local, steps=900, precision="split"):
+def split_leg(deck, local, steps=EXTRA_STEPS_207K, precision="split"):
     """The reduced-precision step on the 207K mesh (tile layout, autotuned):
     time from 100-step graph replays, and its depths after `steps` steps
     against the fp64 step's."""
@@ -420,7 +432,7 @@ def split_leg(deck, local, steps=900, precision="split"):
 
 
 
-def persistent_leg(deck, local, steps=900, graph=100, dambreak_cells=0):
+def persistent_leg(deck, local, steps=EXTRA_STEPS_207K, graph=100, dambreak_cells=0):
     """The plain fp64 step with the whole sequence as one cooperative launch
     (hb_options.persistent: flux records, grid barrier, cells, grid barrier)
     next to the two-kernel sequence (flux and cell kernels chained by
@@ -454,6 +466,37 @@ def persistent_leg(deck, local, steps=900, graph=100, dambreak_cells=0):
     out = {"c207k": pair(deck, steps, graph)}
     if dambreak_cells:
         out["dambreak"] = pair(hb.Deck(_dambreak_root(dambreak_cells, 2000)), 200, 50)
+    return out
+
+
+def reference_gpu_leg(root: str, cells: int, steps: int = EXTRA_STEPS_207K, repeat: int = 5) -> dict:
+    """The reference's own fp64 CUDA kernels (cuda_native_impl, variant H,
+    built for sm_100a by oracle/ref.mk) on the same 207K deck, timed by the
+    reference driver's own loops (cuda_native_impl/benchmark.cu:172-266):
+    sync (a device synchronize after every step), async (no synchronize) and
+    graph (one captured CalculateFlux + UpdateCell pair replayed per step).
+    Each figure is the driver's median over `repeat` runs of `steps` steps,
+    host wall clock around the launches and a final synchronize."""
+    binary = os.path.join(ROOT, "oracle", "_ref", "ref_h64")
+    if not os.path.exists(binary):
+        return {"error": "oracle/_ref/ref_h64 not built"}
+    run = os.path.join(root, "run")
+    os.makedirs(run, exist_ok=True)
+    t0 = time.perf_counter()
+    r = subprocess.run([binary, str(steps), str(repeat)], cwd=run, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return {"error": f"ref_h64 exited {r.returncode}: {r.stdout[-200:]} {r.stderr[-200:]}"}
+    out = {"binary": "cuda_native_impl (benchmark.cu + hydro-cal-src), nvcc -O3 -rdc=true -arch=sm_100a",
+           "cells": cells, "steps": steps, "repeat": repeat,
+           "timing": "reference driver's own: median of repeat runs, host wall clock (benchmark.cu:172-266)",
+           "wall_s": time.perf_counter() - t0}
+    for mode in ("Sync", "Async", "Graph"):
+        m = re.search(rf"^{mode}:\s*median=([0-9.]+) ms,\s*([0-9.]+) us/step", r.stdout, re.M)
+        if m:
+            us = float(m.group(2))
+            out[f"{mode.lower()}_us_per_step"] = us
+            out[f"{mode.lower()}_value"] = cells / (us * 1e-6)
+    out["unit"] = METRIC
     return out
 
 
@@ -584,8 +627,18 @@ def dambreak_leg(local, steps=2000, every=100, ncells=2_000_000):
                                "mass_rel": e["mass_rel"], "wet_cells": int(wet64.sum()),
                                "wet_dry_mismatch": int(np.sum(wet64 != (hs > hm2))),
                                "rel_max_deeper_0.1m": float(np.max((np.abs(hs - h64) / h64)[h64 > 0.1]))})
-    out["error_vs_fp64"] = rows["split"]
-    out["fp32_error_vs_fp64"] = rows["fp32"]
+    def digest(rs):
+        """The last comparison and the worst of every comparison (one row per `every` steps)."""
+        keys = ("rel_max_wet", "normwise", "rel_max_deeper_0.1m", "wet_dry_mismatch")
+        worst = {k: max(r[k] for r in rs) for k in keys}
+        worst["mass_rel_abs"] = max(abs(r["mass_rel"]) for r in rs)
+        early = [r for r in rs if r["step"] <= 400]
+        if early:
+            worst["normwise_steps_100_400"] = max(r["normwise"] for r in early)
+        return {"compared": len(rs), "last": rs[-1], "max_over_compares": worst}
+
+    out["error_vs_fp64"] = digest(rows["split"])
+    out["fp32_error_vs_fp64"] = digest(rows["fp32"])
     n = every * (steps // every)
     edges = unique_edges(deck)
     for name in runs:
@@ -600,6 +653,56 @@ def dambreak_leg(local, steps=2000, every=100, ncells=2_000_000):
     return out
 
 
+def summarize(extras: dict, us_step: float, cells: int) -> dict:
+    """The headline figure of every addition in one small object (the full
+    records follow it in the line); a failed addition shows its error."""
+    def pick(d, *path):
+        for k in path:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+
+    s = {}
+    for key, leg in extras.items():
+        if isinstance(leg, dict) and "error" in leg and len(leg) == 1:
+            s[key] = {"error": leg["error"]}
+    for key in ("split_207k", "fp32_207k"):
+        if key in extras and "error" not in extras[key]:
+            s[key] = {"us_per_step": pick(extras, key, "us_per_step"), "value": pick(extras, key, "value"),
+                      "vs_fp64_step": us_step / extras[key]["us_per_step"],
+                      "depth_rel_max_wet": pick(extras, key, "error_vs_fp64", "rel_max")}
+    if "persistent" in extras and "error" not in extras["persistent"]:
+        s["persistent"] = {m: {"two_kernel_us": pick(extras, "persistent", m, "us_per_step_two_kernel"),
+                               "persistent_us": pick(extras, "persistent", m, "us_per_step_persistent"),
+                               "bit_identical": pick(extras, "persistent", m, "bit_identical")}
+                           for m in ("c207k", "dambreak") if m in extras["persistent"]}
+    if "ensemble" in extras and "error" not in extras["ensemble"]:
+        s["ensemble"] = {"split_vs_fp64": pick(extras, "ensemble", "split_vs_fp64"),
+                         "split_value": pick(extras, "ensemble", "split", "value"),
+                         "split_vs_plain_fp64_step": (pick(extras, "ensemble", "split", "value") or 0)
+                         / (cells / (us_step * 1e-6)),
+                         "split_error": pick(extras, "ensemble", "split", "error_vs_fp64")}
+    if "adjoint" in extras and "error" not in extras["adjoint"]:
+        s["adjoint"] = {"ratio_to_forward": pick(extras, "adjoint", "ratio_to_forward"),
+                        "forward_ms": pick(extras, "adjoint", "forward_ms")}
+    if "dambreak" in extras and "error" not in extras["dambreak"]:
+        s["dambreak"] = {k: pick(extras, "dambreak", k) for k in
+                         ("fp64_us_per_step", "split_us_per_step", "fp32_us_per_step", "split_vs_fp64")}
+        s["dambreak"]["fp64_frac"] = pick(extras, "dambreak", "fp64_roofline", "frac")
+        s["dambreak"]["split_normwise_steps_100_400"] = pick(extras, "dambreak", "error_vs_fp64",
+                                                             "max_over_compares", "normwise_steps_100_400")
+    if "halo" in extras and "error" not in extras["halo"]:
+        s["halo"] = {k: (v.get("us_per_step") if isinstance(v, dict) else v) for k, v in extras["halo"].items()
+                     if k.startswith("parts_") or k == "whole_us_per_step"}
+    if "refgpu" in extras and "error" not in extras["refgpu"]:
+        g = extras["refgpu"]
+        s["reference_gpu"] = {k: g.get(k) for k in ("sync_us_per_step", "async_us_per_step", "graph_us_per_step")}
+        if g.get("graph_us_per_step"):
+            s["reference_gpu"]["speedup_vs_reference_graph"] = g["graph_us_per_step"] / us_step
+    return s
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -611,7 +714,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--extras", default="all",
-                    choices=["all", "none", "ensemble", "adjoint", "split", "fp32", "dambreak", "halo", "persistent"])
+                    choices=["all", "none", "ensemble", "adjoint", "split", "fp32", "dambreak", "halo", "persistent",
+                             "refgpu"])
     ap.add_argument("--only-extras", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=1000)
     ap.add_argument("--ensemble-steps", type=int, default=1000)
@@ -640,7 +744,9 @@ def main():
             dist.barrier()
 
     K, W, G = args.steps, args.warmup, max(1, min(args.graph_steps, args.steps))
-    total_steps = W + K + args.e2e_steps + 20
+    # boundary tables long enough for the main run and for every addition
+    # stepped on this deck (split / fp32 / persistent: up to 910 steps)
+    total_steps = max(W + K + args.e2e_steps + 20, EXTRA_STEPS_207K + 100)
     d, root = make_deck(total_steps, f"r{rank}")
     deck = hb.Deck(root)
     C = deck.cells
@@ -654,7 +760,8 @@ def main():
                 "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
                 "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells),
                 "halo": lambda: halo_leg(local, ncells=args.dambreak_cells, rank=rank, world=world),
-                "persistent": lambda: persistent_leg(deck, local, dambreak_cells=args.dambreak_cells)}
+                "persistent": lambda: persistent_leg(deck, local, dambreak_cells=args.dambreak_cells),
+                "refgpu": lambda: reference_gpu_leg(root, C)}
         if world > 1 and args.extras not in ("ensemble", "halo"):
             raise SystemExit("--only-extras on several GPUs runs the ensemble or the halo leg (--extras ensemble|halo)")
         out = {k: fn() for k, fn in legs.items() if args.extras in ("all", k)}
@@ -772,7 +879,8 @@ def main():
                 "adjoint": lambda: adjoint_leg(local, args.adjoint_steps),
                 "dambreak": lambda: dambreak_leg(local, ncells=args.dambreak_cells),
                 "halo": lambda: halo_leg(local, ncells=args.dambreak_cells),
-                "persistent": lambda: persistent_leg(deck, local, dambreak_cells=args.dambreak_cells)}
+                "persistent": lambda: persistent_leg(deck, local, dambreak_cells=args.dambreak_cells),
+                "refgpu": lambda: reference_gpu_leg(root, C)}
         for name, fn in legs.items():
             if args.extras in ("all", name):
                 try:
@@ -812,6 +920,8 @@ def main():
             "gpu_launches_e2e": launches_e2e,
             "cpu_baseline": cpu,
         }
+        if extras:
+            line["summary"] = summarize(extras, step_ms * 1e3, C)
         line.update(extras)
         print(json.dumps(line), flush=True)
     if world > 1:

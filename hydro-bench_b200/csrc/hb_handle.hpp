@@ -56,8 +56,9 @@ struct hb_handle {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_steps = 0;
     int launch_config = 0;           // index into LAUNCH_CONFIGS
-    // persistent handles: the grid-barrier arrival counter, the resident CTAs of
-    // the cooperative launch (0 = not yet queried), and the barrier wait bound
+    // persistent handles: the grid-barrier words {arrival count, give-up flag}
+    // (both zeroed before each launch), the resident CTAs of the cooperative
+    // launch (0 = not yet queried), and the barrier wait bound
     unsigned *d_bar = nullptr;
     int persist_blocks = 0;
     unsigned long long barrier_limit_ns = 1000000000ull;

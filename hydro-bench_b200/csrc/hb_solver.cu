@@ -618,11 +618,20 @@ int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
 
 // Persistent handles: the whole sequence as cooperative launches of the
 // default edge shape (128 threads, 6 CTAs per SM), as many CTAs as are
-// resident at once, each launch preceded by zeroing its barrier counter.
-// Sequences of more than PERSIST_MAX_STEPS steps take several launches (the
-// arrival count stays within 32 bits); the extra flux writes at the end of
-// each launch leave the same final fluxes.
+// resident at once, each launch preceded by zeroing its barrier words.
+// A launch takes at most PERSIST_MAX_STEPS steps, and fewer where its grid
+// is larger: every step adds 2 x grid arrivals to the 32-bit arrival count,
+// which must stay below 2^32 (phantom arrivals included) so that no barrier
+// target wraps.  Longer sequences take several launches; the extra flux
+// writes at the end of each launch leave the same final fluxes.
 constexpr int PERSIST_THREADS = 128, PERSIST_MINB = 6, PERSIST_MAX_STEPS = 1 << 20;
+
+// Steps one cooperative launch of `grid` CTAs may take (>= 1).
+inline int persist_steps_per_launch(unsigned grid, unsigned phantom) {
+    const unsigned long long room = 0xFFFFFFFFull - phantom;
+    const unsigned long long k = room / (2ull * std::max(1u, grid) + 1ull);
+    return (int)std::max(1ull, std::min(k, (unsigned long long)PERSIST_MAX_STEPS));
+}
 
 template <class A, int VARIANT, bool SEG>
 int launch_persistent_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
@@ -647,9 +656,10 @@ int launch_persistent_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) 
     cfg.stream = st;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    const int kmax = persist_steps_per_launch(cfg.gridDim.x, h->barrier_phantom);
     for (int done = 0; done < n;) {
-        const int k = std::min(n - done, PERSIST_MAX_STEPS);
-        HB_CUDA_RET(cudaMemsetAsync(h->d_bar, 0, sizeof(unsigned), st));
+        const int k = std::min(n - done, kmax);
+        HB_CUDA_RET(cudaMemsetAsync(h->d_bar, 0, 2 * sizeof(unsigned), st));
         HB_CUDA_RET(cudaLaunchKernelEx(&cfg, kernel, m, k, nflux, ncell, h->d_bar, h->barrier_phantom,
                                        h->barrier_limit_ns));
         // the step counter advances per launch: the next launch's steps follow on
@@ -833,7 +843,7 @@ extern "C" int hb_create_batch(const hb_mesh_desc *meshes, int32_t n, const hb_o
     h->launch_config = config_for(opt.layout, opt.tile_config);
     int st;
     if ((st = dev_alloc(h, &h->d_err, 1)) != HB_OK || (st = dev_alloc(h, &h->d_ctr, 1)) != HB_OK ||
-        (st = dev_alloc(h, &h->d_bar, 1)) != HB_OK) {
+        (st = dev_alloc(h, &h->d_bar, 2)) != HB_OK) {
         delete h;
         return st;
     }

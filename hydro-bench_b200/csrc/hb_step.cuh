@@ -516,16 +516,19 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // poll is an L2 round trip (>= 0.3 us), so this many polls last >= 10 s.
 constexpr unsigned BARRIER_MAX_POLLS = 1u << 25;
 
-// Grid-wide barrier of a cooperative launch.  *bar counts CTA arrivals since
-// the launch began (the host zeroes it before each launch); a barrier returns
-// once `target` arrivals are counted.  The wait is bounded: after limit_ns of
-// the global timer (or BARRIER_MAX_POLLS polls), or as soon as another CTA has
-// given up, it sets ERRBIT_BARRIER and returns false, and the caller's CTA
-// leaves the kernel, so a barrier that cannot complete ends the launch with a
-// status instead of a hang.  Ordering is the grid-sync pattern: the CTA's
-// writes are ordered before thread 0's arrival by __syncthreads and a device
-// fence, and thread 0's fence after it saw the count orders the CTA's later
-// reads after every arrived CTA's writes.
+// Grid-wide barrier of a cooperative launch.  bar[0] counts CTA arrivals
+// since the launch began and bar[1] is the launch's give-up flag (the host
+// zeroes both before each launch); a barrier returns once `target` arrivals
+// are counted.  The wait is bounded: after limit_ns of the global timer (or
+// BARRIER_MAX_POLLS polls), or as soon as another CTA of this launch has given
+// up, it raises the flag and the sticky ERRBIT_BARRIER (which hb_sync reports)
+// and returns false, and the caller's CTA leaves the kernel, so a barrier that
+// cannot complete ends the launch with a status instead of a hang.  The flag
+// is per launch, so an error bit left by an earlier launch (or restored from
+// a checkpoint) does not end later launches.  Ordering is the grid-sync
+// pattern: the CTA's writes are ordered before thread 0's arrival by
+// __syncthreads and a device fence, and thread 0's fence after it saw the
+// count orders the CTA's later reads after every arrived CTA's writes.
 __device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned target, uint32_t *err,
                                              unsigned long long limit_ns) {
     __shared__ int ok;
@@ -541,8 +544,9 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned target, uin
                 seen = *(volatile unsigned *)bar;
                 if (seen >= target) break;
                 if ((polls & 15u) == 0) {
-                    const bool other_gave_up = (*(volatile uint32_t *)err & ERRBIT_BARRIER) != 0;
+                    const bool other_gave_up = *(volatile unsigned *)(bar + 1) != 0u;
                     if (other_gave_up || global_ns() - t0 > limit_ns || polls >= BARRIER_MAX_POLLS) {
+                        atomicExch(bar + 1, 1u);
                         atomicOr(err, ERRBIT_BARRIER);
                         good = 0;
                         break;

@@ -569,17 +569,25 @@ def write_deck(deck: Deck, root: str, *, cpu_solver_layout: bool = False) -> str
     return root
 
 
-def write_cpu_solver_deck(deck: Deck, root: str, steps: int) -> str:
+def write_cpu_solver_deck(deck: Deck, root: str, steps: int, open_boundaries: bool = False) -> str:
     """Deck for timing ``hydro-cal-fortan/calculate.cpp`` over ``steps`` steps.
 
     That solver runs every step of every table interval
     (``calculate.cpp:1163-1186``), so the deck is one interval of ``steps``
     steps. Its discharge/level table code is undefined behaviour for NQ > 0
     (``QZSTIME2`` never sized, ``calculate.cpp:1089-1096``) and indexes the
-    ZT/QT tables transposed (``calculate.cpp:1165-1175``), so the open
-    boundaries become walls: same mesh, same per-cell work, no tables.
+    ZT/QT tables transposed (``calculate.cpp:1165-1175``).  With
+    ``open_boundaries`` the deck keeps the mesh's boundary codes and tables,
+    for the solver built with the minimal patch of ``oracle/calc_patch.sed``;
+    otherwise the open boundaries become walls (same mesh, same per-cell
+    work, no tables) for the unpatched solver.
     """
     d = dataclasses.replace(deck)
+    d.mdt = int(round(steps * deck.dt))
+    d.ndays = 1
+    if open_boundaries:
+        write_deck(d, root, cpu_solver_layout=True)
+        return root
     klas = deck.klas.copy()
     klas[(klas != 0)] = KLAS_WALL
     d.klas = klas

@@ -89,7 +89,11 @@ int hb_ref_take_device_errors(uint32_t *bits);
  *   launched.
  * - The first call on a device looks up the array's device address
  *   (cudaGetSymbolAddress) with that device current; make that first call
- *   before any stream capture.
+ *   before any stream capture.  The address is kept for the life of the
+ *   process, so do not use this entry point on a device after
+ *   cudaDeviceReset (or any other teardown of its primary context): the
+ *   module, and with it the array, is loaded anew there and the kept address
+ *   no longer points at it.
  * - Every call shares the one array: calls whose work overlaps on the GPU
  *   (other streams, other threads) race on it.  Each call writes every term it
  *   later reads, so nothing needs clearing between calls.

@@ -1,7 +1,7 @@
 # Builds the reference's own programs from their sources where they lie, into
 # oracle/_ref/ (git-ignored; travels with the tree to the GPU host).
 #
-#   make -f oracle/ref.mk REF=/root/reference
+#   make -f oracle/ref.mk REF=<reference checkout>
 #
 # hot-path binaries (the reference's dump/timing driver, cuda_native_impl/benchmark.cu):
 #   ref_h64  cuda_native_impl/{benchmark.cu,hydro-cal-src}                  variant H, fp64
@@ -11,10 +11,21 @@
 # with the flags of each tree's build.sh (-O3 -rdc=true, default fmad; only
 # fp32_src/build.sh adds --fmad=false) and -arch=sm_100a in place of sm_80.
 #
-# CPU solver: hydro-cal-fortan/calculate.cpp, g++ -O3, no source change; it
-# reads ./origin/changjiangkou/ relative to its working directory.
-REF ?= /root/reference
+# CPU solver: hydro-cal-fortan/calculate.cpp, g++ -O3.
+#   calculate       no source change; reads ./origin/changjiangkou/ relative
+#                   to its working directory.
+#   calculate_open  the same source with the documented minimal patch applied
+#                   by oracle/calc_patch.sed to a copy under oracle/_ref/ (the
+#                   reference tree is never written): the discharge series
+#                   buffers are sized before they are filled and the day-table
+#                   indices are put in [cell][day] order with the last day
+#                   clamped, so decks with open boundaries (NQ, NZ > 0) run
+#                   without undefined behaviour.
+ifndef REF
+$(error REF is not set: make -f oracle/ref.mk REF=<reference checkout>)
+endif
 OUT := $(dir $(lastword $(MAKEFILE_LIST)))_ref
+HERE := $(dir $(lastword $(MAKEFILE_LIST)))
 NVCC ?= nvcc
 ARCH ?= sm_100a
 CNI := $(REF)/cuda_native_impl
@@ -27,7 +38,7 @@ $(OUT)/$(1): $$(wildcard $(2)/benchmark.cu $(2)/hydro-cal-src/src/* $(2)/hydro-c
 	    $(2)/hydro-cal-src/src/cell.cpp $(2)/hydro-cal-src/src/side.cpp -o $$@ -lcudadevrt
 endef
 
-all: $(OUT)/ref_h64 $(OUT)/ref_f64 $(OUT)/ref_h32 $(OUT)/ref_f32 $(OUT)/calculate
+all: $(OUT)/ref_h64 $(OUT)/ref_f64 $(OUT)/ref_h32 $(OUT)/ref_f32 $(OUT)/calculate $(OUT)/calculate_open
 
 $(eval $(call ref_bin,ref_h64,$(CNI),))
 $(eval $(call ref_bin,ref_f64,$(CNI)/baselines/native_cuda_v0/fp64,))
@@ -37,5 +48,9 @@ $(eval $(call ref_bin,ref_f32,$(CNI)/baselines/native_cuda_v0/fp32,))
 $(OUT)/calculate: $(REF)/hydro-cal-fortan/calculate.cpp
 	@mkdir -p $(OUT)
 	g++ -O3 -std=c++17 -w -I$(REF)/hydro-cal-fortan $< -o $@
+
+$(OUT)/calculate_open: $(REF)/hydro-cal-fortan/calculate.cpp $(HERE)calc_patch.sed
+	@mkdir -p $(OUT)
+	sed -f $(HERE)calc_patch.sed $< | g++ -O3 -std=c++17 -w -I$(REF)/hydro-cal-fortan -x c++ - -o $@
 
 .PHONY: all

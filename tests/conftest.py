@@ -46,6 +46,24 @@ def deck_dir(tmp_path_factory):
     return out
 
 
+REF_DECKS = ("ref_f1", "ref_f2_24k")
+
+
+@pytest.fixture(scope="session")
+def ref_deck_dir(tmp_path_factory):
+    """The reference's own shipped decks (tests/golden/<name>.tar.xz, packed by
+    tests/golden/pack_ref_decks.py), unpacked once per session; name -> directory."""
+    import tarfile
+    base = tmp_path_factory.mktemp("ref_decks")
+    out = {}
+    for name in REF_DECKS:
+        path = str(base / name)
+        with tarfile.open(os.path.join(GOLDEN, name + ".tar.xz"), "r:xz") as tar:
+            tar.extractall(path, filter="data")
+        out[name] = path
+    return out
+
+
 @pytest.fixture(scope="session")
 def manifest():
     import json

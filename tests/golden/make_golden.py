@@ -22,6 +22,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -52,7 +53,8 @@ def run_ref(binary: str, deck_dir: str, steps: int, dump: str) -> None:
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
-    ap.add_argument("--work", default=os.path.join(ROOT, "_work", "golden_decks"))
+    ap.add_argument("--work", default=os.path.join(tempfile.gettempdir(), "hb_golden_decks"),
+                    help="where the decks and the reference's dumps are written")
     ap.add_argument("--only", default="")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)

@@ -32,6 +32,38 @@ def test_reader_matches_oracle_reader(deck_dir, name):
     assert d.mesh.steps_per_day == int(o.scalars["mdt"] / o.scalars["dt"])
 
 
+@pytest.mark.parametrize("name", ["ref_f1", "ref_f2_24k"])
+def test_reader_on_the_reference_decks(ref_deck_dir, name):
+    """The reference's own shipped decks (data/F1_text with the F1_native_data
+    time files, data/F2_24K_text) load through hb_deck_load unchanged and give
+    the oracle reader's arrays bit for bit; the fixtures are the packed bytes."""
+    import hashlib
+    import json
+    with open(os.path.join(ROOT, "tests", "golden", "ref_decks.json")) as f:
+        pinned = json.load(f)[name]
+    h = hashlib.sha256()
+    root = ref_deck_dir[name]
+    files = sorted(os.path.relpath(os.path.join(dp, fn), root) for dp, _, fns in os.walk(root) for fn in fns)
+    for rel in files:
+        h.update(rel.encode())
+        with open(os.path.join(root, rel), "rb") as f:
+            h.update(f.read())
+    assert len(files) == pinned["files"] and h.hexdigest() == pinned["sha256"]
+    d = hb.Deck(root)
+    o = O.OracleDeck(root)
+    for k in ARRAYS:
+        a, b = d.array(k), o.arr(k)
+        assert a.shape == b.shape and np.array_equal(a, b), k
+    st = d.state()
+    for k in "HUVZW":
+        assert np.array_equal(st[k], o.arr(k.lower())), k
+    klas = d.array("klas")
+    counts = {int(v): int((klas == v).sum()) for v in np.unique(klas)}
+    expect = {"ref_f1": {0: 25972, 4: 708, 10: 8, 13: 12}, "ref_f2_24k": {0: 94332, 1: 169, 4: 1579}}[name]
+    assert counts == expect
+    assert d.cells == {"ref_f1": 6675, "ref_f2_24k": 24020}[name]
+
+
 def test_reader_missing_file_is_io_error(deck_dir, tmp_path):
     root = tmp_path / "broken"
     shutil.copytree(deck_dir["stress_a"], root)

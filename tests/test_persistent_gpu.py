@@ -147,6 +147,34 @@ def test_persistent_barrier_timeout_is_a_status(deck_dir):
     _same_run(one, two, "after a timed-out launch")
 
 
+def test_persistent_handle_steps_again_after_a_timeout(deck_dir):
+    """The give-up flag is per launch: after a launch timed out, the same
+    handle (its sticky error bit still set, so hb_sync keeps reporting the
+    timeout) runs its next launches to the end once the phantom arrival is
+    gone, bit for bit like the two-kernel sequence from the same state."""
+    deck = hb.Deck(deck_dir["stress_a"])
+    s = hb.Solver(deck, persistent=True)
+    s.set_barrier_limit(20_000_000, phantom_arrivals=1)
+    s.step(2)
+    with pytest.raises(hb.HydroError):
+        s.sync()
+    s.set_barrier_limit(1_000_000_000, phantom_arrivals=0)
+    st = deck.state()
+    s.set_position(0)
+    s.set_state(st["H"], st["U"], st["V"], st["Z"], st["W"])
+    t0 = time.perf_counter()
+    s.step(6)
+    with pytest.raises(hb.HydroError) as e:
+        s.sync()
+    assert e.value.status == 5 and time.perf_counter() - t0 < 5.0
+    two = hb.Solver(deck)
+    two.step(6)
+    two.sync()
+    a, b = s.get_state(), two.get_state()
+    for k in "HUVZW":
+        assert _bits_equal(a[k], b[k]), k
+
+
 def test_persistent_handle_arguments(deck_dir):
     deck = hb.Deck(deck_dir["stress_a"])
     s = hb.Solver(deck, persistent=True)

@@ -47,6 +47,26 @@ def test_static_step_matches_existing_entry_points(deck_dir, name, variant):
     assert hb.take_ref_device_errors() == 0
 
 
+def test_static_step_takes_no_device_memory(deck_dir):
+    """The property the entry point exists for: once the library is loaded and
+    the first call has looked up the array's address, further calls change
+    the device's free memory by nothing (every other buffer here is the
+    caller's, allocated before the measurement)."""
+    import torch
+    lib = _lib.lib()
+    deck = hb.Deck(deck_dir["f1"])
+    new = hb.RefLayoutMesh(deck)
+    stream = torch.cuda.current_stream().cuda_stream
+    _lib.check(lib.hb_ref_step_static(C.byref(new.view), 1, 0, 0, stream))
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for kt in range(2, 12):
+        _lib.check(lib.hb_ref_step_static(C.byref(new.view), kt, 0, 0, stream))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_static_step_rejects_meshes_beyond_capacity():
     view = _lib.RefMeshView()
     view.CELL = _lib.REF_STEP_STATIC_MAX_CELLS + 1
