@@ -746,7 +746,7 @@ def main():
     K, W, G = args.steps, args.warmup, max(1, min(args.graph_steps, args.steps))
     # boundary tables long enough for the main run and for every addition
     # stepped on this deck (split / fp32 / persistent: up to 910 steps)
-    total_steps = max(W + K + args.e2e_steps + 20, EXTRA_STEPS_207K + 100)
+    total_steps = max(max(W, G) + K + args.e2e_steps + 20, EXTRA_STEPS_207K + 100)
     d, root = make_deck(total_steps, f"r{rank}")
     deck = hb.Deck(root)
     C = deck.cells
@@ -774,11 +774,12 @@ def main():
     solver = hb.Solver(deck, precision=args.precision, device=local)
     stream = torch.cuda.current_stream()
     solver.capture_graph(G, stream)
-    # warm-up
+    # warm-up: at least W steps and at least one replay of the captured graph
+    # (its first launch uploads it to the device, which is not step time)
     done = 0
-    while done + G <= W:
+    while done + G <= W or done == 0:
         solver.graph_launch(stream); done += G
-    if W - done:
+    if W - done > 0:
         solver.step(W - done, stream)
     torch.cuda.synchronize()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")

@@ -18,7 +18,7 @@ OBJ_DIR = os.path.join(HERE, "_build")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["hb_solver.cu", "hb_ref_layout.cu", "hb_adjoint.cu"]
+CU_SOURCES = ["hb_solver.cu", "hb_tiles.cu", "hb_ref_layout.cu", "hb_adjoint.cu"]
 CPP_SOURCES = ["hb_deck.cpp"]
 
 

@@ -223,6 +223,14 @@ void tile_partition(int C, const std::vector<int32_t> &nbr4, int T, std::vector<
 
 namespace {
 
+// a and b have the same bit pattern (so -0.0 differs from +0.0)
+bool same_bits(double a, double b) {
+    uint64_t x, y;
+    std::memcpy(&x, &a, sizeof x);
+    std::memcpy(&y, &b, sizeof y);
+    return x == y;
+}
+
 // Host image of the device mesh of every scenario, concatenated.
 template <class A>
 struct HostMesh {
@@ -234,6 +242,8 @@ struct HostMesh {
     std::vector<int4> rix;
     std::vector<uint8_t> rmeta;
     std::vector<R> rgeo;
+    std::vector<uint32_t> rloc;               // tile layout: staged-kernel local indices per record
+    std::vector<int32_t> halo;                // tile layout: every tile's halo cells (device indices)
     std::vector<int32_t> bcell;               // global table row, -1 = none
     // one entry per table row: the row's values for each interval of its scenario
     std::vector<std::vector<R>> qt, dqt;
@@ -339,6 +349,7 @@ int append_scenario(const hb_mesh_desc *md, int scn, const hb_options &opt, hb::
     sc.slot_index.assign(S, -1);
     sc.npairs = 0;
     sc.tiles.clear();
+    std::vector<int32_t> halo_mark(opt.layout == HB_LAYOUT_TILE ? C : 0, -1), halo_slot(halo_mark.size(), 0);
     for (size_t t = 0; t + 1 < starts.size(); t++) {
         hb::TileDesc td{scn, c0 + starts[t], starts[t + 1] - starts[t], (int)hm.rix.size(), 0, 0};
         for (int i = starts[t]; i < starts[t + 1]; i++) {
@@ -354,9 +365,12 @@ int append_scenario(const hb_mesh_desc *md, int scn, const hb_options &opt, hb::
                 if (jb < 0) continue;
                 const size_t sb = 4 * (size_t)nb + jb;
                 const size_t oa = slot_of(i, j), ob = slot_of(nb, jb);
-                // the two slots must see one edge: code 0 both, negated normal, same length
-                if ((meta4[sb] & hb::META_CODE) != hb::CODE_ZERO || !real4[sb] || md->cosf[ob] != -md->cosf[oa] ||
-                    md->sinf[ob] != -md->sinf[oa] || md->side[ob] != md->side[oa])
+                // the two slots must see one edge: code 0 both, negated normal, same
+                // length, bit for bit (a zero component must have the opposite sign
+                // too: the mirrored side is evaluated with the negated normal, and a
+                // wrongly signed zero changes the sign of zero results)
+                if ((meta4[sb] & hb::META_CODE) != hb::CODE_ZERO || !real4[sb] || !same_bits(md->cosf[ob], -md->cosf[oa]) ||
+                    !same_bits(md->sinf[ob], -md->sinf[oa]) || !same_bits(md->side[ob], md->side[oa]))
                     continue;
                 paired[sn] = paired[sb] = 1;
                 push(i, nb, sn, (long long)sb, meta4[sn], oa);
@@ -371,6 +385,36 @@ int append_scenario(const hb_mesh_desc *md, int scn, const hb_options &opt, hb::
                 push(i, nbr4[sn], sn, -1, meta4[sn], slot_of(i, j));
                 td.nsingles++;
             }
+        }
+        if (opt.layout == HB_LAYOUT_TILE) {
+            // local indices of the staged tile kernel: the tile's own cells,
+            // then its halo (neighbours outside the tile, first use first)
+            td.halo0 = (int)hm.halo.size();
+            const int t0 = starts[t], tn = starts[t + 1] - starts[t];
+            if (tn > hb::LOC_MAX_CELL + 1)
+                return hb::set_error(HB_E_INVALID, "tile of %d cells: the staged tile kernel takes at most %d", tn,
+                                     hb::LOC_MAX_CELL + 1);
+            auto local = [&](int cell) -> uint32_t {   // scenario-local device cell -> staged index
+                if (tile_of[cell] == (int32_t)t) return (uint32_t)(cell - t0);
+                if (halo_mark[cell] != (int32_t)t) {
+                    halo_mark[cell] = (int32_t)t;
+                    halo_slot[cell] = tn + (int)(hm.halo.size() - td.halo0);
+                    hm.halo.push_back(c0 + cell);
+                }
+                return (uint32_t)halo_slot[cell];
+            };
+            for (size_t r = td.rec0; r < hm.rix.size(); r++) {
+                const int4 ix = hm.rix[r];
+                const int a = ix.x - c0, b = ix.y < 0 ? -1 : ix.y - c0;
+                const uint32_t la = (uint32_t)(a - t0), ja = (uint32_t)(ix.z - 4 * ix.x);
+                const uint32_t lb = b < 0 ? hb::LOC_NONE : local(b);
+                const uint32_t jb = ix.w < 0 ? 0u : (uint32_t)(ix.w - 4 * ix.y);
+                if (lb != hb::LOC_NONE && lb >= hb::LOC_NONE)
+                    return hb::set_error(HB_E_INVALID, "tile with a halo of %d cells: too large for the staged tile kernel",
+                                         (int)(hm.halo.size() - td.halo0));
+                hm.rloc.push_back(hb::loc_pack(la, lb, ja, jb));
+            }
+            td.nhalo = (int)hm.halo.size() - td.halo0;
         }
         sc.npairs += td.npairs;
         sc.tiles.push_back(td);
@@ -480,6 +524,13 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *mds, int n, hb::DevMesh<
         TRY(dev_upload(h, &rp, hm.rgeo)); m.rgeo = rp;
     }
     TRY(dev_upload(h, &up, hm.rmeta)); m.rmeta = up;
+    m.rloc = nullptr;
+    m.halo = nullptr;
+    if (h->opt.layout == HB_LAYOUT_TILE) {
+        uint32_t *lp32;
+        TRY(dev_upload(h, &lp32, hm.rloc)); m.rloc = lp32;
+        if (!hm.halo.empty()) { TRY(dev_upload(h, &ip, hm.halo)); m.halo = ip; }
+    }
     TRY(dev_upload(h, &ip, hm.bcell)); m.bcell = ip;
     TRY(dev_upload(h, &rp, bqt)); m.bqt = rp;
     TRY(dev_upload(h, &rp, bdqt)); m.bdqt = rp;
@@ -537,11 +588,13 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *mds, int n, hb::DevMesh<
         std::vector<hb::TileDesc> tiles;
         m.max_tile_cells = 1;
         m.max_tile_pairs = 1;
+        m.max_tile_halo = 0;
         for (const auto &sc : h->scn)
             for (const auto &td : sc.tiles) {
                 tiles.push_back(td);
                 m.max_tile_cells = std::max(m.max_tile_cells, td.cells);
                 m.max_tile_pairs = std::max(m.max_tile_pairs, td.npairs);
+                m.max_tile_halo = std::max(m.max_tile_halo, td.nhalo);
             }
         m.ntiles = (int)tiles.size();
         hb::TileDesc *tp;
@@ -669,60 +722,6 @@ int launch_persistent_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) 
     return HB_OK;
 }
 
-size_t tile_smem_bytes(int max_cells, int max_pairs, size_t real_size) {
-    return 16 * real_size * (size_t)max_cells + sizeof(int) * (size_t)max_pairs;
-}
-
-// Calls f(kernel, threads) with the tile kernel of a tile-layout launch shape.
-template <class A, int VARIANT, class F>
-int with_tile_kernel(int config, F &&f) {
-    using namespace hb;
-    switch (config) {
-    case 8: return f(tile_kernel<A, VARIANT, 256, 3>, 256);
-    case 9: return f(tile_kernel<A, VARIANT, 256, 2>, 256);
-    case 10: return f(tile_kernel<A, VARIANT, 128, 6>, 128);
-    case 11: return f(tile_kernel<A, VARIANT, 128, 4>, 128);
-    case 12: return f(tile_kernel<A, VARIANT, 512, 1>, 512);
-    default: return f(tile_kernel<A, VARIANT, 256, 4>, 256);
-    }
-}
-
-template <class A, int VARIANT>
-int launch_tiles_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3((unsigned)std::max(1, m.ntiles));
-    cfg.stream = st;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cfg.dynamicSmemBytes = tile_smem_bytes(m.max_tile_cells, m.max_tile_pairs, sizeof(typename A::real));
-    const int rc = with_tile_kernel<A, VARIANT>(h->launch_config, [&](auto kernel, int threads) -> int {
-        cfg.blockDim = dim3(threads);
-        for (int k = 0; k < n; k++) HB_CUDA_RET(cudaLaunchKernelEx(&cfg, kernel, m, k, (int)(k == n - 1)));
-        return HB_OK;
-    });
-    if (rc != HB_OK) return rc;
-    return launch_tick(h, n, st);
-}
-
-// Lets every tile kernel of the handle's policy use the shared memory its
-// largest tile needs (beyond the 48 KB default).
-template <class A, int VARIANT>
-int set_tile_smem(const hb::DevMesh<A> &m) {
-    const size_t bytes = tile_smem_bytes(m.max_tile_cells, m.max_tile_pairs, sizeof(typename A::real));
-    for (int c = 0; c < hb::N_LAUNCH_CONFIGS; c++) {
-        if (hb::LAUNCH_CONFIGS[c].layout != hb::LAYOUT_TILE) continue;
-        const int rc = with_tile_kernel<A, VARIANT>(c, [&](auto kernel, int) -> int {
-            HB_CUDA_RET(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-            return HB_OK;
-        });
-        if (rc != HB_OK) return rc;
-    }
-    return HB_OK;
-}
-
 int enqueue_steps(hb_handle *h, int n, cudaStream_t st) {
     if (n <= 0) return HB_OK;
     const bool f = h->opt.variant == HB_VARIANT_F;
@@ -730,7 +729,7 @@ int enqueue_steps(hb_handle *h, int n, cudaStream_t st) {
     const bool tiles = h->opt.layout == HB_LAYOUT_TILE;
     return h->with_mesh([&](auto &m) {
         using A = typename std::remove_reference<decltype(m)>::type::Policy;
-        if (tiles) return f ? launch_tiles_t<A, 1>(h, m, n, st) : launch_tiles_t<A, 0>(h, m, n, st);
+        if (tiles) return hb_tiles_launch(h, n, st);
         if (h->opt.persistent) {
             if (seg) return f ? launch_persistent_t<A, 1, true>(h, m, n, st) : launch_persistent_t<A, 0, true>(h, m, n, st);
             return f ? launch_persistent_t<A, 1, false>(h, m, n, st) : launch_persistent_t<A, 0, false>(h, m, n, st);
@@ -762,6 +761,7 @@ int check_range(hb_handle *h, long long n) {
 }  // namespace
 
 int hb_enqueue_steps(hb_handle *h, int n, cudaStream_t st) { return enqueue_steps(h, n, st); }
+int hb_launch_tick(hb_handle *h, int n, cudaStream_t st) { return launch_tick(h, n, st); }
 int hb_check_range(hb_handle *h, long long n) { return check_range(h, n); }
 
 int hb_forward_step_into(hb_handle *h, long long t0, int k, const double *in, double *out, double *terms,
@@ -848,11 +848,7 @@ extern "C" int hb_create_batch(const hb_mesh_desc *meshes, int32_t n, const hb_o
         return st;
     }
     st = h->with_mesh([&](auto &m) { return build_device_mesh(h, meshes, n, m); });
-    if (st == HB_OK && opt.layout == HB_LAYOUT_TILE)
-        st = h->with_mesh([&](auto &m) {
-            using A = typename std::remove_reference<decltype(m)>::type::Policy;
-            return opt.variant == HB_VARIANT_F ? set_tile_smem<A, 1>(m) : set_tile_smem<A, 0>(m);
-        });
+    if (st == HB_OK && opt.layout == HB_LAYOUT_TILE) st = hb_tiles_set_smem(h);
     if (st != HB_OK) { delete h; return st; }
     *out = h;
     return HB_OK;
@@ -1160,6 +1156,9 @@ extern "C" int hb_set_tile_config(hb_handle *h, int32_t tile_config) {
     if (c < 0) return hb::set_error(HB_E_INVALID, "tile_config %d is no shape of this handle's layout", tile_config);
     if (h->opt.persistent && c != hb::DEFAULT_EDGE_CONFIG)
         return hb::set_error(HB_E_INVALID, "a persistent handle keeps the default launch shape");
+    if (hb::config_staged(c) && !h->staged_ok)
+        return hb::set_error(HB_E_INVALID, "tile_config %d: the staged tile kernel's shared memory exceeds a CTA's "
+                             "on this mesh", tile_config);
     if (c != h->launch_config) h->drop_graph();
     h->launch_config = c;
     return HB_OK;
@@ -1223,6 +1222,7 @@ extern "C" int hb_autotune(hb_handle *h, int32_t steps, void *stream, float *ms_
     for (int c = 0; rc == HB_OK && c < hb::N_LAUNCH_CONFIGS; c++) {
         if (ms_per_step && c < capacity) ms_per_step[c] = 0.f;
         if (hb::LAUNCH_CONFIGS[c].layout != h->opt.layout) continue;
+        if (hb::config_staged(c) && !h->staged_ok) continue;
         h->launch_config = c;
         if ((rc = copy_all(false)) != HB_OK) break;
         if ((rc = enqueue_steps(h, 1, st)) != HB_OK) break;

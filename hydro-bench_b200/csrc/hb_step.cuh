@@ -21,14 +21,21 @@ enum : uint8_t { META_CODE = 0x0F, META_OWN_FIRST = 0x10, META_HAS_NB = 0x20 };
 // Launch shapes.  Edge layout: the flux kernel's threads per CTA and CTAs per
 // SM asked of the compiler through __launch_bounds__ (which caps registers
 // per thread), and the cell kernel's CTAs per SM (it has UPDATE_THREADS
-// threads).  Tile layout: the tile kernel's threads per CTA and CTAs per SM.
+// threads).  Tile layout: the tile kernel's threads per CTA and CTAs per SM,
+// and in the last field 1 for the staged tile kernel (cell states staged in
+// shared memory), 0 for the tile kernel that gathers them from global memory.
 enum Layout : int { LAYOUT_EDGE = HB_LAYOUT_EDGE, LAYOUT_TILE = HB_LAYOUT_TILE };
 struct LaunchConfig { int layout, threads, min_blocks, update_min_blocks; };
 constexpr LaunchConfig LAUNCH_CONFIGS[] = {
     {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 8}, {LAYOUT_EDGE, 128, 8, 8}, {LAYOUT_EDGE, 256, 3, 6},
     {LAYOUT_EDGE, 256, 4, 8}, {LAYOUT_EDGE, 128, 4, 6}, {LAYOUT_EDGE, 256, 2, 6}, {LAYOUT_EDGE, 64, 12, 8},
     {LAYOUT_TILE, 256, 3, 0}, {LAYOUT_TILE, 256, 2, 0}, {LAYOUT_TILE, 128, 6, 0}, {LAYOUT_TILE, 128, 4, 0},
-    {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0}};
+    {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0},
+    {LAYOUT_TILE, 256, 3, 1}, {LAYOUT_TILE, 128, 6, 1}, {LAYOUT_TILE, 256, 2, 1}, {LAYOUT_TILE, 384, 2, 1},
+    {LAYOUT_TILE, 512, 1, 1}, {LAYOUT_TILE, 128, 4, 1}};
+constexpr bool config_staged(int c) {
+    return LAUNCH_CONFIGS[c].layout == LAYOUT_TILE && LAUNCH_CONFIGS[c].update_min_blocks == 1;
+}
 constexpr int N_LAUNCH_CONFIGS = sizeof(LAUNCH_CONFIGS) / sizeof(LAUNCH_CONFIGS[0]);
 constexpr int DEFAULT_EDGE_CONFIG = 0;
 constexpr int DEFAULT_TILE_CONFIG = 8;
@@ -36,8 +43,23 @@ constexpr int UPDATE_THREADS = 128;
 
 // One tile of the tile layout: a compact group of cells, contiguous in the
 // device order, with its records (mirror pairs inside the tile, then every
-// other real slot of its cells).
-struct TileDesc { int scn, cell0, cells, rec0, npairs, nsingles; };
+// other real slot of its cells) and its halo: the cells outside the tile that
+// its single records have as neighbours, halo[halo0 .. halo0 + nhalo).
+struct TileDesc { int scn, cell0, cells, rec0, npairs, nsingles, halo0, nhalo; };
+
+// A record's cells as indices into its tile's staged states (the tile's own
+// cells 0 .. cells-1, then its halo), with the slot numbers within the cells:
+// bits 0-11 own cell, 12-24 neighbour (LOC_NONE: no neighbour), 25-26 the
+// own cell's slot j, 27-28 (pairs) the neighbour's slot.
+constexpr int LOC_MAX_CELL = 0xFFF;
+constexpr uint32_t LOC_NONE = 0x1FFF;
+__host__ __device__ inline uint32_t loc_pack(uint32_t la, uint32_t lb, uint32_t ja, uint32_t jb) {
+    return la | (lb << 12) | (ja << 25) | (jb << 27);
+}
+struct Loc { int la, lb, ja, jb; };
+__device__ __forceinline__ Loc loc_unpack(uint32_t x) {
+    return {(int)(x & 0xFFFu), (int)((x >> 12) & 0x1FFFu), (int)((x >> 25) & 3u), (int)((x >> 27) & 3u)};
+}
 
 // Constants of one scenario of a batch (the only entry for a single mesh).
 struct ScnParams {
@@ -96,7 +118,9 @@ struct DevMesh {
     int rev_update;
     // tile layout
     const TileDesc *tiles;     // [ntiles]
-    int ntiles, max_tile_cells, max_tile_pairs;
+    int ntiles, max_tile_cells, max_tile_pairs, max_tile_halo;
+    const uint32_t *rloc;      // [nrecords] loc_pack of each record (tile layout)
+    const int32_t *halo;       // the tiles' halo cells, concatenated (tile layout)
 };
 
 struct StepIndex { int par, kt, jt; };
@@ -187,21 +211,20 @@ __device__ __forceinline__ void store_flux(const DevMesh<A> &m, int s, const typ
 }
 
 // One slot on its own: flux_slot with its boundary tables (functors.cu:47-202).
+// single_core takes the slot's cell a (device order, for its table row), its
+// slot sa, both cells' states and the record's code byte and geometry.
 template <class A, int VARIANT, class T>
-__device__ __forceinline__ void single_record(const DevMesh<A> &m, int r, const StepIndex &si,
-                                              const StepParams &p, int write_flux, const T &tout) {
+__device__ __forceinline__ void single_core(const DevMesh<A> &m, int r, int a, int sa, const CellStateA<A> &own,
+                                            const CellStateA<A> &nb, uint8_t meta, const Vec4<typename A::real> &g,
+                                            const StepIndex &si, const StepParams &p, int write_flux, const T &tout) {
     using R = typename A::real;
-    const int4 ix = m.rix[r];
-    const int a = ix.x, b = ix.y, sa = ix.z;
-    const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
     using L = typename A::level;
     SlotInA<A> in;
-    in.own = load_cell(m, si.par, a);
-    const uint8_t meta = m.rmeta[r];
+    in.own = own;
     in.code = (int8_t)(meta & META_CODE);
     in.own_first = meta & META_OWN_FIRST;
     in.has_nb = meta & META_HAS_NB;
-    in.nb = in.has_nb ? load_cell(m, si.par, b) : CellStateA<A>{R(0), R(0), R(0), L(0), L(0)};
+    in.nb = nb;
     in.cosj = g.x; in.sinj = g.y; in.side = g.z;
     auto fetch = [&]() {
         BoundaryInA<A> bi;
@@ -233,15 +256,28 @@ __device__ __forceinline__ void single_record(const DevMesh<A> &m, int r, const 
     if (o.undefined) atomicOr(m.err, ERRBIT_UNDEFINED);
 }
 
-// The mirrored Osher of a pair computed on its own (when its inputs differ
-// from the direct route's in the normal velocity).
-template <class A, class T>
-__device__ __forceinline__ void pair_mirror(const DevMesh<A> &m, int r, const StepIndex &si,
-                                            const StepParams &p, int write_flux, const T &tout) {
+template <class A, int VARIANT, class T>
+__device__ __forceinline__ void single_record(const DevMesh<A> &m, int r, const StepIndex &si,
+                                              const StepParams &p, int write_flux, const T &tout) {
     using R = typename A::real;
+    using L = typename A::level;
     const int4 ix = m.rix[r];
     const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
-    const CellStateA<A> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
+    const uint8_t meta = m.rmeta[r];
+    const CellStateA<A> own = load_cell(m, si.par, ix.x);
+    const CellStateA<A> nb =
+        (meta & META_HAS_NB) ? load_cell(m, si.par, ix.y) : CellStateA<A>{R(0), R(0), R(0), L(0), L(0)};
+    single_core<A, VARIANT>(m, r, ix.x, ix.z, own, nb, meta, g, si, p, write_flux, tout);
+}
+
+// The mirrored Osher of a pair computed on its own (when its inputs differ
+// from the direct route's in the normal velocity); mirror_core takes the
+// pair's cells a (direct side) and b, its geometry and b's slot sb.
+template <class A, class T>
+__device__ __forceinline__ void mirror_core(const DevMesh<A> &m, const CellStateA<A> &A_, const CellStateA<A> &B_,
+                                            const Vec4<typename A::real> &g, int sb, const StepParams &p,
+                                            int write_flux, const T &tout) {
+    using R = typename A::real;
     const R cs = g.x, sn = g.y;
     const R clA = A::sqrt(A::mul(A::c(9.81), A_.h));
     const OsherIn<R> oi = osher_inputs<A>(A_, B_, cs, sn, clA, true, p);
@@ -251,8 +287,18 @@ __device__ __forceinline__ void pair_mirror(const DevMesh<A> &m, int r, const St
     fb[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, oi.ur);
     fb[2] = fo[2];
     fb[3] = mirror_f3<A>(fo[3], A_.zbc, B_.zbc);
-    if (write_flux) store_flux(m, ix.w, fb);
-    store_terms<A>(tout, ix.w, fb, g.z, -cs, -sn);
+    if (write_flux) store_flux(m, sb, fb);
+    store_terms<A>(tout, sb, fb, g.z, -cs, -sn);
+}
+
+template <class A, class T>
+__device__ __forceinline__ void pair_mirror(const DevMesh<A> &m, int r, const StepIndex &si,
+                                            const StepParams &p, int write_flux, const T &tout) {
+    using R = typename A::real;
+    const int4 ix = m.rix[r];
+    const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
+    const CellStateA<A> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
+    mirror_core<A>(m, A_, B_, g, ix.w, p, write_flux, tout);
 }
 
 template <class R>
@@ -269,13 +315,15 @@ __device__ __forceinline__ bool same_bits(R a, R b) {
 // the b side's FLUX2 is re-summed with its own tangent if only that differs;
 // otherwise the pair goes to the CTA's queue, whose mirrored Osher
 // evaluations run together after the main pass (pair_mirror).
+// pair_core takes both cells' states, the geometry of a's slot and the two
+// slots sa, sb; a pair whose mirrored Osher must run on its own is queued as
+// record r.
 template <class A, int VARIANT, class T>
-__device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const StepIndex &si, const StepParams &p,
-                                            int write_flux, const T &tout, int *queue, int *qn) {
+__device__ __forceinline__ void pair_core(const DevMesh<A> &m, int r, const CellStateA<A> &A_,
+                                          const CellStateA<A> &B_, const Vec4<typename A::real> &g, int sa, int sb,
+                                          const StepParams &p, int write_flux, const T &tout, int *queue, int *qn) {
     using R = typename A::real;
-    const int4 ix = m.rix[r];
-    const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
-    const CellStateA<A> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
+    const int4 ix = make_int4(0, 0, sa, sb);
     const R cs = g.x, sn = g.y;
     const R clA = A::sqrt(A::mul(A::c(9.81), A_.h));
     auto nofetch = []() { return BoundaryInA<A>{}; };
@@ -338,6 +386,16 @@ __device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const St
     }
 }
 
+template <class A, int VARIANT, class T>
+__device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const StepIndex &si, const StepParams &p,
+                                            int write_flux, const T &tout, int *queue, int *qn) {
+    using R = typename A::real;
+    const int4 ix = m.rix[r];
+    const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
+    const CellStateA<A> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
+    pair_core<A, VARIANT>(m, r, A_, B_, g, ix.z, ix.w, p, write_flux, tout, queue, qn);
+}
+
 // Flux of every record of one step.  Single mesh (SEG = false): records
 // [0, npairs) are mirror pairs and the rest single slots, one per thread.
 // Batch (SEG = true): CTA b takes the scenario and record range of fseg[b].
@@ -383,14 +441,15 @@ __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k
 // zero-length fourth slot of a triangle is evaluated here without pow
 // (flux_slot's ZERO_LEN), exactly when fluxes are written out.
 // SMEM_TERMS: `terms` is in shared memory (tile layout), else global.
+// update_core takes the cell's stored state record `raw` and bed `zbc`.
 template <class A, int VARIANT, bool COEF = false, bool SMEM_TERMS = false>
-__device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const StepIndex &si, const StepParams &p,
-                                           int write_flux, const typename A::real *terms) {
+__device__ __forceinline__ void update_core(const DevMesh<A> &m, int c, const Vec4<typename A::real> &raw,
+                                            typename A::level zbc, const StepIndex &si, const StepParams &p,
+                                            int write_flux, const typename A::real *terms) {
     using R = typename A::real;
     using L = typename A::level;
-    const Vec4<R> raw = ldg4(m.S[si.par] + 4 * (size_t)c);
     CellStateA<A> st;
-    st.h = raw.x; st.u = raw.y; st.v = raw.z; st.zbc = m.zbc[c];
+    st.h = raw.x; st.u = raw.y; st.v = raw.z; st.zbc = zbc;
     if constexpr (is_split<A>::value) st.z = split_level<A>(raw.x, raw.w, st.zbc);
     else st.z = raw.w;
     const unsigned mask = m.cmask[c];
@@ -442,6 +501,13 @@ __device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const Ste
     else stg4(m.S[np] + 4 * (size_t)c, o.h, o.u, o.v, o.z);
     m.W[c] = o.w;
     if (!(isfinite((double)o.h) && isfinite((double)o.u) && isfinite((double)o.v))) atomicOr(m.err, ERRBIT_NONFINITE);
+}
+
+template <class A, int VARIANT, bool COEF = false, bool SMEM_TERMS = false>
+__device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const StepIndex &si, const StepParams &p,
+                                           int write_flux, const typename A::real *terms) {
+    const Vec4<typename A::real> raw = ldg4(m.S[si.par] + 4 * (size_t)c);
+    update_core<A, VARIANT, COEF, SMEM_TERMS>(m, c, raw, m.zbc[c], si, p, write_flux, terms);
 }
 
 // Every cell of one step.  Single mesh: a grid-stride loop over the cells.
@@ -501,6 +567,89 @@ __global__ void __launch_bounds__(THREADS, MINB) tile_kernel(DevMesh<A> m, int k
     __syncthreads();
     for (int c = threadIdx.x; c < td.cells; c += THREADS)
         update_one<A, VARIANT, false, true>(m, td.cell0 + c, si, p, write_flux, terms + 16 * c);
+}
+
+// Shared memory of the staged tile kernel, in this order: the slot terms
+// [cells][4 slots][4] R; the staged state records [cells + halo][4] R; the
+// staged beds [cells + halo] L; the mirrored-Osher queue [pairs] int.
+template <class A>
+__host__ __device__ inline size_t staged_smem_bytes(int cells, int halo, int pairs) {
+    using R = typename A::real;
+    using L = typename A::level;
+    return 16 * sizeof(R) * (size_t)cells + (4 * sizeof(R) + sizeof(L)) * (size_t)(cells + halo) +
+           sizeof(int) * (size_t)pairs;
+}
+
+// The whole step of one tile with its cells' states staged in shared memory.
+// The CTA first copies the state records and beds of the tile's own cells
+// (contiguous: coalesced 256-bit loads) and of its halo cells into shared
+// memory; every record then takes both of its cells from there through the
+// local indices of m.rloc, so no record waits on a dependent global gather.
+// The rest is tile_kernel's sequence: records (pairs, then singles) write
+// their slot terms into shared memory, the queued mirrored Osher evaluations
+// run, and each cell of the tile sums its four slots in order and is updated
+// from its staged state.  Same arithmetic as every other form, so the same
+// bits.
+template <class A, int VARIANT, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) staged_tile_kernel(DevMesh<A> m, int k, int write_flux) {
+    using R = typename A::real;
+    using L = typename A::level;
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    const int cap = m.max_tile_cells + m.max_tile_halo;
+    R *terms = reinterpret_cast<R *>(tile_smem);                        // [max cells][16]
+    R *sst = terms + 16 * (size_t)m.max_tile_cells;                     // [cap][4]
+    L *szb = reinterpret_cast<L *>(sst + 4 * (size_t)cap);              // [cap]
+    int *queue = reinterpret_cast<int *>(szb + cap);                    // [max pairs]
+    __shared__ int qn;
+    const TileDesc td = m.tiles[blockIdx.x];   // constant tables: read before the dependency wait
+    const ScnParams sp = m.scn[td.scn];
+    if (threadIdx.x == 0) qn = 0;
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
+    const StepIndex si = step_index(m, k, sp.per_day, sp.ndays);
+    const StepParams p{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
+    const R *S = m.S[si.par];
+    const int nown = td.cells, nall = td.cells + td.nhalo;
+    for (int i = threadIdx.x; i < nall; i += THREADS) {
+        const int c = i < nown ? td.cell0 + i : m.halo[td.halo0 + (i - nown)];
+        const Vec4<R> v = ldg4(S + 4 * (size_t)c);
+        st4(sst + 4 * i, v.x, v.y, v.z, v.w);
+        szb[i] = m.zbc[c];
+    }
+    __syncthreads();
+    auto cell = [&](int i) -> CellStateA<A> {
+        const Vec4<R> v = ld4(sst + 4 * i);
+        const L zbc = szb[i];
+        if constexpr (is_split<A>::value) return {v.x, v.y, v.z, split_level<A>(v.x, v.w, zbc), zbc};
+        else return {v.x, v.y, v.z, v.w, zbc};
+    };
+    const Terms<R, true> tout{terms, 4 * td.cell0};
+    const int nrec = td.npairs + td.nsingles;
+    for (int i = threadIdx.x; i < nrec; i += THREADS) {
+        const int r = td.rec0 + i;
+        const Loc l = loc_unpack(m.rloc[r]);
+        const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
+        const int a = td.cell0 + l.la;
+        if (i < td.npairs) {
+            pair_core<A, VARIANT>(m, r, cell(l.la), cell(l.lb), g, 4 * a + l.ja, 4 * (td.cell0 + l.lb) + l.jb, p,
+                                  write_flux, tout, queue, &qn);
+        } else {
+            const uint8_t meta = m.rmeta[r];
+            const CellStateA<A> nb = l.lb != (int)LOC_NONE ? cell(l.lb) : CellStateA<A>{R(0), R(0), R(0), L(0), L(0)};
+            single_core<A, VARIANT>(m, r, a, 4 * a + l.ja, cell(l.la), nb, meta, g, si, p, write_flux, tout);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < qn; i += THREADS) {
+        const int r = queue[i];
+        const Loc l = loc_unpack(m.rloc[r]);
+        const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
+        mirror_core<A>(m, cell(l.la), cell(l.lb), g, 4 * (td.cell0 + l.lb) + l.jb, p, write_flux, tout);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < td.cells; c += THREADS)
+        update_core<A, VARIANT, false, true>(m, td.cell0 + c, ld4(sst + 4 * c), szb[c], si, p, write_flux,
+                                             terms + 16 * c);
 }
 
 // ---------------------------------------------------------------------------
