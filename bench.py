@@ -490,12 +490,23 @@ def reference_gpu_leg(root: str, cells: int, steps: int = EXTRA_STEPS_207K, repe
            "cells": cells, "steps": steps, "repeat": repeat,
            "timing": "reference driver's own: median of repeat runs, host wall clock (benchmark.cu:172-266)",
            "wall_s": time.perf_counter() - t0}
-    for mode in ("Sync", "Async", "Graph"):
-        m = re.search(rf"^{mode}:\s*median=([0-9.]+) ms,\s*([0-9.]+) us/step", r.stdout, re.M)
-        if m:
-            us = float(m.group(2))
-            out[f"{mode.lower()}_us_per_step"] = us
-            out[f"{mode.lower()}_value"] = cells / (us * 1e-6)
+    def parse(text, prefix):
+        for mode in ("Sync", "Async", "Graph"):
+            m = re.search(rf"^{mode}:\s*median=([0-9.]+) ms,\s*([0-9.]+) us/step", text, re.M)
+            if m:
+                us = float(m.group(2))
+                out[f"{prefix}{mode.lower()}_us_per_step"] = us
+                out[f"{prefix}{mode.lower()}_value"] = cells / (us * 1e-6)
+
+    parse(r.stdout, "")
+    # the same driver linked against this library in place of functors.cu
+    # (oracle/ref.mk's ref_dropin): the drop-in path's own speed
+    dropin = os.path.join(ROOT, "oracle", "_ref", "ref_dropin")
+    if os.path.exists(dropin):
+        r = subprocess.run([dropin, str(steps), str(repeat)], cwd=run, capture_output=True, text=True, timeout=900)
+        if r.returncode == 0:
+            parse(r.stdout, "dropin_")
+            out["dropin"] = "the same driver, functors.cu replaced by libhydrob200.so (CalculateFlux / UpdateCell)"
     out["unit"] = METRIC
     return out
 
@@ -697,7 +708,8 @@ def summarize(extras: dict, us_step: float, cells: int) -> dict:
                      if k.startswith("parts_") or k == "whole_us_per_step"}
     if "refgpu" in extras and "error" not in extras["refgpu"]:
         g = extras["refgpu"]
-        s["reference_gpu"] = {k: g.get(k) for k in ("sync_us_per_step", "async_us_per_step", "graph_us_per_step")}
+        s["reference_gpu"] = {k: g.get(k) for k in ("sync_us_per_step", "async_us_per_step", "graph_us_per_step",
+                                                     "dropin_graph_us_per_step")}
         if g.get("graph_us_per_step"):
             s["reference_gpu"]["speedup_vs_reference_graph"] = g["graph_us_per_step"] / us_step
     return s

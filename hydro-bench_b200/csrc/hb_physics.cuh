@@ -350,10 +350,13 @@ __device__ __forceinline__ void osher(typename A::real cl, const typename A::rea
     const bool p6 = any && (k2 == 4 ? k1 <= 2 : k1 >= 3);
     const bool n6 = k2 != 4;                                   // piece 6 subtracted
     const bool p7 = any && k1 >= 3;
+    // Every piece is evaluated only where its case takes it: pieces 2, 3, 5
+    // and 6 divide, and subcritical flow mostly takes 3 or 5 alone; pieces 1
+    // and 7 (supercritical flow out of a side) are rare, so a warp usually
+    // skips them altogether.
     // piece 1: QF(QL)
-    qf_acc_if<A>(out, p1, false, ql[0], ql[1], ql[2], tr, 0);
-    // Pieces 2, 3, 5 and 6 divide; each is evaluated only where its case
-    // takes it (subcritical flow mostly takes 3 or 5 alone).
+    if (p1) qf_acc_if<A>(out, true, false, ql[0], ql[1], ql[2], tr, 0);
+    else qf_skip<A>(tr, 0);
     // piece 2: US = FIL/3, HS = US^2/9.81
     if (p2) {
         R us = A::divk(fil, 3.0);
@@ -388,7 +391,8 @@ __device__ __forceinline__ void osher(typename A::real cl, const typename A::rea
         qf_skip<A>(tr, 4);
     }
     // piece 7: QF(QR)
-    qf_acc_if<A>(out, p7, false, qr[0], qr[1], qr[2], tr, 5);
+    if (p7) qf_acc_if<A>(out, true, false, qr[0], qr[1], qr[2], tr, 5);
+    else qf_skip<A>(tr, 5);
 }
 
 // ---------------------------------------------------------------------------

@@ -471,6 +471,17 @@ __device__ __forceinline__ void update_core(const DevMesh<A> &m, int c, const Ve
             wu = A::add(wu, t[j].y);
             wv = A::add(wv, t[j].z);
         } else {
+            // A zero-length slot adds SIDE*F0 = 0*F0 to WH and 0*(...) to WU and
+            // WV.  For a finite state (h > 0) its fluxes are finite, so each
+            // addend is a zero and leaves a non-zero partial sum unchanged bit
+            // for bit: the slot is then skipped.  Only a zero partial sum (whose
+            // sign the addend may change) or a non-finite state takes the full
+            // evaluation, as does the last step of a sequence, which writes the
+            // slot's fluxes.
+            if (!write_flux && wh != R(0) && wu != R(0) && wv != R(0) && st.h > R(0) &&
+                isfinite((double)st.h) && isfinite((double)st.u) && isfinite((double)st.v) &&
+                isfinite((double)st.z) && isfinite((double)st.zbc))
+                continue;
             SlotInA<A> in;
             in.own = st;
             in.nb = {R(0), R(0), R(0), L(0), L(0)};

@@ -54,6 +54,7 @@ def lib():
         l.orc_update.argtypes = [C.POINTER(_Deck), C.c_int]
         l.orc_run.argtypes = [C.POINTER(_Deck), C.c_int, C.c_int, C.c_int]
         l.orc_run.restype = C.c_int
+        l.orc_set_iterations.argtypes = [C.c_int, C.POINTER(C.c_byte)]
         if l.orc_deck_sizeof() != C.sizeof(_Deck):
             raise RuntimeError("oracle struct layout mismatch")
         _lib = l
@@ -117,6 +118,50 @@ class OracleDeck:
         done = lib().orc_run(C.byref(self._d), self.variant, self.step_index, n)
         self.step_index += done
         return done
+
+    def gauge_rollout(self, n, zbc, Z0, U0, V0, gauges, obs_every: int, nsteps: int, counts=None,
+                      mode: int = 0) -> np.ndarray:
+        """The adjoint's rollout restated: from the level Z0 and velocities
+        (initial depth as mesh.cpp:350-361: H = Z0 - ZBC where the level is
+        above the bed, else H = HM1 and Z = ZBC + HM1), Manning n (FNC = 9.81
+        n^2, mesh.cpp:364) and bed ZBC (ZB1 = ZBC + HM1), nsteps steps of the
+        driver's loop from step 0; returns the gauge depths after every
+        obs_every steps [nobs][ngauges].
+
+        Iteration counts of the boundary fixed points (orc_set_iterations):
+        mode 1 records them into counts [nsteps][4*cells] (int8), mode 2
+        replays them, mode 0 runs the reference's stopping tests."""
+        d = self._d
+        hm1 = d.hm1
+        zbc = np.asarray(zbc, np.float64)
+        Z0 = np.asarray(Z0, np.float64)
+        self.arr("fnc")[:] = 9.81 * np.asarray(n, np.float64) * np.asarray(n, np.float64)
+        self.arr("zbc")[:] = zbc
+        self.arr("zb1")[:] = zbc + hm1
+        dry = Z0 <= zbc
+        self.arr("h")[:] = np.where(dry, hm1, Z0 - zbc)
+        self.arr("z")[:] = np.where(dry, zbc + hm1, Z0)
+        self.arr("u")[:] = U0
+        self.arr("v")[:] = V0
+        for f in ("f0", "f1", "f2", "f3"):
+            self.arr(f)[:] = 0.0
+        self.step_index = 0
+        g = np.asarray(gauges, dtype=np.int64)
+        out = []
+        h = self.arr("h")
+        try:
+            for t in range(nsteps):
+                if mode:
+                    row = np.ascontiguousarray(counts[t])
+                    lib().orc_set_iterations(mode, row.ctypes.data_as(C.POINTER(C.c_byte)))
+                self.run(1)
+                if mode == 1:
+                    counts[t] = row
+                if (t + 1) % obs_every == 0:
+                    out.append(h[g].copy())
+        finally:
+            lib().orc_set_iterations(0, None)
+        return np.array(out)
 
     def dump(self) -> Dict[str, np.ndarray]:
         """The arrays of a reference ``--dump`` (benchmark.cu:141-162), copied."""

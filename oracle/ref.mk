@@ -38,12 +38,25 @@ $(OUT)/$(1): $$(wildcard $(2)/benchmark.cu $(2)/hydro-cal-src/src/* $(2)/hydro-c
 	    $(2)/hydro-cal-src/src/cell.cpp $(2)/hydro-cal-src/src/side.cpp -o $$@ -lcudadevrt
 endef
 
-all: $(OUT)/ref_h64 $(OUT)/ref_f64 $(OUT)/ref_h32 $(OUT)/ref_f32 $(OUT)/calculate $(OUT)/calculate_open
+all: $(OUT)/ref_h64 $(OUT)/ref_f64 $(OUT)/ref_h32 $(OUT)/ref_f32 $(OUT)/ref_dropin $(OUT)/calculate $(OUT)/calculate_open
 
 $(eval $(call ref_bin,ref_h64,$(CNI),))
 $(eval $(call ref_bin,ref_f64,$(CNI)/baselines/native_cuda_v0/fp64,))
 $(eval $(call ref_bin,ref_h32,$(CNI)/fp32_src,--fmad=false))
 $(eval $(call ref_bin,ref_f32,$(CNI)/baselines/native_cuda_v0/fp32,))
+
+# The link-level drop-in: the reference's own driver and host code
+# (benchmark.cu, mesh.cpp, cell.cpp, side.cpp) built exactly as build.sh builds
+# them but with functors.cu left out, linked against libhydrob200.so, which
+# exports CalculateFlux / UpdateCell with the reference's mangled names
+# (functors.cuh:59-65).  The library is found next to the tree at run time.
+LIBDIR := $(abspath $(HERE)../hydro-bench_b200/hydrob200)
+$(OUT)/ref_dropin: $(CNI)/benchmark.cu $(LIBDIR)/libhydrob200.so
+	@mkdir -p $(OUT)
+	$(NVCC) -O3 -arch=$(ARCH) -rdc=true --std=c++17 -I$(CNI)/hydro-cal-src/include \
+	    $(CNI)/benchmark.cu $(CNI)/hydro-cal-src/src/mesh.cpp $(CNI)/hydro-cal-src/src/cell.cpp \
+	    $(CNI)/hydro-cal-src/src/side.cpp -L$(LIBDIR) -lhydrob200 \
+	    -Xlinker -rpath='$$ORIGIN/../../hydro-bench_b200/hydrob200' -o $@ -lcudadevrt
 
 $(OUT)/calculate: $(REF)/hydro-cal-fortan/calculate.cpp
 	@mkdir -p $(OUT)

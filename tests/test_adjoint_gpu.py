@@ -169,6 +169,60 @@ def test_autograd_function(setup):
     a.close()
 
 
+def test_adjoint_configuration_against_frozen_finite_differences(tmp_path):
+    """The adjoint configuration: 24,020-cell channel, 1000 steps, 50 gauges
+    every 10 steps, observations from n_true = 0.025 exp(0.2 g), gradient at
+    n = 0.025, checkpoint intervals 10, 50 and 100 (bit-identical gradients).
+
+    Directional derivatives g . v for n and ZBC against central differences
+    of the same rollout on the CPU oracle with the boundary fixed points'
+    iteration counts frozen at the base run (oracle gauge_rollout, modes 1/2):
+    the adjoint freezes them too, and without freezing the loss is only
+    piecewise smooth (a stopping test that flips between the two runs of a
+    difference adds a jump).  Bound 1e-6 relative, at two step sizes."""
+    from oracle import oracle as O
+    d, n_true, gauges = D.adjoint_case(steps=1000)
+    root = str(tmp_path / "c24k")
+    D.write_deck(d, root)
+    deck = hb.Deck(root)
+    T, every = 1000, 10
+    st = deck.state()
+    zbc = deck.array("zbc").copy()
+    n0 = np.full(deck.cells, 0.025)
+    grads = []
+    for k in (10, 50, 100):
+        a = Adjoint(deck, gauges, every, T, checkpoint_every=k)
+        a.set_parameters(n_true, zbc)
+        _, obs = a.forward()
+        a.set_observations(obs)
+        a.set_parameters(n0, zbc)
+        a.forward()
+        grads.append(a.backward())
+        a.close()
+    for gn, gz in grads[1:]:
+        np.testing.assert_array_equal(gn, grads[0][0])
+        np.testing.assert_array_equal(gz, grads[0][1])
+    gn, gz = grads[0]
+    o = O.OracleDeck(root)
+    counts = np.zeros((T, 4 * deck.cells), np.int8)
+    o.gauge_rollout(n0, zbc, st["Z"], st["U"], st["V"], gauges, every, T, counts, 1)
+
+    def loss(n, z):
+        g = o.gauge_rollout(n, z, st["Z"], st["U"], st["V"], gauges, every, T, counts, 2)
+        r = g - obs
+        return float(np.sum(r * r))
+
+    rng = np.random.default_rng(7)
+    vn, vz = rng.standard_normal(deck.cells), rng.standard_normal(deck.cells)
+    adj_n, adj_z = float(gn @ vn), float(gz @ vz)
+    for rel in (1e-4, 1e-5):
+        e = rel * 0.025
+        fd_n = (loss(n0 + e * vn, zbc) - loss(n0 - e * vn, zbc)) / (2 * e)
+        fd_z = (loss(n0, zbc + rel * vz) - loss(n0, zbc - rel * vz)) / (2 * rel)
+        assert abs(adj_n - fd_n) <= 1e-6 * abs(fd_n), ("n", rel, adj_n, fd_n)
+        assert abs(adj_z - fd_z) <= 1e-6 * abs(fd_z), ("zbc", rel, adj_z, fd_z)
+
+
 def test_rejects_codes_without_a_reverse(deck_dir):
     deck = hb.Deck(deck_dir["stress_a"])
     with pytest.raises(hb.HydroError):

@@ -147,3 +147,27 @@ def test_breach_reference_reads_uninitialised_depth(deck_dir):
     for k in ("U", "V"):
         assert normwise(d[k][keep], g[k][keep]) <= 1e-14
     assert normwise(d["H"], g["H"]) <= 1e-14
+
+
+def test_frozen_iteration_counts_replay_exactly(deck_dir):
+    """The oracle's gauge rollout with the boundary fixed points' iteration
+    counts recorded (mode 1) and then replayed (mode 2) at the same parameters
+    gives the free run's depths bit for bit; the recorded counts are those of
+    the KLAS 1 / 10 slots only, within the loops' limits."""
+    import hydrob200 as hb
+    deck = hb.Deck(deck_dir["f1"])
+    o = O.OracleDeck(deck_dir["f1"])
+    st = deck.state()
+    n = np.sqrt(deck.array("fnc") / 9.81)
+    zbc = deck.array("zbc").copy()
+    gauges = np.arange(0, deck.cells, 97)
+    T = 40
+    free = o.gauge_rollout(n, zbc, st["Z"], st["U"], st["V"], gauges, 5, T)
+    counts = np.zeros((T, 4 * deck.cells), np.int8)
+    rec = o.gauge_rollout(n, zbc, st["Z"], st["U"], st["V"], gauges, 5, T, counts, 1)
+    rep = o.gauge_rollout(n, zbc, st["Z"], st["U"], st["V"], gauges, 5, T, counts, 2)
+    assert np.array_equal(free, rec) and np.array_equal(free, rep)
+    klas = deck.array("klas")
+    used = np.nonzero(counts.any(axis=0))[0]
+    assert used.size > 0 and set(np.unique(klas[used]).tolist()) <= {1.0, 10.0}
+    assert counts.min() >= 0 and counts.max() <= 30

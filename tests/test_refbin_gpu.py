@@ -107,6 +107,29 @@ def test_fp64_bit_exact_against_the_reference_program(decks, name, binary):
         assert hb.take_ref_device_errors() == 0
 
 
+DROPIN = os.path.join(ROOT, "oracle", "_ref", "ref_dropin")
+
+
+@pytest.mark.skipif(not (os.path.exists(DROPIN) and os.path.exists(REFBIN["h64"])),
+                    reason="link-level drop-in program not built (oracle/ref.mk)")
+@pytest.mark.parametrize("name,steps", [("stress_a", 50), ("f1", 100), ("ref_f1", 50), ("c207k", 50)])
+def test_link_level_dropin_program(decks, deck_dir, name, steps):
+    """The reference's own driver and host code (benchmark.cu, mesh.cpp,
+    cell.cpp, side.cpp) linked against libhydrob200.so in place of
+    functors.cu (oracle/ref.mk's ref_dropin): its --dump equals the unmodified
+    reference program's bit for bit (state, geometry and fluxes)."""
+    root = decks.get(name) or deck_dir[name]
+    run = os.path.join(root, "run")
+    os.makedirs(run, exist_ok=True)
+    out = os.path.join(run, f"dropin_{steps}.bin")
+    r = subprocess.run([DROPIN, str(steps), "1", "--dump", out], cwd=run, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0 and "hydrob200:" not in r.stderr, r.stdout[-1500:] + r.stderr[-1500:]
+    got = read_dump(out, np.float64)
+    ref = ref_dump("h64", root, steps)
+    for k in ref:
+        assert_bits(got[k], ref[k], f"ref_dropin {name}/s{steps}/{k}")
+
+
 @need_ref
 @pytest.mark.parametrize("name,threads,tile_cells", [("c207k", 256, 0), ("c207k", 384, 512), ("ref_f1", 128, 64)])
 def test_staged_tile_kernel_bit_exact_against_the_reference_program(decks, name, threads, tile_cells):
