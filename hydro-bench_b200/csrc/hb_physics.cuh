@@ -259,7 +259,23 @@ __device__ __forceinline__ void qf_acc(typename A::real out[4], typename A::real
 // tangential velocity: f0[i] = h*u of piece i (pieces 1, 2, 3, 5, 6, 7 in that
 // order; 1-3 carry QL's tangent, 5-7 QR's), act/neg bit i = added / subtracted.
 template <class R>
-struct OsherTrace { R f0[6]; unsigned act, neg; };
+struct OsherTrace {
+    R f0[6];
+    unsigned act, neg;
+    __device__ __forceinline__ void set(int i, R v) { f0[i] = v; }
+    __device__ __forceinline__ R get(int i) const { return f0[i]; }
+};
+// The same record with the products kept in memory the caller provides, at
+// p[i * stride] (shared memory: they are read back only for the rare re-summed
+// FLUX2, so they need not occupy registers across the rest of the evaluation).
+template <class R>
+struct OsherTraceAt {
+    R *p;
+    int stride;
+    unsigned act, neg;
+    __device__ __forceinline__ void set(int i, R v) { p[i * stride] = v; }
+    __device__ __forceinline__ R get(int i) const { return p[i * stride]; }
+};
 
 // out += QF(h, u, v) (or -=, `neg`) when `on`, with the reference build's sums
 // (functors.cu:453-497, :505-511); `out` is untouched otherwise.
@@ -277,7 +293,7 @@ __device__ __forceinline__ void qf_acc_if(typename A::real out[4], bool on, bool
     R o3 = A::madd(neg ? -h4 : h4, h, out[3], M_ACC123);
     if (on) { out[0] = o0; out[1] = o1; out[2] = o2; out[3] = o3; }
     if constexpr (!std::is_same<TR, void>::value) {
-        tr->f0[piece] = f0;
+        tr->set(piece, f0);
         tr->act |= (on ? 1u : 0u) << piece;
         tr->neg |= (neg ? 1u : 0u) << piece;
     }
@@ -286,20 +302,20 @@ __device__ __forceinline__ void qf_acc_if(typename A::real out[4], bool on, bool
 // A piece that is not taken: traced as inactive (osher_f2 skips it).
 template <class A, class TR>
 __device__ __forceinline__ void qf_skip(TR *tr, int piece) {
-    if constexpr (!std::is_same<TR, void>::value) tr->f0[piece] = typename A::real(0);
+    if constexpr (!std::is_same<TR, void>::value) tr->set(piece, typename A::real(0));
 }
 
 // FLUX2 of a traced Osher evaluation re-summed with tangents ql2 / qr2, in the
 // same order and with the same fused sums as qf_acc_if.
-template <class A>
-__device__ __forceinline__ typename A::real osher_f2(const OsherTrace<typename A::real> &tr, typename A::real ql2,
-                                                     typename A::real qr2) {
+template <class A, class TR>
+__device__ __forceinline__ typename A::real osher_f2(const TR &tr, typename A::real ql2, typename A::real qr2) {
     using R = typename A::real;
     R acc = R(0);
 #pragma unroll
     for (int i = 0; i < 6; i++) {
         const R v = i < 3 ? ql2 : qr2;
-        const R sf0 = ((tr.neg >> i) & 1u) ? -tr.f0[i] : tr.f0[i];
+        const R f0 = tr.get(i);
+        const R sf0 = ((tr.neg >> i) & 1u) ? -f0 : f0;
         const R o2 = A::madd(sf0, v, acc, M_ACC123);
         if ((tr.act >> i) & 1u) acc = o2;
     }
@@ -766,11 +782,18 @@ __device__ __forceinline__ OsherIn<typename A::real> osher_inputs(const CellStat
     return o;
 }
 
-// FLUX1's correction term and the two routes' epilogues (functors.cu:162-163, :191-199)
+// FLUX1's correction term and the two routes' epilogues (functors.cu:162-163, :191-199).
+// The term does not depend on Osher's result, so a caller may form it first
+// (osher_f1_term) and add it afterwards: the same two roundings.
+template <class A>
+__device__ __forceinline__ typename A::real osher_f1_term(typename A::real ratio, typename A::real hcR,
+                                                          typename A::real ur) {
+    return A::mul(A::mul(A::mul(A::mul(A::sub(A::c(1.0), ratio), hcR), ur), ur), A::c(0.5));
+}
 template <class A>
 __device__ __forceinline__ typename A::real osher_f1(typename A::real fo1, typename A::real ratio,
                                                      typename A::real hcR, typename A::real ur) {
-    return A::add(fo1, A::mul(A::mul(A::mul(A::mul(A::sub(A::c(1.0), ratio), hcR), ur), ur), A::c(0.5)));
+    return A::add(fo1, osher_f1_term<A>(ratio, hcR, ur));
 }
 template <class A>
 __device__ __forceinline__ typename A::real mirror_f3(typename A::real fo3, typename A::level zbcL,

@@ -317,11 +317,16 @@ __device__ __forceinline__ bool same_bits(R a, R b) {
 // evaluations run together after the main pass (pair_mirror).
 // pair_core takes both cells' states, the geometry of a's slot and the two
 // slots sa, sb; a pair whose mirrored Osher must run on its own is queued as
-// record r.
+// record r.  tslot is the thread's shared-memory slot for the Osher trace.
+template <class R>
+struct TraceSlot { R *p; int stride; };   // 8 values at p[i * stride]
+constexpr int TRACE_VALUES = 8;
+
 template <class A, int VARIANT, class T>
 __device__ __forceinline__ void pair_core(const DevMesh<A> &m, int r, const CellStateA<A> &A_,
                                           const CellStateA<A> &B_, const Vec4<typename A::real> &g, int sa, int sb,
-                                          const StepParams &p, int write_flux, const T &tout, int *queue, int *qn) {
+                                          const StepParams &p, int write_flux, const T &tout, int *queue, int *qn,
+                                          const TraceSlot<typename A::real> &tslot) {
     using R = typename A::real;
     const int4 ix = make_int4(0, 0, sa, sb);
     const R cs = g.x, sn = g.y;
@@ -352,48 +357,58 @@ __device__ __forceinline__ void pair_core(const DevMesh<A> &m, int r, const Cell
     }
     if (ra_ | rb_) {
         // the two routes' inputs differ only in QL2, UR and so QR1 (osher_inputs)
-        OsherIn<R> oi = osher_inputs<A>(A_, B_, cs, sn, clA, ra_ == 0, p);
-        const R ql2_d = oi.ql[2], ur_d = oi.ur, qr1_d = oi.qr[1];
-        const R ql2_m = ra_ ? A::dot(A_.v, cs, -A_.u, sn, M_QL2M) : ql2_d;
-        const R ur_m = ra_ ? A::dot(B_.u, cs, B_.v, sn, M_UR1) : ur_d;
+        const OsherIn<R> oi = osher_inputs<A>(A_, B_, cs, sn, clA, ra_ == 0, p);
+        // Everything the epilogues take besides Osher's result is formed first
+        // (same operations, same bits), so that few values stay live across
+        // Osher: FLUX1's correction of each side, whether b's mirrored Osher
+        // equals this one (QR1 agrees), and whether b's FLUX2 must be re-summed
+        // with its own tangent (only QL2 differs; the tangents and the
+        // per-piece products then wait in shared memory).
+        const R ur_m = ra_ ? A::dot(B_.u, cs, B_.v, sn, M_UR1) : oi.ur;
         R qr1_m = A::mul(ur_m, oi.ratio);
         if (oi.hcR <= A::c(p.hm2) || oi.qr[0] <= A::c(p.hm2)) qr1_m = A::copysign(A::c(K::VMIN), ur_m);
+        const bool b_same = rb_ && (!ra_ || same_bits(oi.qr[1], qr1_m));
+        const R ql2_m = ra_ ? A::dot(A_.v, cs, -A_.u, sn, M_QL2M) : oi.ql[2];
+        const bool b_resum = b_same && ra_ && !same_bits(oi.ql[2], ql2_m);
+        const R term_a = osher_f1_term<A>(oi.ratio, oi.hcR, oi.ur);
+        const R term_b = osher_f1_term<A>(oi.ratio, oi.hcR, ur_m);
+        if (b_resum) { tslot.p[6 * tslot.stride] = ql2_m; tslot.p[7 * tslot.stride] = oi.qr[2]; }
+        const typename A::level zbcA = A_.zbc, zbcB = B_.zbc;
         R fo[4];
-        OsherTrace<R> tr;
+        OsherTraceAt<R> tr{tslot.p, tslot.stride, 0u, 0u};
         osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo, &tr);
         if (ra_) {
             R f[4];
             f[0] = fo[0];
-            f[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, ur_d);
+            f[1] = A::add(fo[1], term_a);
             f[2] = fo[2];
             f[3] = fo[3];
             if (write_flux) store_flux(m, ix.z, f);
             store_terms<A>(tout, ix.z, f, g.z, cs, sn);
         }
-        if (rb_) {
-            if (!ra_ || same_bits(qr1_d, qr1_m)) {
-                R f[4];
-                f[0] = -fo[0];
-                f[1] = osher_f1<A>(fo[1], oi.ratio, oi.hcR, ur_m);
-                f[2] = (!ra_ || same_bits(ql2_d, ql2_m)) ? fo[2] : osher_f2<A>(tr, ql2_m, oi.qr[2]);
-                f[3] = mirror_f3<A>(fo[3], A_.zbc, B_.zbc);
-                if (write_flux) store_flux(m, ix.w, f);
-                store_terms<A>(tout, ix.w, f, g.z, -cs, -sn);
-            } else {
-                queue[atomicAdd(qn, 1)] = r;
-            }
+        if (b_same) {
+            R f[4];
+            f[0] = -fo[0];
+            f[1] = A::add(fo[1], term_b);
+            f[2] = b_resum ? osher_f2<A>(tr, tslot.p[6 * tslot.stride], tslot.p[7 * tslot.stride]) : fo[2];
+            f[3] = mirror_f3<A>(fo[3], zbcA, zbcB);
+            if (write_flux) store_flux(m, ix.w, f);
+            store_terms<A>(tout, ix.w, f, g.z, -cs, -sn);
+        } else if (rb_) {
+            queue[atomicAdd(qn, 1)] = r;
         }
     }
 }
 
 template <class A, int VARIANT, class T>
 __device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const StepIndex &si, const StepParams &p,
-                                            int write_flux, const T &tout, int *queue, int *qn) {
+                                            int write_flux, const T &tout, int *queue, int *qn,
+                                            const TraceSlot<typename A::real> &tslot) {
     using R = typename A::real;
     const int4 ix = m.rix[r];
     const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
     const CellStateA<A> A_ = load_cell(m, si.par, ix.x), B_ = load_cell(m, si.par, ix.y);
-    pair_core<A, VARIANT>(m, r, A_, B_, g, ix.z, ix.w, p, write_flux, tout, queue, qn);
+    pair_core<A, VARIANT>(m, r, A_, B_, g, ix.z, ix.w, p, write_flux, tout, queue, qn, tslot);
 }
 
 // Flux of every record of one step.  Single mesh (SEG = false): records
@@ -403,6 +418,8 @@ template <class A, int VARIANT, int THREADS, int MINB, bool SEG>
 __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k, int write_flux) {
     __shared__ int queue[THREADS];
     __shared__ int qn;
+    __shared__ typename A::real trace[TRACE_VALUES * THREADS];
+    const TraceSlot<typename A::real> tslot{trace + threadIdx.x, THREADS};
     if (threadIdx.x == 0) qn = 0;
     int r;
     bool valid, pair;
@@ -430,7 +447,7 @@ __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k
     __syncthreads();
     const Terms<typename A::real> tout{m.slotw, 0};
     if (valid) {
-        if (pair) pair_record<A, VARIANT>(m, r, si, p, write_flux, tout, queue, &qn);
+        if (pair) pair_record<A, VARIANT>(m, r, si, p, write_flux, tout, queue, &qn, tslot);
         else single_record<A, VARIANT>(m, r, si, p, write_flux, tout);
     }
     __syncthreads();
@@ -569,8 +586,10 @@ __global__ void __launch_bounds__(THREADS, MINB) tile_kernel(DevMesh<A> m, int k
     const Terms<R, true> tout{terms, 4 * td.cell0};
     __syncthreads();
     const int nrec = td.npairs + td.nsingles;
+    __shared__ R trace[TRACE_VALUES * THREADS];
+    const TraceSlot<R> tslot{trace + threadIdx.x, THREADS};
     for (int i = threadIdx.x; i < nrec; i += THREADS) {
-        if (i < td.npairs) pair_record<A, VARIANT>(m, td.rec0 + i, si, p, write_flux, tout, queue, &qn);
+        if (i < td.npairs) pair_record<A, VARIANT>(m, td.rec0 + i, si, p, write_flux, tout, queue, &qn, tslot);
         else single_record<A, VARIANT>(m, td.rec0 + i, si, p, write_flux, tout);
     }
     __syncthreads();
@@ -635,6 +654,8 @@ __global__ void __launch_bounds__(THREADS, MINB) staged_tile_kernel(DevMesh<A> m
         else return {v.x, v.y, v.z, v.w, zbc};
     };
     const Terms<R, true> tout{terms, 4 * td.cell0};
+    __shared__ R trace[TRACE_VALUES * THREADS];
+    const TraceSlot<R> tslot{trace + threadIdx.x, THREADS};
     const int nrec = td.npairs + td.nsingles;
     for (int i = threadIdx.x; i < nrec; i += THREADS) {
         const int r = td.rec0 + i;
@@ -643,7 +664,7 @@ __global__ void __launch_bounds__(THREADS, MINB) staged_tile_kernel(DevMesh<A> m
         const int a = td.cell0 + l.la;
         if (i < td.npairs) {
             pair_core<A, VARIANT>(m, r, cell(l.la), cell(l.lb), g, 4 * a + l.ja, 4 * (td.cell0 + l.lb) + l.jb, p,
-                                  write_flux, tout, queue, &qn);
+                                  write_flux, tout, queue, &qn, tslot);
         } else {
             const uint8_t meta = m.rmeta[r];
             const CellStateA<A> nb = l.lb != (int)LOC_NONE ? cell(l.lb) : CellStateA<A>{R(0), R(0), R(0), L(0), L(0)};
@@ -735,6 +756,8 @@ __global__ void __launch_bounds__(THREADS, MINB)
                       unsigned long long limit_ns) {
     __shared__ int queue[THREADS];
     __shared__ int qn;
+    __shared__ typename A::real trace[TRACE_VALUES * THREADS];
+    const TraceSlot<typename A::real> tslot{trace + threadIdx.x, THREADS};
     const Terms<typename A::real> tout{m.slotw, 0};
     unsigned arrivals = 0;
     for (int k = 0; k < n; k++) {
@@ -763,7 +786,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
             if ((int)threadIdx.x < cnt) {
                 const int r = r0 + (int)threadIdx.x;
                 const bool pair = SEG ? seg_pairs : r < m.npairs;
-                if (pair) pair_record<A, VARIANT>(m, r, si, p, wf, tout, queue, &qn);
+                if (pair) pair_record<A, VARIANT>(m, r, si, p, wf, tout, queue, &qn, tslot);
                 else single_record<A, VARIANT>(m, r, si, p, wf, tout);
             }
             __syncthreads();
