@@ -56,7 +56,6 @@ struct hb_handle {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_steps = 0;
     int launch_config = 0;           // index into LAUNCH_CONFIGS
-    bool staged_ok = false;          // tile layout: the staged tile kernel's shared memory fits a CTA
     // persistent handles: the grid-barrier words {arrival count, give-up flag}
     // (both zeroed before each launch), the resident CTAs of the cooperative
     // launch (0 = not yet queried), and the barrier wait bound
@@ -128,7 +127,7 @@ int hb_enqueue_steps(hb_handle *h, int n, cudaStream_t st);
 int hb_check_range(hb_handle *h, long long n);
 int hb_launch_tick(hb_handle *h, int n, cudaStream_t st);
 // the tile layout (hb_tiles.cu): n steps at the handle's launch shape, and the
-// shared-memory attributes of its tile kernels (sets staged_ok)
+// shared-memory attributes of its tile kernels
 int hb_tiles_launch(hb_handle *h, int n, cudaStream_t st);
 int hb_tiles_set_smem(hb_handle *h);
 // One fp64 edge-layout step t0 + k (the device step counter must hold t0)

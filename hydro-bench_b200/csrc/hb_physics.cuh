@@ -265,16 +265,16 @@ struct OsherTrace {
     __device__ __forceinline__ void set(int i, R v) { f0[i] = v; }
     __device__ __forceinline__ R get(int i) const { return f0[i]; }
 };
-// The same record with the products kept in memory the caller provides, at
-// p[i * stride] (shared memory: they are read back only for the rare re-summed
-// FLUX2, so they need not occupy registers across the rest of the evaluation).
-template <class R>
-struct OsherTraceAt {
-    R *p;
-    int stride;
+// The same record with the products kept in a store the caller provides
+// (TS: set(i, v) / get(i)), e.g. shared memory: they are read back only for
+// the rare re-summed FLUX2, so they need not occupy registers across the rest
+// of the evaluation.
+template <class TS>
+struct OsherTraceIn {
+    TS *ts;
     unsigned act, neg;
-    __device__ __forceinline__ void set(int i, R v) { p[i * stride] = v; }
-    __device__ __forceinline__ R get(int i) const { return p[i * stride]; }
+    template <class R> __device__ __forceinline__ void set(int i, R v) { ts->set(i, v); }
+    __device__ __forceinline__ auto get(int i) const { return ts->get(i); }
 };
 
 // out += QF(h, u, v) (or -=, `neg`) when `on`, with the reference build's sums

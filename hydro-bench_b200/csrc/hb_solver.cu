@@ -242,8 +242,6 @@ struct HostMesh {
     std::vector<int4> rix;
     std::vector<uint8_t> rmeta;
     std::vector<R> rgeo;
-    std::vector<uint32_t> rloc;               // tile layout: staged-kernel local indices per record
-    std::vector<int32_t> halo;                // tile layout: every tile's halo cells (device indices)
     std::vector<int32_t> bcell;               // global table row, -1 = none
     // one entry per table row: the row's values for each interval of its scenario
     std::vector<std::vector<R>> qt, dqt;
@@ -349,7 +347,6 @@ int append_scenario(const hb_mesh_desc *md, int scn, const hb_options &opt, hb::
     sc.slot_index.assign(S, -1);
     sc.npairs = 0;
     sc.tiles.clear();
-    std::vector<int32_t> halo_mark(opt.layout == HB_LAYOUT_TILE ? C : 0, -1), halo_slot(halo_mark.size(), 0);
     for (size_t t = 0; t + 1 < starts.size(); t++) {
         hb::TileDesc td{scn, c0 + starts[t], starts[t + 1] - starts[t], (int)hm.rix.size(), 0, 0};
         for (int i = starts[t]; i < starts[t + 1]; i++) {
@@ -385,36 +382,6 @@ int append_scenario(const hb_mesh_desc *md, int scn, const hb_options &opt, hb::
                 push(i, nbr4[sn], sn, -1, meta4[sn], slot_of(i, j));
                 td.nsingles++;
             }
-        }
-        if (opt.layout == HB_LAYOUT_TILE) {
-            // local indices of the staged tile kernel: the tile's own cells,
-            // then its halo (neighbours outside the tile, first use first)
-            td.halo0 = (int)hm.halo.size();
-            const int t0 = starts[t], tn = starts[t + 1] - starts[t];
-            if (tn > hb::LOC_MAX_CELL + 1)
-                return hb::set_error(HB_E_INVALID, "tile of %d cells: the staged tile kernel takes at most %d", tn,
-                                     hb::LOC_MAX_CELL + 1);
-            auto local = [&](int cell) -> uint32_t {   // scenario-local device cell -> staged index
-                if (tile_of[cell] == (int32_t)t) return (uint32_t)(cell - t0);
-                if (halo_mark[cell] != (int32_t)t) {
-                    halo_mark[cell] = (int32_t)t;
-                    halo_slot[cell] = tn + (int)(hm.halo.size() - td.halo0);
-                    hm.halo.push_back(c0 + cell);
-                }
-                return (uint32_t)halo_slot[cell];
-            };
-            for (size_t r = td.rec0; r < hm.rix.size(); r++) {
-                const int4 ix = hm.rix[r];
-                const int a = ix.x - c0, b = ix.y < 0 ? -1 : ix.y - c0;
-                const uint32_t la = (uint32_t)(a - t0), ja = (uint32_t)(ix.z - 4 * ix.x);
-                const uint32_t lb = b < 0 ? hb::LOC_NONE : local(b);
-                const uint32_t jb = ix.w < 0 ? 0u : (uint32_t)(ix.w - 4 * ix.y);
-                if (lb != hb::LOC_NONE && lb >= hb::LOC_NONE)
-                    return hb::set_error(HB_E_INVALID, "tile with a halo of %d cells: too large for the staged tile kernel",
-                                         (int)(hm.halo.size() - td.halo0));
-                hm.rloc.push_back(hb::loc_pack(la, lb, ja, jb));
-            }
-            td.nhalo = (int)hm.halo.size() - td.halo0;
         }
         sc.npairs += td.npairs;
         sc.tiles.push_back(td);
@@ -524,13 +491,6 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *mds, int n, hb::DevMesh<
         TRY(dev_upload(h, &rp, hm.rgeo)); m.rgeo = rp;
     }
     TRY(dev_upload(h, &up, hm.rmeta)); m.rmeta = up;
-    m.rloc = nullptr;
-    m.halo = nullptr;
-    if (h->opt.layout == HB_LAYOUT_TILE) {
-        uint32_t *lp32;
-        TRY(dev_upload(h, &lp32, hm.rloc)); m.rloc = lp32;
-        if (!hm.halo.empty()) { TRY(dev_upload(h, &ip, hm.halo)); m.halo = ip; }
-    }
     TRY(dev_upload(h, &ip, hm.bcell)); m.bcell = ip;
     TRY(dev_upload(h, &rp, bqt)); m.bqt = rp;
     TRY(dev_upload(h, &rp, bdqt)); m.bdqt = rp;
@@ -583,18 +543,17 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *mds, int n, hb::DevMesh<
     }
     m.fseg = h->d_fseg[1];
     m.useg = h->d_useg;
-    m.rev_update = 1;
+    m.rev_flux = 1;     // single mesh: flux CTAs last range first, cells first range first
+    m.rev_update = 1;   // batches: flux segments in order, cells reversed
     {
         std::vector<hb::TileDesc> tiles;
         m.max_tile_cells = 1;
         m.max_tile_pairs = 1;
-        m.max_tile_halo = 0;
         for (const auto &sc : h->scn)
             for (const auto &td : sc.tiles) {
                 tiles.push_back(td);
                 m.max_tile_cells = std::max(m.max_tile_cells, td.cells);
                 m.max_tile_pairs = std::max(m.max_tile_pairs, td.npairs);
-                m.max_tile_halo = std::max(m.max_tile_halo, td.nhalo);
             }
         m.ntiles = (int)tiles.size();
         hb::TileDesc *tp;
@@ -1156,9 +1115,6 @@ extern "C" int hb_set_tile_config(hb_handle *h, int32_t tile_config) {
     if (c < 0) return hb::set_error(HB_E_INVALID, "tile_config %d is no shape of this handle's layout", tile_config);
     if (h->opt.persistent && c != hb::DEFAULT_EDGE_CONFIG)
         return hb::set_error(HB_E_INVALID, "a persistent handle keeps the default launch shape");
-    if (hb::config_staged(c) && !h->staged_ok)
-        return hb::set_error(HB_E_INVALID, "tile_config %d: the staged tile kernel's shared memory exceeds a CTA's "
-                             "on this mesh", tile_config);
     if (c != h->launch_config) h->drop_graph();
     h->launch_config = c;
     return HB_OK;
@@ -1222,7 +1178,6 @@ extern "C" int hb_autotune(hb_handle *h, int32_t steps, void *stream, float *ms_
     for (int c = 0; rc == HB_OK && c < hb::N_LAUNCH_CONFIGS; c++) {
         if (ms_per_step && c < capacity) ms_per_step[c] = 0.f;
         if (hb::LAUNCH_CONFIGS[c].layout != h->opt.layout) continue;
-        if (hb::config_staged(c) && !h->staged_ok) continue;
         h->launch_config = c;
         if ((rc = copy_all(false)) != HB_OK) break;
         if ((rc = enqueue_steps(h, 1, st)) != HB_OK) break;

@@ -21,21 +21,14 @@ enum : uint8_t { META_CODE = 0x0F, META_OWN_FIRST = 0x10, META_HAS_NB = 0x20 };
 // Launch shapes.  Edge layout: the flux kernel's threads per CTA and CTAs per
 // SM asked of the compiler through __launch_bounds__ (which caps registers
 // per thread), and the cell kernel's CTAs per SM (it has UPDATE_THREADS
-// threads).  Tile layout: the tile kernel's threads per CTA and CTAs per SM,
-// and in the last field 1 for the staged tile kernel (cell states staged in
-// shared memory), 0 for the tile kernel that gathers them from global memory.
+// threads).  Tile layout: the tile kernel's threads per CTA and CTAs per SM.
 enum Layout : int { LAYOUT_EDGE = HB_LAYOUT_EDGE, LAYOUT_TILE = HB_LAYOUT_TILE };
 struct LaunchConfig { int layout, threads, min_blocks, update_min_blocks; };
 constexpr LaunchConfig LAUNCH_CONFIGS[] = {
     {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 8}, {LAYOUT_EDGE, 128, 8, 8}, {LAYOUT_EDGE, 256, 3, 6},
     {LAYOUT_EDGE, 256, 4, 8}, {LAYOUT_EDGE, 128, 4, 6}, {LAYOUT_EDGE, 256, 2, 6}, {LAYOUT_EDGE, 64, 12, 8},
     {LAYOUT_TILE, 256, 3, 0}, {LAYOUT_TILE, 256, 2, 0}, {LAYOUT_TILE, 128, 6, 0}, {LAYOUT_TILE, 128, 4, 0},
-    {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0},
-    {LAYOUT_TILE, 256, 3, 1}, {LAYOUT_TILE, 128, 6, 1}, {LAYOUT_TILE, 256, 2, 1}, {LAYOUT_TILE, 384, 2, 1},
-    {LAYOUT_TILE, 512, 1, 1}, {LAYOUT_TILE, 128, 4, 1}};
-constexpr bool config_staged(int c) {
-    return LAUNCH_CONFIGS[c].layout == LAYOUT_TILE && LAUNCH_CONFIGS[c].update_min_blocks == 1;
-}
+    {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0}};
 constexpr int N_LAUNCH_CONFIGS = sizeof(LAUNCH_CONFIGS) / sizeof(LAUNCH_CONFIGS[0]);
 constexpr int DEFAULT_EDGE_CONFIG = 0;
 constexpr int DEFAULT_TILE_CONFIG = 8;
@@ -43,23 +36,8 @@ constexpr int UPDATE_THREADS = 128;
 
 // One tile of the tile layout: a compact group of cells, contiguous in the
 // device order, with its records (mirror pairs inside the tile, then every
-// other real slot of its cells) and its halo: the cells outside the tile that
-// its single records have as neighbours, halo[halo0 .. halo0 + nhalo).
-struct TileDesc { int scn, cell0, cells, rec0, npairs, nsingles, halo0, nhalo; };
-
-// A record's cells as indices into its tile's staged states (the tile's own
-// cells 0 .. cells-1, then its halo), with the slot numbers within the cells:
-// bits 0-11 own cell, 12-24 neighbour (LOC_NONE: no neighbour), 25-26 the
-// own cell's slot j, 27-28 (pairs) the neighbour's slot.
-constexpr int LOC_MAX_CELL = 0xFFF;
-constexpr uint32_t LOC_NONE = 0x1FFF;
-__host__ __device__ inline uint32_t loc_pack(uint32_t la, uint32_t lb, uint32_t ja, uint32_t jb) {
-    return la | (lb << 12) | (ja << 25) | (jb << 27);
-}
-struct Loc { int la, lb, ja, jb; };
-__device__ __forceinline__ Loc loc_unpack(uint32_t x) {
-    return {(int)(x & 0xFFFu), (int)((x >> 12) & 0x1FFFu), (int)((x >> 25) & 3u), (int)((x >> 27) & 3u)};
-}
+// other real slot of its cells).
+struct TileDesc { int scn, cell0, cells, rec0, npairs, nsingles; };
 
 // Constants of one scenario of a batch (the only entry for a single mesh).
 struct ScnParams {
@@ -112,15 +90,17 @@ struct DevMesh {
     const ScnParams *scn;      // [nscen]
     const int4 *fseg;          // flux CTAs {scenario, first record, records, 1 = mirror pairs}
     const int4 *useg;          // update CTAs {scenario, first cell, cells, 0}
-    // edge layout: the cell kernel takes its CTAs' cell ranges in reverse order
-    // (last range first), so it starts on the slot terms the flux kernel wrote
+    // edge layout, single mesh: the flux kernel takes its CTAs' record ranges
+    // in reverse order (rev_flux), so the single records at the end of the
+    // list (boundary slots, whose fixed-point iterations make them the slowest)
+    // start first instead of forming the launch's tail.  The cell kernel takes
+    // its ranges in the opposite order of the flux kernel (batches: reversed
+    // when rev_update), so it starts on the slot terms the flux kernel wrote
     // last, which are still in L2 when the mesh's terms exceed it
-    int rev_update;
+    int rev_flux, rev_update;
     // tile layout
     const TileDesc *tiles;     // [ntiles]
-    int ntiles, max_tile_cells, max_tile_pairs, max_tile_halo;
-    const uint32_t *rloc;      // [nrecords] loc_pack of each record (tile layout)
-    const int32_t *halo;       // the tiles' halo cells, concatenated (tile layout)
+    int ntiles, max_tile_cells, max_tile_pairs;
 };
 
 struct StepIndex { int par, kt, jt; };
@@ -317,16 +297,30 @@ __device__ __forceinline__ bool same_bits(R a, R b) {
 // evaluations run together after the main pass (pair_mirror).
 // pair_core takes both cells' states, the geometry of a's slot and the two
 // slots sa, sb; a pair whose mirrored Osher must run on its own is queued as
-// record r.  tslot is the thread's shared-memory slot for the Osher trace.
-template <class R>
-struct TraceSlot { R *p; int stride; };   // 8 values at p[i * stride]
+// record r.  tslot stores the Osher trace and the tangents of a re-summed
+// FLUX2 (TRACE_VALUES values): SmemTrace, the thread's slot in shared memory
+// (the edge-layout kernels, whose registers are scarce), or RegTrace
+// (registers: the tile kernel, whose shared memory is).
 constexpr int TRACE_VALUES = 8;
+template <class R>
+struct SmemTrace {   // values at p[i * stride]
+    R *p;
+    int stride;
+    __device__ __forceinline__ void set(int i, R v) { p[i * stride] = v; }
+    __device__ __forceinline__ R get(int i) const { return p[i * stride]; }
+};
+template <class R>
+struct RegTrace {
+    R v[TRACE_VALUES];
+    __device__ __forceinline__ void set(int i, R x) { v[i] = x; }
+    __device__ __forceinline__ R get(int i) const { return v[i]; }
+};
 
-template <class A, int VARIANT, class T>
+template <class A, int VARIANT, class T, class TS>
 __device__ __forceinline__ void pair_core(const DevMesh<A> &m, int r, const CellStateA<A> &A_,
                                           const CellStateA<A> &B_, const Vec4<typename A::real> &g, int sa, int sb,
                                           const StepParams &p, int write_flux, const T &tout, int *queue, int *qn,
-                                          const TraceSlot<typename A::real> &tslot) {
+                                          TS &tslot) {
     using R = typename A::real;
     const int4 ix = make_int4(0, 0, sa, sb);
     const R cs = g.x, sn = g.y;
@@ -372,10 +366,10 @@ __device__ __forceinline__ void pair_core(const DevMesh<A> &m, int r, const Cell
         const bool b_resum = b_same && ra_ && !same_bits(oi.ql[2], ql2_m);
         const R term_a = osher_f1_term<A>(oi.ratio, oi.hcR, oi.ur);
         const R term_b = osher_f1_term<A>(oi.ratio, oi.hcR, ur_m);
-        if (b_resum) { tslot.p[6 * tslot.stride] = ql2_m; tslot.p[7 * tslot.stride] = oi.qr[2]; }
+        if (b_resum) { tslot.set(6, ql2_m); tslot.set(7, oi.qr[2]); }
         const typename A::level zbcA = A_.zbc, zbcB = B_.zbc;
         R fo[4];
-        OsherTraceAt<R> tr{tslot.p, tslot.stride, 0u, 0u};
+        OsherTraceIn<TS> tr{&tslot, 0u, 0u};
         osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo, &tr);
         if (ra_) {
             R f[4];
@@ -390,7 +384,7 @@ __device__ __forceinline__ void pair_core(const DevMesh<A> &m, int r, const Cell
             R f[4];
             f[0] = -fo[0];
             f[1] = A::add(fo[1], term_b);
-            f[2] = b_resum ? osher_f2<A>(tr, tslot.p[6 * tslot.stride], tslot.p[7 * tslot.stride]) : fo[2];
+            f[2] = b_resum ? osher_f2<A>(tr, tslot.get(6), tslot.get(7)) : fo[2];
             f[3] = mirror_f3<A>(fo[3], zbcA, zbcB);
             if (write_flux) store_flux(m, ix.w, f);
             store_terms<A>(tout, ix.w, f, g.z, -cs, -sn);
@@ -400,10 +394,9 @@ __device__ __forceinline__ void pair_core(const DevMesh<A> &m, int r, const Cell
     }
 }
 
-template <class A, int VARIANT, class T>
+template <class A, int VARIANT, class T, class TS>
 __device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const StepIndex &si, const StepParams &p,
-                                            int write_flux, const T &tout, int *queue, int *qn,
-                                            const TraceSlot<typename A::real> &tslot) {
+                                            int write_flux, const T &tout, int *queue, int *qn, TS &tslot) {
     using R = typename A::real;
     const int4 ix = m.rix[r];
     const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
@@ -419,7 +412,7 @@ __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k
     __shared__ int queue[THREADS];
     __shared__ int qn;
     __shared__ typename A::real trace[TRACE_VALUES * THREADS];
-    const TraceSlot<typename A::real> tslot{trace + threadIdx.x, THREADS};
+    SmemTrace<typename A::real> tslot{trace + threadIdx.x, THREADS};
     if (threadIdx.x == 0) qn = 0;
     int r;
     bool valid, pair;
@@ -440,7 +433,7 @@ __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k
         cudaTriggerProgrammaticLaunchCompletion();
         si = step_index(m, k, m.per_day, m.ndays);
         p = StepParams{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
-        r = blockIdx.x * THREADS + threadIdx.x;
+        r = (m.rev_flux ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x) * THREADS + threadIdx.x;
         valid = r < m.nrecords;
         pair = r < m.npairs;
     }
@@ -543,7 +536,9 @@ __device__ __forceinline__ void update_one(const DevMesh<A> &m, int c, const Ste
 // update coefficients of the wet cells into m.ucoef.
 template <class A, int VARIANT, int UMINB, bool SEG, bool COEF = false>
 __global__ void __launch_bounds__(UPDATE_THREADS, UMINB) update_kernel(DevMesh<A> m, int k, int write_flux) {
-    const int blk = m.rev_update ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+    // batches: the flux segments run forward, so the cells run reversed
+    const bool rev = SEG ? m.rev_update != 0 : m.rev_flux == 0;
+    const int blk = rev ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
     if constexpr (SEG) {
         const int4 d = m.useg[blk];
         const ScnParams sp = m.scn[d.x];
@@ -586,9 +581,8 @@ __global__ void __launch_bounds__(THREADS, MINB) tile_kernel(DevMesh<A> m, int k
     const Terms<R, true> tout{terms, 4 * td.cell0};
     __syncthreads();
     const int nrec = td.npairs + td.nsingles;
-    __shared__ R trace[TRACE_VALUES * THREADS];
-    const TraceSlot<R> tslot{trace + threadIdx.x, THREADS};
     for (int i = threadIdx.x; i < nrec; i += THREADS) {
+        RegTrace<R> tslot;
         if (i < td.npairs) pair_record<A, VARIANT>(m, td.rec0 + i, si, p, write_flux, tout, queue, &qn, tslot);
         else single_record<A, VARIANT>(m, td.rec0 + i, si, p, write_flux, tout);
     }
@@ -597,91 +591,6 @@ __global__ void __launch_bounds__(THREADS, MINB) tile_kernel(DevMesh<A> m, int k
     __syncthreads();
     for (int c = threadIdx.x; c < td.cells; c += THREADS)
         update_one<A, VARIANT, false, true>(m, td.cell0 + c, si, p, write_flux, terms + 16 * c);
-}
-
-// Shared memory of the staged tile kernel, in this order: the slot terms
-// [cells][4 slots][4] R; the staged state records [cells + halo][4] R; the
-// staged beds [cells + halo] L; the mirrored-Osher queue [pairs] int.
-template <class A>
-__host__ __device__ inline size_t staged_smem_bytes(int cells, int halo, int pairs) {
-    using R = typename A::real;
-    using L = typename A::level;
-    return 16 * sizeof(R) * (size_t)cells + (4 * sizeof(R) + sizeof(L)) * (size_t)(cells + halo) +
-           sizeof(int) * (size_t)pairs;
-}
-
-// The whole step of one tile with its cells' states staged in shared memory.
-// The CTA first copies the state records and beds of the tile's own cells
-// (contiguous: coalesced 256-bit loads) and of its halo cells into shared
-// memory; every record then takes both of its cells from there through the
-// local indices of m.rloc, so no record waits on a dependent global gather.
-// The rest is tile_kernel's sequence: records (pairs, then singles) write
-// their slot terms into shared memory, the queued mirrored Osher evaluations
-// run, and each cell of the tile sums its four slots in order and is updated
-// from its staged state.  Same arithmetic as every other form, so the same
-// bits.
-template <class A, int VARIANT, int THREADS, int MINB>
-__global__ void __launch_bounds__(THREADS, MINB) staged_tile_kernel(DevMesh<A> m, int k, int write_flux) {
-    using R = typename A::real;
-    using L = typename A::level;
-    extern __shared__ __align__(16) unsigned char tile_smem[];
-    const int cap = m.max_tile_cells + m.max_tile_halo;
-    R *terms = reinterpret_cast<R *>(tile_smem);                        // [max cells][16]
-    R *sst = terms + 16 * (size_t)m.max_tile_cells;                     // [cap][4]
-    L *szb = reinterpret_cast<L *>(sst + 4 * (size_t)cap);              // [cap]
-    int *queue = reinterpret_cast<int *>(szb + cap);                    // [max pairs]
-    __shared__ int qn;
-    const TileDesc td = m.tiles[blockIdx.x];   // constant tables: read before the dependency wait
-    const ScnParams sp = m.scn[td.scn];
-    if (threadIdx.x == 0) qn = 0;
-    cudaGridDependencySynchronize();
-    cudaTriggerProgrammaticLaunchCompletion();
-    const StepIndex si = step_index(m, k, sp.per_day, sp.ndays);
-    const StepParams p{sp.hm1, sp.hm2, sp.jl, sp.dt, si.kt, si.jt};
-    const R *S = m.S[si.par];
-    const int nown = td.cells, nall = td.cells + td.nhalo;
-    for (int i = threadIdx.x; i < nall; i += THREADS) {
-        const int c = i < nown ? td.cell0 + i : m.halo[td.halo0 + (i - nown)];
-        const Vec4<R> v = ldg4(S + 4 * (size_t)c);
-        st4(sst + 4 * i, v.x, v.y, v.z, v.w);
-        szb[i] = m.zbc[c];
-    }
-    __syncthreads();
-    auto cell = [&](int i) -> CellStateA<A> {
-        const Vec4<R> v = ld4(sst + 4 * i);
-        const L zbc = szb[i];
-        if constexpr (is_split<A>::value) return {v.x, v.y, v.z, split_level<A>(v.x, v.w, zbc), zbc};
-        else return {v.x, v.y, v.z, v.w, zbc};
-    };
-    const Terms<R, true> tout{terms, 4 * td.cell0};
-    __shared__ R trace[TRACE_VALUES * THREADS];
-    const TraceSlot<R> tslot{trace + threadIdx.x, THREADS};
-    const int nrec = td.npairs + td.nsingles;
-    for (int i = threadIdx.x; i < nrec; i += THREADS) {
-        const int r = td.rec0 + i;
-        const Loc l = loc_unpack(m.rloc[r]);
-        const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
-        const int a = td.cell0 + l.la;
-        if (i < td.npairs) {
-            pair_core<A, VARIANT>(m, r, cell(l.la), cell(l.lb), g, 4 * a + l.ja, 4 * (td.cell0 + l.lb) + l.jb, p,
-                                  write_flux, tout, queue, &qn, tslot);
-        } else {
-            const uint8_t meta = m.rmeta[r];
-            const CellStateA<A> nb = l.lb != (int)LOC_NONE ? cell(l.lb) : CellStateA<A>{R(0), R(0), R(0), L(0), L(0)};
-            single_core<A, VARIANT>(m, r, a, 4 * a + l.ja, cell(l.la), nb, meta, g, si, p, write_flux, tout);
-        }
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < qn; i += THREADS) {
-        const int r = queue[i];
-        const Loc l = loc_unpack(m.rloc[r]);
-        const Vec4<R> g = ldg4(m.rgeo + 4 * (size_t)r);
-        mirror_core<A>(m, cell(l.la), cell(l.lb), g, 4 * (td.cell0 + l.lb) + l.jb, p, write_flux, tout);
-    }
-    __syncthreads();
-    for (int c = threadIdx.x; c < td.cells; c += THREADS)
-        update_core<A, VARIANT, false, true>(m, td.cell0 + c, ld4(sst + 4 * c), szb[c], si, p, write_flux,
-                                             terms + 16 * c);
 }
 
 // ---------------------------------------------------------------------------
@@ -757,7 +666,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
     __shared__ int queue[THREADS];
     __shared__ int qn;
     __shared__ typename A::real trace[TRACE_VALUES * THREADS];
-    const TraceSlot<typename A::real> tslot{trace + threadIdx.x, THREADS};
+    SmemTrace<typename A::real> tslot{trace + threadIdx.x, THREADS};
     const Terms<typename A::real> tout{m.slotw, 0};
     unsigned arrivals = 0;
     for (int k = 0; k < n; k++) {

@@ -1,8 +1,6 @@
-// hb_tiles.cu -- launches of the tile layout: one kernel per step over the
-// mesh's tiles, either tile_kernel (cell states gathered from global memory)
-// or staged_tile_kernel (each tile's cell states staged in shared memory
-// first), at the launch shape the handle holds.  A translation unit of its
-// own so the library's kernels compile in parallel.
+// hb_tiles.cu -- launches of the tile layout: one tile_kernel per step over
+// the mesh's tiles, at the launch shape the handle holds.  A translation unit
+// of its own so the library's kernels compile in parallel.
 #include <algorithm>
 #include <type_traits>
 
@@ -25,27 +23,12 @@ int with_tile_kernel(int config, F &&f) {
     case 11: return f(tile_kernel<A, VARIANT, 128, 4>, 128);
     case 12: return f(tile_kernel<A, VARIANT, 512, 1>, 512);
     case 13: return f(tile_kernel<A, VARIANT, 256, 4>, 256);
-    case 14: return f(staged_tile_kernel<A, VARIANT, 256, 3>, 256);
-    case 15: return f(staged_tile_kernel<A, VARIANT, 128, 6>, 128);
-    case 16: return f(staged_tile_kernel<A, VARIANT, 256, 2>, 256);
-    case 17: return f(staged_tile_kernel<A, VARIANT, 384, 2>, 384);
-    case 18: return f(staged_tile_kernel<A, VARIANT, 512, 1>, 512);
-    case 19: return f(staged_tile_kernel<A, VARIANT, 128, 4>, 128);
     default: return hb::set_error(HB_E_INVALID, "launch shape %d is not a tile-layout shape", config + 1);
     }
 }
 
-// Dynamic shared memory of a tile-layout launch shape on the handle's mesh.
-template <class A>
-size_t tile_config_smem(const hb::DevMesh<A> &m, int config) {
-    if (hb::config_staged(config)) return hb::staged_smem_bytes<A>(m.max_tile_cells, m.max_tile_halo, m.max_tile_pairs);
-    return tile_smem_bytes(m.max_tile_cells, m.max_tile_pairs, sizeof(typename A::real));
-}
-
 template <class A, int VARIANT>
 int launch_tiles_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
-    if (hb::config_staged(h->launch_config) && !h->staged_ok)
-        return hb::set_error(HB_E_INVALID, "the staged tile kernel needs more shared memory than a CTA has on this mesh");
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
@@ -54,7 +37,7 @@ int launch_tiles_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     cfg.stream = st;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cfg.dynamicSmemBytes = tile_config_smem(m, h->launch_config);
+    cfg.dynamicSmemBytes = tile_smem_bytes(m.max_tile_cells, m.max_tile_pairs, sizeof(typename A::real));
     const int rc = with_tile_kernel<A, VARIANT>(h->launch_config, [&](auto kernel, int threads) -> int {
         cfg.blockDim = dim3(threads);
         for (int k = 0; k < n; k++) HB_CUDA_RET(cudaLaunchKernelEx(&cfg, kernel, m, k, (int)(k == n - 1)));
@@ -65,17 +48,12 @@ int launch_tiles_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
 }
 
 // Lets every tile kernel of the handle's policy use the shared memory its
-// largest tile needs (beyond the 48 KB default); records whether the staged
-// kernel's fits a CTA (h->staged_ok).
+// largest tile needs (beyond the 48 KB default).
 template <class A, int VARIANT>
-int set_tile_smem(hb_handle *h, const hb::DevMesh<A> &m) {
-    int optin = 0;
-    HB_CUDA_RET(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->opt.device));
-    h->staged_ok = hb::staged_smem_bytes<A>(m.max_tile_cells, m.max_tile_halo, m.max_tile_pairs) <= (size_t)optin;
+int set_tile_smem(const hb::DevMesh<A> &m) {
+    const size_t bytes = tile_smem_bytes(m.max_tile_cells, m.max_tile_pairs, sizeof(typename A::real));
     for (int c = 0; c < hb::N_LAUNCH_CONFIGS; c++) {
         if (hb::LAUNCH_CONFIGS[c].layout != hb::LAYOUT_TILE) continue;
-        if (hb::config_staged(c) && !h->staged_ok) continue;
-        const size_t bytes = tile_config_smem(m, c);
         const int rc = with_tile_kernel<A, VARIANT>(c, [&](auto kernel, int) -> int {
             HB_CUDA_RET(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
             return HB_OK;
@@ -99,6 +77,6 @@ int hb_tiles_set_smem(hb_handle *h) {
     const bool f = h->opt.variant == HB_VARIANT_F;
     return h->with_mesh([&](auto &m) {
         using A = typename std::remove_reference<decltype(m)>::type::Policy;
-        return f ? set_tile_smem<A, 1>(h, m) : set_tile_smem<A, 0>(h, m);
+        return f ? set_tile_smem<A, 1>(m) : set_tile_smem<A, 0>(m);
     });
 }

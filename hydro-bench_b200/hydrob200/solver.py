@@ -28,8 +28,7 @@ def launch_shapes():
     lay, thr, mb = (C.c_int32 * n)(), (C.c_int32 * n)(), (C.c_int32 * n)()
     lib().hb_launch_shapes(lay, thr, mb, n)
     names = {_lib.LAYOUT_EDGE: "edge", _lib.LAYOUT_TILE: "tile"}
-    return {i + 1: dict(layout=names[lay[i]], threads=thr[i], min_blocks=mb[i] // 100, update_min_blocks=mb[i] % 100,
-                        staged=lay[i] == _lib.LAYOUT_TILE and mb[i] % 100 == 1)
+    return {i + 1: dict(layout=names[lay[i]], threads=thr[i], min_blocks=mb[i] // 100, update_min_blocks=mb[i] % 100)
             for i in range(n)}
 
 

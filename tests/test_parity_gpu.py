@@ -46,18 +46,11 @@ def _fp64_cases():
                 yield name, b
 
 
-def _staged_config(threads):
-    """tile_config of the staged tile kernel with `threads` threads per CTA."""
-    return next(k for k, v in hb.launch_shapes().items() if v["staged"] and v["threads"] == threads)
-
-
-@pytest.mark.parametrize("layout,tile_cells,staged", [("edge", 0, 0), ("tile", 0, 0), ("tile", 64, 0),
-                                                      ("tile", 0, 256), ("tile", 64, 128), ("tile", 512, 384)])
+@pytest.mark.parametrize("layout,tile_cells", [("edge", 0), ("tile", 0), ("tile", 64)])
 @pytest.mark.parametrize("name,binary", list(_fp64_cases()))
-def test_handle_path_bit_exact(deck_dir, name, binary, layout, tile_cells, staged):
+def test_handle_path_bit_exact(deck_dir, name, binary, layout, tile_cells):
     deck = hb.Deck(deck_dir[name])
-    s = hb.Solver(deck, variant="H" if binary == "h64" else "F", layout=layout, tile_cells=tile_cells,
-                  tile_config=_staged_config(staged) if staged else 0)
+    s = hb.Solver(deck, variant="H" if binary == "h64" else "F", layout=layout, tile_cells=tile_cells)
     done = 0
     for steps in DECKS[name]["steps"]:
         s.step(steps - done)
