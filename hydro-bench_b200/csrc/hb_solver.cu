@@ -741,7 +741,7 @@ int hb_forward_step_into(hb_handle *h, long long t0, int k, const double *in, do
     cfg.numAttrs = 1;
     cfg.gridDim = dim3((unsigned)((m.nrecords + 127) / 128));
     cfg.blockDim = dim3(128);
-    HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::flux_kernel<hb::F64Exact, 0, 128, 6, false>, m, k, write_flux));
+    HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::flux_kernel<hb::F64Exact, 0, 128, 6, false, false>, m, k, write_flux));
     cfg.gridDim = dim3((unsigned)((m.C + hb::UPDATE_THREADS - 1) / hb::UPDATE_THREADS));
     cfg.blockDim = dim3(hb::UPDATE_THREADS);
     HB_CUDA_RET(cudaLaunchKernelEx(&cfg, hb::update_kernel<hb::F64Exact, 0, 6, false, true>, m, k, write_flux));

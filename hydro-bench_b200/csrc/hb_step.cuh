@@ -407,12 +407,18 @@ __device__ __forceinline__ void pair_record(const DevMesh<A> &m, int r, const St
 // Flux of every record of one step.  Single mesh (SEG = false): records
 // [0, npairs) are mirror pairs and the rest single slots, one per thread.
 // Batch (SEG = true): CTA b takes the scenario and record range of fseg[b].
-template <class A, int VARIANT, int THREADS, int MINB, bool SEG>
+// SMEM_TRACE: the Osher trace in shared memory (fewer registers, more shared
+// memory per CTA) or in registers.
+template <class A, int VARIANT, int THREADS, int MINB, bool SEG, bool SMEM_TRACE = true>
 __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k, int write_flux) {
+    using R = typename A::real;
     __shared__ int queue[THREADS];
     __shared__ int qn;
-    __shared__ typename A::real trace[TRACE_VALUES * THREADS];
-    SmemTrace<typename A::real> tslot{trace + threadIdx.x, THREADS};
+    __shared__ R trace[SMEM_TRACE ? TRACE_VALUES * THREADS : 1];
+    auto tslot = [&]() {
+        if constexpr (SMEM_TRACE) return SmemTrace<R>{trace + threadIdx.x, THREADS};
+        else return RegTrace<R>{};
+    }();
     if (threadIdx.x == 0) qn = 0;
     int r;
     bool valid, pair;
@@ -663,19 +669,39 @@ template <class A, int VARIANT, int THREADS, int MINB, bool SEG>
 __global__ void __launch_bounds__(THREADS, MINB)
     persistent_kernel(DevMesh<A> m, int n, int nflux, int ncell, unsigned *bar, unsigned phantom,
                       unsigned long long limit_ns) {
-    __shared__ int queue[THREADS];
+    // The mirrored-Osher queue collects the pairs of several chunks and is run
+    // when it could not take another chunk's worth, and at the end of the flux
+    // phase: one block barrier per chunk instead of three.  Every queued pair
+    // is run before the grid barrier, as flux_kernel runs it before it ends.
+    constexpr int QCAP = 4 * THREADS;
+    __shared__ int queue[QCAP];
     __shared__ int qn;
     __shared__ typename A::real trace[TRACE_VALUES * THREADS];
     SmemTrace<typename A::real> tslot{trace + threadIdx.x, THREADS};
     const Terms<typename A::real> tout{m.slotw, 0};
     unsigned arrivals = 0;
+    if (threadIdx.x == 0) qn = 0;
+    __syncthreads();
+    auto run_queue = [&](const StepIndex &si, const StepParams &p, int wf) {   // all threads; empties the queue
+        const int nq = qn;
+        for (int i = threadIdx.x; i < nq; i += THREADS) pair_mirror<A>(m, queue[i], si, p, wf, tout);
+        __syncthreads();
+        if (threadIdx.x == 0) qn = 0;
+        __syncthreads();
+    };
     for (int k = 0; k < n; k++) {
         const int wf = k == n - 1;
+        StepIndex si0{};
+        StepParams p0{};
+        if constexpr (!SEG) {
+            si0 = step_index(m, k, m.per_day, m.ndays);
+            p0 = StepParams{m.hm1, m.hm2, m.jl, m.dt, si0.kt, si0.jt};
+        }
         for (int b = blockIdx.x; b < nflux; b += gridDim.x) {
             int r0, cnt;
             bool seg_pairs = false;
-            StepIndex si;
-            StepParams p;
+            StepIndex si = si0;
+            StepParams p = p0;
             if constexpr (SEG) {
                 const int4 d = m.fseg[b];
                 const ScnParams sp = m.scn[d.x];
@@ -685,23 +711,21 @@ __global__ void __launch_bounds__(THREADS, MINB)
                 cnt = d.z;
                 seg_pairs = d.w != 0;
             } else {
-                si = step_index(m, k, m.per_day, m.ndays);
-                p = StepParams{m.hm1, m.hm2, m.jl, m.dt, si.kt, si.jt};
-                r0 = b * THREADS;
+                r0 = (m.rev_flux ? nflux - 1 - b : b) * THREADS;   // boundary singles first, as flux_kernel
                 cnt = min(THREADS, m.nrecords - r0);
             }
-            if (threadIdx.x == 0) qn = 0;
-            __syncthreads();
             if ((int)threadIdx.x < cnt) {
                 const int r = r0 + (int)threadIdx.x;
                 const bool pair = SEG ? seg_pairs : r < m.npairs;
                 if (pair) pair_record<A, VARIANT>(m, r, si, p, wf, tout, queue, &qn, tslot);
                 else single_record<A, VARIANT>(m, r, si, p, wf, tout);
             }
-            __syncthreads();
-            for (int i = threadIdx.x; i < qn; i += THREADS) pair_mirror<A>(m, queue[i], si, p, wf, tout);
-            __syncthreads();   // the queue is reused by the next chunk
+            __syncthreads();   // the queue's count is complete
+            // a batch chunk's pairs have their scenario's parameters: its queue
+            // runs at once; a single mesh's when another chunk might not fit
+            if (SEG || qn > QCAP - THREADS) run_queue(si, p, wf);
         }
+        if constexpr (!SEG) run_queue(si0, p0, wf);
         arrivals += gridDim.x;
         if (!grid_barrier(bar, arrivals + phantom, m.err, limit_ns)) return;
         for (int b = blockIdx.x; b < ncell; b += gridDim.x) {
