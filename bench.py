@@ -409,25 +409,25 @@ def adjoint_leg(local, steps=1000, ks=(10, 50, 100)):
 
 
 def split_leg(deck, local, steps=EXTRA_STEPS_207K, precision="split"):
-    """The reduced-precision step on the 207K mesh (tile layout, autotuned):
-    time from 100-step graph replays, and its depths after `steps` steps
-    against the fp64 step's."""
+    """The reduced-precision step on the 207K mesh (tile layout with the
+    balanced default tile size, default launch shape): time from 100-step
+    graph replays, and its depths after `steps` steps against the fp64
+    step's."""
     import torch
     import hydrob200 as hb
     from hydrob200.accuracy import depth_error
-    sp = hb.Solver(deck, precision=precision, layout="tile", tile_cells=512, device=local)
-    best, _ = sp.autotune(steps=10)
+    sp = hb.Solver(deck, precision=precision, layout="tile", device=local)
     us = _time_graph(sp, steps, 100, torch)
     sp.close()
-    a, b = hb.Solver(deck, device=local), hb.Solver(deck, precision=precision, layout="tile", tile_cells=512,
-                                                     device=local)
+    a, b = hb.Solver(deck, device=local), hb.Solver(deck, precision=precision, layout="tile", device=local)
     a.step(steps)
     b.step(steps)
     a.sync()
     b.sync()
     e = depth_error(b.get_state()["H"], a.get_state()["H"], deck.mesh.hm2, deck.array("area"))
     return {"us_per_step": us, "value": deck.cells / (us * 1e-6), "unit": METRIC, "layout": "tile",
-            "tile_cells": 512, "tile_config": best, "error_vs_fp64": dict(e, after_steps=steps),
+            "tile_cells": "balanced (whole waves of resident CTAs)", "tile_config": "default",
+            "error_vs_fp64": dict(e, after_steps=steps),
             "roofline": hbm_point(precision, deck.cells, unique_edges(deck), us)}
 
 

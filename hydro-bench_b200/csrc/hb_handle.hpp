@@ -56,6 +56,10 @@ struct hb_handle {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_steps = 0;
     int launch_config = 0;           // index into LAUNCH_CONFIGS
+    // tile layout: the cells per tile in use; with the balanced default
+    // (options' tile_cells = 0) also the resident CTAs of the launch shape on
+    // the device and the whole waves of them the tiles must fit in
+    int tile_cells = 256, tile_slots = 0, tile_waves = 0;
     // persistent handles: the grid-barrier words {arrival count, give-up flag}
     // (both zeroed before each launch), the resident CTAs of the cooperative
     // launch (0 = not yet queried), and the barrier wait bound
@@ -130,6 +134,8 @@ int hb_launch_tick(hb_handle *h, int n, cudaStream_t st);
 // shared-memory attributes of its tile kernels
 int hb_tiles_launch(hb_handle *h, int n, cudaStream_t st);
 int hb_tiles_set_smem(hb_handle *h);
+// CTAs per SM of a tile-layout launch shape with tiles of about tile_cells cells
+int hb_tiles_resident(hb_handle *h, int config, int tile_cells, int *per_sm);
 // One fp64 edge-layout step t0 + k (the device step counter must hold t0)
 // from state `in` to state `out` ([C][4] each), keeping the slots' terms of
 // the cell sums in `terms` ([4C][4]) and the update coefficients of the wet

@@ -439,10 +439,25 @@ int build_device_mesh(hb_handle *h, const hb_mesh_desc *mds, int n, hb::DevMesh<
     using R = typename A::real;
     using L = typename A::level;
     HostMesh<A> hm;
-    h->scn.resize(n);
-    for (int s = 0; s < n; s++) {
-        const int st = append_scenario<A>(&mds[s], s, h->opt, h->scn[s], hm);
-        if (st != HB_OK) return n > 1 ? hb::set_error(st, "scenario %d: %s", s, hb_last_error_string()) : st;
+    // tile layout: tiles of h->tile_cells cells; with the balanced default
+    // (tile_waves > 0) the size grows until the tiles fill at most tile_waves
+    // whole waves of tile_slots resident CTAs (a tile count just above a wave
+    // leaves most SMs idle while a few run the extra tiles)
+    hb_options opt = h->opt;
+    for (int pass = 0;; pass++) {
+        opt.tile_cells = h->tile_cells;
+        hm = HostMesh<A>();
+        h->scn.assign(n, hb::Scenario());
+        for (int s = 0; s < n; s++) {
+            const int st = append_scenario<A>(&mds[s], s, opt, h->scn[s], hm);
+            if (st != HB_OK) return n > 1 ? hb::set_error(st, "scenario %d: %s", s, hb_last_error_string()) : st;
+        }
+        if (opt.layout != HB_LAYOUT_TILE || h->tile_waves <= 0 || pass == 3) break;
+        long long tiles = 0;
+        for (const auto &sc : h->scn) tiles += (long long)sc.tiles.size();
+        const long long cap = (long long)h->tile_waves * h->tile_slots;
+        if (tiles <= cap || h->tile_cells >= 1024) break;
+        h->tile_cells = std::min(1024, (int)((h->tile_cells * tiles + cap - 1) / cap) + 1);
     }
     const int C = (int)hm.zbc.size();
     h->C = C;
@@ -800,6 +815,25 @@ extern "C" int hb_create_batch(const hb_mesh_desc *meshes, int32_t n, const hb_o
     auto h = new hb_handle();
     h->opt = opt;
     h->launch_config = config_for(opt.layout, opt.tile_config);
+    h->tile_cells = opt.tile_cells > 0 ? opt.tile_cells : 256;
+    if (opt.layout == HB_LAYOUT_TILE && opt.tile_cells == 0 && opt.precision != HB_FP64) {
+        // balanced default (fp32 state): about 512 cells per tile, adjusted so
+        // the tiles fill whole waves of the launch shape's resident CTAs.  The
+        // fp64 tile kernel keeps 256: its 128 bytes of slot terms per cell make
+        // its occupancy step with the tile size, and smaller balanced tiles
+        // measured slower there.
+        int sms = 0, per_sm = 0;
+        cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, opt.device);
+        int rs = e == cudaSuccess ? hb_tiles_resident(h, h->launch_config, 512, &per_sm) : HB_E_CUDA;
+        if (rs != HB_OK || sms <= 0 || per_sm <= 0) {
+            delete h;
+            return rs != HB_OK ? rs : hb::set_error(HB_E_CUDA, "hb_create: no tile CTA fits on an SM");
+        }
+        h->tile_slots = sms * per_sm;
+        h->tile_waves = (int)std::max(1LL, (total + 512LL * h->tile_slots - 1) / (512LL * h->tile_slots));
+        const long long per_wave = (long long)h->tile_waves * h->tile_slots;
+        h->tile_cells = (int)std::min(1024LL, std::max(64LL, (total + per_wave - 1) / per_wave));
+    }
     int st;
     if ((st = dev_alloc(h, &h->d_err, 1)) != HB_OK || (st = dev_alloc(h, &h->d_ctr, 1)) != HB_OK ||
         (st = dev_alloc(h, &h->d_bar, 2)) != HB_OK) {

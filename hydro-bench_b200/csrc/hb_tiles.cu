@@ -73,6 +73,23 @@ int hb_tiles_launch(hb_handle *h, int n, cudaStream_t st) {
     });
 }
 
+int hb_tiles_resident(hb_handle *h, int config, int tile_cells, int *per_sm) {
+    const bool f = h->opt.variant == HB_VARIANT_F;
+    // shared memory of a tile of up to 5/4 tile_cells cells, with as many
+    // mirror pairs as its slots could form (an upper bound)
+    const int cells = 5 * tile_cells / 4 + 1;
+    return h->with_mesh([&](auto &m) -> int {
+        using A = typename std::remove_reference<decltype(m)>::type::Policy;
+        const size_t bytes = tile_smem_bytes(cells, 2 * cells, sizeof(typename A::real));
+        auto query = [&](auto kernel, int threads) -> int {
+            HB_CUDA_RET(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+            HB_CUDA_RET(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kernel, threads, bytes));
+            return HB_OK;
+        };
+        return f ? with_tile_kernel<A, 1>(config, query) : with_tile_kernel<A, 0>(config, query);
+    });
+}
+
 int hb_tiles_set_smem(hb_handle *h) {
     const bool f = h->opt.variant == HB_VARIANT_F;
     return h->with_mesh([&](auto &m) {

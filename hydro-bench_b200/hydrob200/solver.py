@@ -71,7 +71,10 @@ class Deck:
 
     def __del__(self):
         if getattr(self, "_h", None) and self._h.value:
-            self._lib.hb_deck_free(self._h)
+            try:
+                self._lib.hb_deck_free(self._h)
+            except TypeError:   # interpreter shutdown: ctypes already torn down, the process frees everything
+                pass
             self._h = C.c_void_p()
 
     @property

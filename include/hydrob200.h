@@ -79,7 +79,10 @@ typedef struct hb_options {
     int32_t renumber;         /* 1: reverse Cuthill-McKee cell order on the device (default), 0: input order */
     int32_t tile_config;      /* launch shape: 0 = the layout's default, k > 0 = entry k-1 of hb_launch_shapes() */
     int32_t layout;           /* hb_layout */
-    int32_t tile_cells;       /* HB_LAYOUT_TILE: cells per tile, <= 1024 (0 = 256); tiles hold up to 5*tile_cells/4 */
+    int32_t tile_cells;       /* HB_LAYOUT_TILE: cells per tile, <= 1024; tiles hold up to 5*tile_cells/4.
+                               * 0 = HB_FP32 / HB_SPLIT: balanced, about 512, sized so the tiles fill
+                               * whole waves of the launch shape's resident CTAs on the device;
+                               * HB_FP64: 256 */
     int32_t persistent;       /* HB_LAYOUT_EDGE with the default launch shape only.  1: a step sequence
                                * (hb_step, a captured graph) is one cooperative launch of resident CTAs that
                                * runs every step, flux records then cells, separated by grid barriers whose
