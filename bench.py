@@ -614,7 +614,7 @@ def dambreak_leg(local, steps=2000, every=100, ncells=2_000_000):
     runs = {"fp64": hb.Solver(deck, device=local),
             "split": hb.Solver(deck, precision="split", layout="tile", tile_cells=512, device=local),
             "fp32": hb.Solver(deck, precision="fp32", layout="tile", tile_cells=512, device=local)}
-    tuned = {name: runs[name].autotune(steps=10)[0] for name in ("split", "fp32")}   # state restored
+    tuned = {name: runs[name].autotune(steps=10)[0] for name in ("fp64", "split", "fp32")}   # state restored
     out["tile_config"] = tuned
     st = torch.cuda.current_stream()
     for h in runs.values():

@@ -634,7 +634,7 @@ int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     case 2: rc = go(flux_kernel<A, VARIANT, 128, 8, SEG>, 128, update_kernel<A, VARIANT, 8, SEG>); break;
     case 3: rc = go(flux_kernel<A, VARIANT, 256, 3, SEG>, 256, update_kernel<A, VARIANT, 6, SEG>); break;
     case 4: rc = go(flux_kernel<A, VARIANT, 256, 4, SEG>, 256, update_kernel<A, VARIANT, 8, SEG>); break;
-    case 5: rc = go(flux_kernel<A, VARIANT, 128, 4, SEG>, 128, update_kernel<A, VARIANT, 6, SEG>); break;
+    case 5: rc = go(flux_kernel<A, VARIANT, 128, 7, SEG>, 128, update_kernel<A, VARIANT, 6, SEG>); break;
     case 6: rc = go(flux_kernel<A, VARIANT, 256, 2, SEG>, 256, update_kernel<A, VARIANT, 6, SEG>); break;
     case 7: rc = go(flux_kernel<A, VARIANT, 64, 12, SEG>, 64, update_kernel<A, VARIANT, 8, SEG>); break;
     default: return hb::set_error(HB_E_INVALID, "launch shape %d is not an edge-layout shape", h->launch_config + 1);

@@ -26,7 +26,7 @@ enum Layout : int { LAYOUT_EDGE = HB_LAYOUT_EDGE, LAYOUT_TILE = HB_LAYOUT_TILE }
 struct LaunchConfig { int layout, threads, min_blocks, update_min_blocks; };
 constexpr LaunchConfig LAUNCH_CONFIGS[] = {
     {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 8}, {LAYOUT_EDGE, 128, 8, 8}, {LAYOUT_EDGE, 256, 3, 6},
-    {LAYOUT_EDGE, 256, 4, 8}, {LAYOUT_EDGE, 128, 4, 6}, {LAYOUT_EDGE, 256, 2, 6}, {LAYOUT_EDGE, 64, 12, 8},
+    {LAYOUT_EDGE, 256, 4, 8}, {LAYOUT_EDGE, 128, 7, 6}, {LAYOUT_EDGE, 256, 2, 6}, {LAYOUT_EDGE, 64, 12, 8},
     {LAYOUT_TILE, 256, 3, 0}, {LAYOUT_TILE, 256, 2, 0}, {LAYOUT_TILE, 128, 6, 0}, {LAYOUT_TILE, 128, 4, 0},
     {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0}};
 constexpr int N_LAUNCH_CONFIGS = sizeof(LAUNCH_CONFIGS) / sizeof(LAUNCH_CONFIGS[0]);
@@ -301,19 +301,25 @@ __device__ __forceinline__ bool same_bits(R a, R b) {
 // FLUX2 (TRACE_VALUES values): SmemTrace, the thread's slot in shared memory
 // (the edge-layout kernels, whose registers are scarce), or RegTrace
 // (registers: the tile kernel, whose shared memory is).
-constexpr int TRACE_VALUES = 8;
+constexpr int TRACE_VALUES = 16;
 template <class R>
 struct SmemTrace {   // values at p[i * stride]
     R *p;
     int stride;
     __device__ __forceinline__ void set(int i, R v) { p[i * stride] = v; }
     __device__ __forceinline__ R get(int i) const { return p[i * stride]; }
+    // a value kept out of registers across a stretch of code: the volatile
+    // access makes the compiler read it back instead of holding it
+    __device__ __forceinline__ void park(int i, R v) { *(volatile R *)(p + i * stride) = v; }
+    __device__ __forceinline__ R unpark(int i) const { return *(volatile R *)(p + i * stride); }
 };
 template <class R>
 struct RegTrace {
     R v[TRACE_VALUES];
     __device__ __forceinline__ void set(int i, R x) { v[i] = x; }
     __device__ __forceinline__ R get(int i) const { return v[i]; }
+    __device__ __forceinline__ void park(int i, R x) { v[i] = x; }
+    __device__ __forceinline__ R unpark(int i) const { return v[i]; }
 };
 
 template <class A, int VARIANT, class T, class TS>
@@ -364,30 +370,39 @@ __device__ __forceinline__ void pair_core(const DevMesh<A> &m, int r, const Cell
         const bool b_same = rb_ && (!ra_ || same_bits(oi.qr[1], qr1_m));
         const R ql2_m = ra_ ? A::dot(A_.v, cs, -A_.u, sn, M_QL2M) : oi.ql[2];
         const bool b_resum = b_same && ra_ && !same_bits(oi.ql[2], ql2_m);
-        const R term_a = osher_f1_term<A>(oi.ratio, oi.hcR, oi.ur);
-        const R term_b = osher_f1_term<A>(oi.ratio, oi.hcR, ur_m);
         if (b_resum) { tslot.set(6, ql2_m); tslot.set(7, oi.qr[2]); }
-        const typename A::level zbcA = A_.zbc, zbcB = B_.zbc;
+        // the epilogues' other inputs wait across Osher in the trace store too
+        // (read back afterwards rather than held in registers)
+        tslot.park(8, osher_f1_term<A>(oi.ratio, oi.hcR, oi.ur));   // FLUX1 term of side a
+        tslot.park(9, osher_f1_term<A>(oi.ratio, oi.hcR, ur_m));    // FLUX1 term of side b
+        tslot.park(10, cs);
+        tslot.park(11, sn);
+        tslot.park(12, g.z);
+        using L = typename A::level;
+        L zbcA = A_.zbc, zbcB = B_.zbc;
+        if constexpr (std::is_same<L, R>::value) { tslot.park(13, zbcA); tslot.park(14, zbcB); }
         R fo[4];
         OsherTraceIn<TS> tr{&tslot, 0u, 0u};
         osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo, &tr);
+        const R pcs = tslot.unpark(10), psn = tslot.unpark(11), pside = tslot.unpark(12);
+        if constexpr (std::is_same<L, R>::value) { zbcA = tslot.unpark(13); zbcB = tslot.unpark(14); }
         if (ra_) {
             R f[4];
             f[0] = fo[0];
-            f[1] = A::add(fo[1], term_a);
+            f[1] = A::add(fo[1], tslot.unpark(8));
             f[2] = fo[2];
             f[3] = fo[3];
             if (write_flux) store_flux(m, ix.z, f);
-            store_terms<A>(tout, ix.z, f, g.z, cs, sn);
+            store_terms<A>(tout, ix.z, f, pside, pcs, psn);
         }
         if (b_same) {
             R f[4];
             f[0] = -fo[0];
-            f[1] = A::add(fo[1], term_b);
+            f[1] = A::add(fo[1], tslot.unpark(9));
             f[2] = b_resum ? osher_f2<A>(tr, tslot.get(6), tslot.get(7)) : fo[2];
             f[3] = mirror_f3<A>(fo[3], zbcA, zbcB);
             if (write_flux) store_flux(m, ix.w, f);
-            store_terms<A>(tout, ix.w, f, g.z, -cs, -sn);
+            store_terms<A>(tout, ix.w, f, pside, -pcs, -psn);
         } else if (rb_) {
             queue[atomicAdd(qn, 1)] = r;
         }
