@@ -381,20 +381,28 @@ __device__ __forceinline__ void osher(typename A::real cl, const typename A::rea
     } else {
         qf_skip<A>(tr, 1);
     }
-    // pieces 3 and 5 share UA = (FIL + FIR)/2
+    // pieces 3 and 5 share UA = (FIL + FIR)/2 and the same arithmetic on
+    // their own inputs (FIL - UA with QL's tangent, FIR - UA with QR's); no
+    // case takes both, so one code path forms whichever is taken and a warp
+    // whose lanes take different ones runs it once
     const R ua35 = A::mul(A::add(fil, fir), A::c(0.5));
-    if (p3) {
-        R fil3 = A::sub(fil, ua35);
-        R ha = A::divk(A::mul(fil3, fil3), 39.24);
-        qf_acc_if<A>(out, true, false, ha, ua35, ql[2], tr, 2);
+    const R fir5 = A::sub(fir, ua35);
+    if (p3 || p5) {
+        const R d = p3 ? A::sub(fil, ua35) : fir5;
+        const R ha = A::divk(A::mul(d, d), 39.24);
+        const R vt = p3 ? ql[2] : qr[2];
+        const R f0 = A::mul(ha, ua35);
+        out[0] = A::madd(ha, ua35, out[0], M_ACC0);
+        out[1] = A::madd(f0, ua35, out[1], M_ACC123);
+        out[2] = A::madd(f0, vt, out[2], M_ACC123);
+        out[3] = A::madd(A::mul(A::c(4.905), ha), ha, out[3], M_ACC123);
+        if constexpr (!std::is_same<TR, void>::value) {
+            tr->set(2, p3 ? f0 : R(0));
+            tr->set(3, p5 ? f0 : R(0));
+            tr->act |= (p3 ? 4u : 0u) | (p5 ? 8u : 0u);
+        }
     } else {
         qf_skip<A>(tr, 2);
-    }
-    R fir5 = A::sub(fir, ua35);
-    if (p5) {
-        R ha = A::divk(A::mul(fir5, fir5), 39.24);
-        qf_acc_if<A>(out, true, false, ha, ua35, qr[2], tr, 3);
-    } else {
         qf_skip<A>(tr, 3);
     }
     // piece 6: US = FIR/3 with FIR as piece 5 left it

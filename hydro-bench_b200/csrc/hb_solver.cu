@@ -637,6 +637,9 @@ int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     case 5: rc = go(flux_kernel<A, VARIANT, 128, 7, SEG>, 128, update_kernel<A, VARIANT, 6, SEG>); break;
     case 6: rc = go(flux_kernel<A, VARIANT, 256, 2, SEG>, 256, update_kernel<A, VARIANT, 6, SEG>); break;
     case 7: rc = go(flux_kernel<A, VARIANT, 64, 12, SEG>, 64, update_kernel<A, VARIANT, 8, SEG>); break;
+    case 14: rc = go(flux_kernel<A, VARIANT, 128, 7, SEG>, 128, update_kernel<A, VARIANT, 8, SEG>); break;
+    case 15: rc = go(flux_kernel<A, VARIANT, 128, 6, SEG>, 128, update_kernel<A, VARIANT, 9, SEG>); break;
+    case 16: rc = go(flux_kernel<A, VARIANT, 128, 7, SEG>, 128, update_kernel<A, VARIANT, 9, SEG>); break;
     default: return hb::set_error(HB_E_INVALID, "launch shape %d is not an edge-layout shape", h->launch_config + 1);
     }
     if (rc != HB_OK) return rc;

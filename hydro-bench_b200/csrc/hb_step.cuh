@@ -28,7 +28,8 @@ constexpr LaunchConfig LAUNCH_CONFIGS[] = {
     {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 8}, {LAYOUT_EDGE, 128, 8, 8}, {LAYOUT_EDGE, 256, 3, 6},
     {LAYOUT_EDGE, 256, 4, 8}, {LAYOUT_EDGE, 128, 7, 6}, {LAYOUT_EDGE, 256, 2, 6}, {LAYOUT_EDGE, 64, 12, 8},
     {LAYOUT_TILE, 256, 3, 0}, {LAYOUT_TILE, 256, 2, 0}, {LAYOUT_TILE, 128, 6, 0}, {LAYOUT_TILE, 128, 4, 0},
-    {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0}};
+    {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0},
+    {LAYOUT_EDGE, 128, 7, 8}, {LAYOUT_EDGE, 128, 6, 9}, {LAYOUT_EDGE, 128, 7, 9}};
 constexpr int N_LAUNCH_CONFIGS = sizeof(LAUNCH_CONFIGS) / sizeof(LAUNCH_CONFIGS[0]);
 constexpr int DEFAULT_EDGE_CONFIG = 0;
 constexpr int DEFAULT_TILE_CONFIG = 8;
@@ -469,8 +470,9 @@ __global__ void __launch_bounds__(THREADS, MINB) flux_kernel(DevMesh<A> m, int k
 }
 
 // Sums and update of one cell (UpdateCellKernel, functors.cu:717-784).  The
-// zero-length fourth slot of a triangle is evaluated here without pow
-// (flux_slot's ZERO_LEN), exactly when fluxes are written out.
+// zero-length fourth slot of a triangle is evaluated here, without pow
+// (flux_slot's ZERO_LEN) unless fluxes are written out, and only where its
+// zero addends can change the sums.
 // SMEM_TERMS: `terms` is in shared memory (tile layout), else global.
 // update_core takes the cell's stored state record `raw` and bed `zbc`.
 template <class A, int VARIANT, bool COEF = false, bool SMEM_TERMS = false>
@@ -492,42 +494,61 @@ __device__ __forceinline__ void update_core(const DevMesh<A> &m, int c, const Ve
     for (int j = 0; j < 4; j++)
         t[j] = !(mask & (1u << j)) ? Vec4<R>{R(0), R(0), R(0), R(0)}
                                    : (SMEM_TERMS ? ld4(terms + 4 * j) : ldg4(terms + 4 * j));
+    // The slot sums in slot order j = 0..3.  A zero-length slot (a
+    // triangle's fourth) adds SIDE*F0 = 0*F0 to WH and 0*(...) to WU and WV.
+    // For a finite state (h > 0) its fluxes are finite, so each addend is a
+    // zero and leaves a non-zero partial sum unchanged bit for bit: the first
+    // pass skips such slots.  Only a zero partial sum at a zero-length slot
+    // (whose sign the addend may change), a non-finite state, or the last
+    // step of a sequence (which writes the slot's fluxes) needs the slot's
+    // flux: the second pass then evaluates it once (every zero-length slot of
+    // a cell has the same inputs: the cell's state, no neighbour, zero
+    // geometry and code 0) and redoes the sums with every slot in order.
+    // Keeping that evaluation off the common path keeps the kernel's
+    // register count that of the sums and the update.
     R wh = R(0), wu = R(0), wv = R(0);
+    const bool finite_state = st.h > R(0) && isfinite((double)st.h) && isfinite((double)st.u) &&
+                              isfinite((double)st.v) && isfinite((double)st.z) && isfinite((double)st.zbc);
+    bool need_zero = false;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-        const int s = 4 * c + j;
         if (mask & (1u << j)) {
             // F0 and SIDE for WH; the WU/WV increments were formed by the flux kernel
             wh = A::madd(t[j].w, t[j].x, wh, M_WH);
             wu = A::add(wu, t[j].y);
             wv = A::add(wv, t[j].z);
+        } else if (write_flux || !finite_state || wh == R(0) || wu == R(0) || wv == R(0)) {
+            need_zero = true;
+        }
+    }
+    if (need_zero) {
+        SlotInA<A> in;
+        in.own = st;
+        in.nb = {R(0), R(0), R(0), L(0), L(0)};
+        in.has_nb = false; in.own_first = false; in.code = CODE_ZERO;
+        in.cosj = R(0); in.sinj = R(0); in.side = R(0);
+        auto nofetch = []() { return BoundaryInA<A>{}; };
+        SlotOut<R> o;
+        if (write_flux) {
+            flux_slot<A, VARIANT, decltype(nofetch), false>(in, A::sqrt(A::mul(A::c(9.81), st.h)), p, nofetch, o);
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (!(mask & (1u << j))) store_flux(m, 4 * c + j, o.f);
         } else {
-            // A zero-length slot adds SIDE*F0 = 0*F0 to WH and 0*(...) to WU and
-            // WV.  For a finite state (h > 0) its fluxes are finite, so each
-            // addend is a zero and leaves a non-zero partial sum unchanged bit
-            // for bit: the slot is then skipped.  Only a zero partial sum (whose
-            // sign the addend may change) or a non-finite state takes the full
-            // evaluation, as does the last step of a sequence, which writes the
-            // slot's fluxes.
-            if (!write_flux && wh != R(0) && wu != R(0) && wv != R(0) && st.h > R(0) &&
-                isfinite((double)st.h) && isfinite((double)st.u) && isfinite((double)st.v) &&
-                isfinite((double)st.z) && isfinite((double)st.zbc))
-                continue;
-            SlotInA<A> in;
-            in.own = st;
-            in.nb = {R(0), R(0), R(0), L(0), L(0)};
-            in.has_nb = false; in.own_first = false; in.code = CODE_ZERO;
-            in.cosj = R(0); in.sinj = R(0); in.side = R(0);
-            auto nofetch = []() { return BoundaryInA<A>{}; };
-            SlotOut<R> o;
-            if (write_flux) {
-                flux_slot<A, VARIANT, decltype(nofetch), false>(in, A::sqrt(A::mul(A::c(9.81), st.h)), p, nofetch, o);
-                store_flux(m, s, o.f);
+            flux_chain<A, VARIANT, decltype(nofetch), true>(in, R(0), p, nofetch, o);
+        }
+        wh = R(0); wu = R(0); wv = R(0);
+#pragma unroll 1
+        for (int j = 0; j < 4; j++) {
+            if (mask & (1u << j)) {
+                const Vec4<R> tj = SMEM_TERMS ? ld4(terms + 4 * j) : ldg4(terms + 4 * j);
+                wh = A::madd(tj.w, tj.x, wh, M_WH);
+                wu = A::add(wu, tj.y);
+                wv = A::add(wv, tj.z);
             } else {
-                flux_chain<A, VARIANT, decltype(nofetch), true>(in, R(0), p, nofetch, o);
+                // zero-length slot: SIDE = SLCOS = SLSIN = 0 (mesh.cpp:293-306, :347-370)
+                wsum_add<A>(wh, wu, wv, o.f[0], o.f[1], o.f[2], o.f[3], R(0), R(0), R(0));
             }
-            // zero-length slot: SIDE = SLCOS = SLSIN = 0 (mesh.cpp:293-306, :347-370)
-            wsum_add<A>(wh, wu, wv, o.f[0], o.f[1], o.f[2], o.f[3], R(0), R(0), R(0));
         }
     }
     CellUpdateIn<R, L> ci;
