@@ -629,7 +629,7 @@ int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     int rc;
     using namespace hb;
     switch (h->launch_config) {
-    case 0: rc = go(flux_kernel<A, VARIANT, 128, 6, SEG>, 128, update_kernel<A, VARIANT, 6, SEG>); break;
+    case 0: rc = go(flux_kernel<A, VARIANT, 128, 7, SEG>, 128, update_kernel<A, VARIANT, 8, SEG>); break;
     case 1: rc = go(flux_kernel<A, VARIANT, 128, 6, SEG>, 128, update_kernel<A, VARIANT, 8, SEG>); break;
     case 2: rc = go(flux_kernel<A, VARIANT, 128, 8, SEG>, 128, update_kernel<A, VARIANT, 8, SEG>); break;
     case 3: rc = go(flux_kernel<A, VARIANT, 256, 3, SEG>, 256, update_kernel<A, VARIANT, 6, SEG>); break;
@@ -637,7 +637,7 @@ int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     case 5: rc = go(flux_kernel<A, VARIANT, 128, 7, SEG>, 128, update_kernel<A, VARIANT, 6, SEG>); break;
     case 6: rc = go(flux_kernel<A, VARIANT, 256, 2, SEG>, 256, update_kernel<A, VARIANT, 6, SEG>); break;
     case 7: rc = go(flux_kernel<A, VARIANT, 64, 12, SEG>, 64, update_kernel<A, VARIANT, 8, SEG>); break;
-    case 14: rc = go(flux_kernel<A, VARIANT, 128, 7, SEG>, 128, update_kernel<A, VARIANT, 8, SEG>); break;
+    case 14: rc = go(flux_kernel<A, VARIANT, 128, 6, SEG>, 128, update_kernel<A, VARIANT, 6, SEG>); break;
     case 15: rc = go(flux_kernel<A, VARIANT, 128, 6, SEG>, 128, update_kernel<A, VARIANT, 9, SEG>); break;
     case 16: rc = go(flux_kernel<A, VARIANT, 128, 7, SEG>, 128, update_kernel<A, VARIANT, 9, SEG>); break;
     default: return hb::set_error(HB_E_INVALID, "launch shape %d is not an edge-layout shape", h->launch_config + 1);
@@ -646,8 +646,8 @@ int launch_steps_t(hb_handle *h, hb::DevMesh<A> m, int n, cudaStream_t st) {
     return launch_tick(h, n, st);
 }
 
-// Persistent handles: the whole sequence as cooperative launches of the
-// default edge shape (128 threads, 6 CTAs per SM), as many CTAs as are
+// Persistent handles: the whole sequence as cooperative launches of
+// persistent_kernel (128 threads, 6 CTAs per SM), as many CTAs as are
 // resident at once, each launch preceded by zeroing its barrier words.
 // A launch takes at most PERSIST_MAX_STEPS steps, and fewer where its grid
 // is larger: every step adds 2 x grid arrivals to the 32-bit arrival count,

@@ -25,11 +25,11 @@ enum : uint8_t { META_CODE = 0x0F, META_OWN_FIRST = 0x10, META_HAS_NB = 0x20 };
 enum Layout : int { LAYOUT_EDGE = HB_LAYOUT_EDGE, LAYOUT_TILE = HB_LAYOUT_TILE };
 struct LaunchConfig { int layout, threads, min_blocks, update_min_blocks; };
 constexpr LaunchConfig LAUNCH_CONFIGS[] = {
-    {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 8}, {LAYOUT_EDGE, 128, 8, 8}, {LAYOUT_EDGE, 256, 3, 6},
+    {LAYOUT_EDGE, 128, 7, 8}, {LAYOUT_EDGE, 128, 6, 8}, {LAYOUT_EDGE, 128, 8, 8}, {LAYOUT_EDGE, 256, 3, 6},
     {LAYOUT_EDGE, 256, 4, 8}, {LAYOUT_EDGE, 128, 7, 6}, {LAYOUT_EDGE, 256, 2, 6}, {LAYOUT_EDGE, 64, 12, 8},
     {LAYOUT_TILE, 256, 3, 0}, {LAYOUT_TILE, 256, 2, 0}, {LAYOUT_TILE, 128, 6, 0}, {LAYOUT_TILE, 128, 4, 0},
     {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0},
-    {LAYOUT_EDGE, 128, 7, 8}, {LAYOUT_EDGE, 128, 6, 9}, {LAYOUT_EDGE, 128, 7, 9}};
+    {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 9}, {LAYOUT_EDGE, 128, 7, 9}};
 constexpr int N_LAUNCH_CONFIGS = sizeof(LAUNCH_CONFIGS) / sizeof(LAUNCH_CONFIGS[0]);
 constexpr int DEFAULT_EDGE_CONFIG = 0;
 constexpr int DEFAULT_TILE_CONFIG = 8;
