@@ -760,10 +760,16 @@ struct hb_adjoint {
     hb::adj::AdjMesh am{};
     cudaGraphExec_t fwd_graph = nullptr;    // k forward steps with checkpoint and gauge kernels
     cudaGraphExec_t fwd_graph_multi = nullptr;   // 100 / k such segments
+    // the whole backward pass (recomputation and reverse steps on their two
+    // streams), one graph for a backward that follows its forward (whose last
+    // segment is in place) and one for a repeated backward
+    cudaGraphExec_t bwd_graph[2] = {nullptr, nullptr};
     bool forward_done = false;
     ~hb_adjoint() {
         if (fwd_graph) cudaGraphExecDestroy(fwd_graph);
         if (fwd_graph_multi) cudaGraphExecDestroy(fwd_graph_multi);
+        for (auto &g : bwd_graph)
+            if (g) cudaGraphExecDestroy(g);
         for (int q = 0; q < 2; q++) {
             if (ev_recomputed[q]) cudaEventDestroy(ev_recomputed[q]);
             if (ev_reversed[q]) cudaEventDestroy(ev_reversed[q]);
@@ -1102,27 +1108,13 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
     return HB_OK;
 }
 
-extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_zbc, void *stream) {
-    NvtxRange nvtx_("hb_adjoint_backward");
-    if (!a) return hb::set_error(HB_E_INVALID, "null adjoint");
-    if (!a->forward_done) return hb::set_error(HB_E_INVALID, "hb_adjoint_backward: run hb_adjoint_forward first");
+namespace {
+
+// The backward pass's device work, on the reverse stream `st` and the
+// recompute stream (forked from and joined back to `st`).  have_last: the
+// forward left the last segment's states and coefficients in place.
+int enqueue_backward(hb_adjoint *a, bool have_last, cudaStream_t st, std::vector<cudaEvent_t> &temp_events) {
     hb_handle *h = a->h;
-    // The reverse steps run on the adjoint's own lowest-priority stream and
-    // the recomputation of the next segment on its highest-priority one, both
-    // joined to the caller's stream.  The recomputation is a chain of small
-    // kernels; given priority, its blocks start as soon as they are ready
-    // instead of queueing behind the reverse grids, which fill the rest of
-    // the GPU (measured: backward 19.4 -> 17.1 ms on the 24K-cell, 1000-step
-    // case; the other way round, 21.1 ms).
-    cudaStream_t user = (cudaStream_t)stream;
-    cudaStream_t st = a->reverse;
-    {
-        cudaEvent_t join = nullptr;
-        HB_CUDA_RET(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
-        HB_CUDA_RET(cudaEventRecord(join, user));
-        HB_CUDA_RET(cudaStreamWaitEvent(st, join, 0));
-        cudaEventDestroy(join);
-    }
     const int C = a->C;
     const size_t S4 = 4 * (size_t)C;
     hb::adj::AdjMesh am = a->am;
@@ -1149,18 +1141,18 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
     // counter or any other array the forward kernels write besides the
     // segment buffers.
     cudaStream_t rs = a->recompute;
-    cudaEvent_t start_ev = nullptr;
-    HB_CUDA_RET(cudaEventCreateWithFlags(&start_ev, cudaEventDisableTiming));
-    HB_CUDA_RET(cudaEventRecord(start_ev, st));
-    HB_CUDA_RET(cudaStreamWaitEvent(rs, start_ev, 0));   // after this call's earlier work on st
-    cudaEventDestroy(start_ev);
+    cudaEvent_t fork = nullptr, join = nullptr;
+    HB_CUDA_RET(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    temp_events.push_back(fork);
+    HB_CUDA_RET(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    temp_events.push_back(join);
+    HB_CUDA_RET(cudaEventRecord(fork, st));
+    HB_CUDA_RET(cudaStreamWaitEvent(rs, fork, 0));   // after this pass's earlier work on st
     bool reversed_once[2] = {false, false};
     // state i of segment sgi: its checkpoint, then the segment buffer
     auto seg_state = [&](int sgi, int i) -> const double * {
         return i == 0 ? a->d_ckpt + (size_t)sgi * S4 : a->d_seg[sgi & 1] + (size_t)i * S4;
     };
-    // the forward left the last segment's states and coefficients in place
-    const bool have_last = a->recorded_seg == nseg - 1;
     auto issue_recompute = [&](int sgi) -> int {
         const int b = sgi & 1;
         const int t0 = sgi * a->k, len = std::min(t0 + a->k, a->T) - t0;
@@ -1193,6 +1185,9 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
         HB_CUDA_RET(cudaEventRecord(a->ev_reversed[b], st));
         reversed_once[b] = true;
     }
+    // the recompute stream's work is all joined by now; join it explicitly too
+    HB_CUDA_RET(cudaEventRecord(join, rs));
+    HB_CUDA_RET(cudaStreamWaitEvent(st, join, 0));
     // the adjoint of x_0 (step 0 wrote copy 0)
     hb::adj::adj_gather_kernel<<<(4 * C + 127) / 128, 128, 0, st>>>(C, am, a->d_dir[0], a->d_so[0], a->d_sn[0]);
     HB_CUDA_RET(cudaGetLastError());
@@ -1200,6 +1195,63 @@ extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_z
     HB_CUDA_RET(cudaGetLastError());
     // leave the handle's counter where the forward left it
     hb::adj::set_counter_kernel<<<1, 1, 0, st>>>(h->d_ctr, a->T);
+    return HB_OK;
+}
+
+// Captures enqueue_backward on the reverse stream into an executable graph
+// that keeps the recompute stream's higher priority per node.
+int capture_backward(hb_adjoint *a, bool have_last, cudaGraphExec_t *exec) {
+    cudaStream_t st = a->reverse;
+    std::vector<cudaEvent_t> temp;
+    HB_CUDA_RET(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue_backward(a, have_last, st, temp);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    for (cudaEvent_t ev : temp) cudaEventDestroy(ev);
+    if (rc != HB_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return hb::set_error(HB_E_CUDA, "adjoint backward capture: %s", cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiateWithFlags(exec, g, cudaGraphInstantiateFlagUseNodePriority);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        *exec = nullptr;
+        return hb::set_error(HB_E_CUDA, "adjoint backward graph: %s", cudaGetErrorString(ei));
+    }
+    return HB_OK;
+}
+
+}  // namespace
+
+extern "C" int hb_adjoint_backward(hb_adjoint *a, double *grad_n, double *grad_zbc, void *stream) {
+    NvtxRange nvtx_("hb_adjoint_backward");
+    if (!a) return hb::set_error(HB_E_INVALID, "null adjoint");
+    if (!a->forward_done) return hb::set_error(HB_E_INVALID, "hb_adjoint_backward: run hb_adjoint_forward first");
+    hb_handle *h = a->h;
+    // The reverse steps run on the adjoint's own lowest-priority stream and
+    // the recomputation of the next segment on its highest-priority one, both
+    // joined to the caller's stream.  The recomputation is a chain of small
+    // kernels; given priority, its blocks start as soon as they are ready
+    // instead of queueing behind the reverse grids, which fill the rest of
+    // the GPU (measured: backward 19.4 -> 17.1 ms on the 24K-cell, 1000-step
+    // case; the other way round, 21.1 ms).  The pass is one graph, captured
+    // on first use (per kind of pass) and replayed after: its thousands of
+    // launches then cost no host time each.
+    cudaStream_t user = (cudaStream_t)stream;
+    cudaStream_t st = a->reverse;
+    {
+        cudaEvent_t join = nullptr;
+        HB_CUDA_RET(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+        HB_CUDA_RET(cudaEventRecord(join, user));
+        HB_CUDA_RET(cudaStreamWaitEvent(st, join, 0));
+        cudaEventDestroy(join);
+    }
+    const int C = a->C;
+    const hb::adj::AdjMesh am = a->am;
+    const int nseg = (a->T + a->k - 1) / a->k;
+    // the forward left the last segment's states and coefficients in place
+    const bool have_last = a->recorded_seg == nseg - 1;
+    cudaGraphExec_t &ge = a->bwd_graph[have_last ? 1 : 0];
+    if (!ge) TRY(capture_backward(a, have_last, &ge));
+    HB_CUDA_RET(cudaGraphLaunch(ge, st));
     a->recorded_seg = -1;   // the segment buffers were reused
     {
         cudaEvent_t done = nullptr;

@@ -29,7 +29,7 @@ constexpr LaunchConfig LAUNCH_CONFIGS[] = {
     {LAYOUT_EDGE, 256, 4, 8}, {LAYOUT_EDGE, 128, 7, 6}, {LAYOUT_EDGE, 256, 2, 6}, {LAYOUT_EDGE, 64, 12, 8},
     {LAYOUT_TILE, 256, 3, 0}, {LAYOUT_TILE, 256, 2, 0}, {LAYOUT_TILE, 128, 6, 0}, {LAYOUT_TILE, 128, 4, 0},
     {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0},
-    {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 9}, {LAYOUT_EDGE, 128, 7, 9}};
+    {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 9}, {LAYOUT_EDGE, 128, 7, 9}, {LAYOUT_TILE, 128, 8, 0}};
 constexpr int N_LAUNCH_CONFIGS = sizeof(LAUNCH_CONFIGS) / sizeof(LAUNCH_CONFIGS[0]);
 constexpr int DEFAULT_EDGE_CONFIG = 0;
 constexpr int DEFAULT_TILE_CONFIG = 8;
@@ -382,19 +382,28 @@ __device__ __forceinline__ void pair_core(const DevMesh<A> &m, int r, const Cell
         using L = typename A::level;
         L zbcA = A_.zbc, zbcB = B_.zbc;
         if constexpr (std::is_same<L, R>::value) { tslot.park(13, zbcA); tslot.park(14, zbcB); }
+        // the two slot indices wait in the trace store too (fp64: one 64-bit slot)
+        int psa = ix.z, psb = ix.w;
+        if constexpr (sizeof(R) == 8)
+            tslot.park(15, __longlong_as_double((long long)(((unsigned long long)(unsigned)psb << 32) | (unsigned)psa)));
         R fo[4];
         OsherTraceIn<TS> tr{&tslot, 0u, 0u};
         osher<A>(oi.cl, oi.ql, oi.qr, oi.fil, fo, &tr);
         const R pcs = tslot.unpark(10), psn = tslot.unpark(11), pside = tslot.unpark(12);
         if constexpr (std::is_same<L, R>::value) { zbcA = tslot.unpark(13); zbcB = tslot.unpark(14); }
+        if constexpr (sizeof(R) == 8) {
+            const unsigned long long w = (unsigned long long)__double_as_longlong((double)tslot.unpark(15));
+            psa = (int)(unsigned)(w & 0xFFFFFFFFull);
+            psb = (int)(unsigned)(w >> 32);
+        }
         if (ra_) {
             R f[4];
             f[0] = fo[0];
             f[1] = A::add(fo[1], tslot.unpark(8));
             f[2] = fo[2];
             f[3] = fo[3];
-            if (write_flux) store_flux(m, ix.z, f);
-            store_terms<A>(tout, ix.z, f, pside, pcs, psn);
+            if (write_flux) store_flux(m, psa, f);
+            store_terms<A>(tout, psa, f, pside, pcs, psn);
         }
         if (b_same) {
             R f[4];
@@ -402,8 +411,8 @@ __device__ __forceinline__ void pair_core(const DevMesh<A> &m, int r, const Cell
             f[1] = A::add(fo[1], tslot.unpark(9));
             f[2] = b_resum ? osher_f2<A>(tr, tslot.get(6), tslot.get(7)) : fo[2];
             f[3] = mirror_f3<A>(fo[3], zbcA, zbcB);
-            if (write_flux) store_flux(m, ix.w, f);
-            store_terms<A>(tout, ix.w, f, pside, -pcs, -psn);
+            if (write_flux) store_flux(m, psb, f);
+            store_terms<A>(tout, psb, f, pside, -pcs, -psn);
         } else if (rb_) {
             queue[atomicAdd(qn, 1)] = r;
         }

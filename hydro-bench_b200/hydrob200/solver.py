@@ -73,9 +73,9 @@ class Deck:
         if getattr(self, "_h", None) and self._h.value:
             try:
                 self._lib.hb_deck_free(self._h)
+                self._h = C.c_void_p()
             except TypeError:   # interpreter shutdown: ctypes already torn down, the process frees everything
                 pass
-            self._h = C.c_void_p()
 
     @property
     def cells(self) -> int:

@@ -209,3 +209,46 @@ def test_step_host_block_rows_equal_device_steps(deck_dir, persistent):
     for i, k in enumerate("HUVZ"):
         assert _bits_equal(block[i], ref[k]), k
     assert _bits_equal(b.get_state()["W"], ref["W"])
+
+
+@pytest.mark.parametrize("persistent", [False, True])
+def test_step_host_page_locked_graph_equals_device_steps(deck_dir, persistent):
+    """hb_step_host with page-locked buffers (as the end-to-end bench passes
+    them), switching buffers, step counts per call, W and the launch shape
+    between calls: every call equals hb_step + hb_get_state bit for bit (fp64)."""
+    import torch
+    deck = hb.Deck(deck_dir["f1"])
+    a = hb.Solver(deck)
+    b = hb.Solver(deck, persistent=persistent)
+    st = deck.state()
+    C = deck.cells
+    blk1 = torch.empty((4, C), dtype=torch.float64).pin_memory()
+    blk2 = torch.empty((4, C), dtype=torch.float64).pin_memory()
+    w = torch.empty(C, dtype=torch.float64).pin_memory()
+    for i, k in enumerate("HUVZ"):
+        blk1[i].copy_(torch.from_numpy(st[k]))
+    done = 0
+    # (buffer, steps per call, calls), then a new step count, a new buffer with W,
+    # and a launch-shape change
+    plan = [(blk1, 1, 4), (blk1, 3, 2), (blk2, 1, 2), (blk2, 2, 2), ("shape", 0, 0), (blk2, 2, 2)]
+    cur = blk1
+    for buf, n, calls in plan:
+        if isinstance(buf, str):
+            if not persistent:
+                b.tile_config = 2
+            continue
+        if buf is not cur:
+            buf.copy_(cur)
+            cur = buf
+        for c in range(calls):
+            b.step_host(buf[0], buf[1], buf[2], buf[3], w if buf is blk2 else None, n)
+            done += n
+        b.sync()
+        a.step(n * calls)
+        a.sync()
+        ref = a.get_state()
+        for i, k in enumerate("HUVZ"):
+            assert _bits_equal(buf[i].numpy(), ref[k]), f"{k} after {done} steps"
+        if buf is blk2:
+            assert _bits_equal(w.numpy(), ref["W"])
+    assert b.position == a.position
