@@ -825,6 +825,13 @@ extern "C" int hb_adjoint_create(hb_handle *h, const int32_t *gauges, int32_t ng
     const int C = sc.cells;
     for (int i = 0; i < ngauges; i++)
         if (gauges[i] < 0 || gauges[i] >= C) return hb::set_error(HB_E_INVALID, "hb_adjoint_create: gauge %d out of range", gauges[i]);
+    {   // one gauge per cell: the reverse sweep and the fused forward map each cell to one gauge
+        std::vector<char> seen(C, 0);
+        for (int i = 0; i < ngauges; i++) {
+            if (seen[gauges[i]]) return hb::set_error(HB_E_INVALID, "hb_adjoint_create: cell %d is a gauge twice", gauges[i]);
+            seen[gauges[i]] = 1;
+        }
+    }
     // per-slot geometry, codes and facing slots (device order); codes without a reverse are rejected
     std::vector<double> cs4(4 * (size_t)C, 0.0), sn4(4 * (size_t)C, 0.0), side4(4 * (size_t)C, 0.0);
     std::vector<int32_t> nbr4(4 * (size_t)C, -1), mirror4(4 * (size_t)C, -1);
@@ -996,8 +1003,31 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
+    // Fused form (plain fp64 edge-layout handles): the cell kernel of each
+    // step writes the checkpoints and gauge depths itself (hb::DevMesh's
+    // adjoint outputs), so a run of segments is one step sequence with no
+    // kernels between the steps; checkpoint 0 is copied once up front.
+    const bool fused = hb_steps_take_mesh(h);
+    hb::DevMesh<hb::F64Exact> mk = h->m64;
+    mk.ckpt = a->d_ckpt;
+    mk.ckpt_every = a->k;
+    mk.gauge_of = a->am.gauge_of;
+    mk.gauge_out = a->d_gd;
+    mk.obs_every = a->obs_every;
+    mk.ngauge = a->ng;
+    if (fused) {
+        cudaLaunchConfig_t c0{};
+        c0.gridDim = dim3(64);
+        c0.blockDim = dim3(256);
+        c0.stream = st;
+        c0.attrs = attr;
+        c0.numAttrs = 1;
+        HB_CUDA_RET(cudaLaunchKernelEx(&c0, hb::adj::ckpt_kernel, (const double *)h->m64.S[0],
+                                       (const double *)h->m64.S[1], a->d_ckpt, (const long long *)h->d_ctr, a->k, S4));
+    }
     // nsegs k-step segments from a step that is a multiple of k
     auto enqueue = [&](int nsegs, cudaStream_t s) -> int {
+        if (fused) return hb_enqueue_steps_mesh(h, mk, nsegs * a->k, s);
         const double *S0 = h->m64.S[0], *S1 = h->m64.S[1];
         cudaLaunchConfig_t ck{};
         ck.gridDim = dim3(64);
@@ -1070,9 +1100,11 @@ extern "C" int hb_adjoint_forward(hb_adjoint *a, double *loss, double *gauge_dep
         cudaLaunchConfig_t gk = ck;
         gk.gridDim = dim3((unsigned)((a->ng + 127) / 128));
         gk.blockDim = dim3(128);
-        HB_CUDA_RET(cudaLaunchKernelEx(&ck, hb::adj::ckpt_kernel, (const double *)h->m64.S[0],
-                                       (const double *)h->m64.S[1], a->d_ckpt, (const long long *)h->d_ctr, a->k,
-                                       S4));
+        // (fused: the segment's checkpoint was written by the step before it, or up front)
+        if (!fused)
+            HB_CUDA_RET(cudaLaunchKernelEx(&ck, hb::adj::ckpt_kernel, (const double *)h->m64.S[0],
+                                           (const double *)h->m64.S[1], a->d_ckpt, (const long long *)h->d_ctr, a->k,
+                                           S4));
         for (int i = 0; i < len; i++) {
             const double *in = i == 0 ? h->m64.S[t0 & 1] : a->d_seg[b] + (size_t)i * S4;
             double *out = a->d_seg[b] + (size_t)(i + 1) * S4;

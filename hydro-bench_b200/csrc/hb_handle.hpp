@@ -128,6 +128,11 @@ int dev_alloc(hb_handle *h, T **dst, size_t count) {
 
 // the forward step machinery of hb_solver.cu
 int hb_enqueue_steps(hb_handle *h, int n, cudaStream_t st);
+// n steps of a plain fp64 edge-layout single mesh (hb_steps_take_mesh) at the
+// handle's launch shape, from `m`, a copy of the handle's device mesh with the
+// adjoint forward's checkpoint and gauge outputs set
+bool hb_steps_take_mesh(const hb_handle *h);
+int hb_enqueue_steps_mesh(hb_handle *h, const hb::DevMesh<hb::F64Exact> &m, int n, cudaStream_t st);
 int hb_check_range(hb_handle *h, long long n);
 int hb_launch_tick(hb_handle *h, int n, cudaStream_t st);
 // the tile layout (hb_tiles.cu): n steps at the handle's launch shape, and the

@@ -738,6 +738,17 @@ int check_range(hb_handle *h, long long n) {
 }  // namespace
 
 int hb_enqueue_steps(hb_handle *h, int n, cudaStream_t st) { return enqueue_steps(h, n, st); }
+
+bool hb_steps_take_mesh(const hb_handle *h) {
+    return h->opt.precision == HB_FP64 && h->opt.layout == HB_LAYOUT_EDGE && !h->opt.persistent && !h->segmented();
+}
+
+int hb_enqueue_steps_mesh(hb_handle *h, const hb::DevMesh<hb::F64Exact> &m, int n, cudaStream_t st) {
+    if (!hb_steps_take_mesh(h)) return hb::set_error(HB_E_INVALID, "steps from a mesh copy: fp64 edge-layout single meshes only");
+    if (n <= 0) return HB_OK;
+    return h->opt.variant == HB_VARIANT_F ? launch_steps_t<hb::F64Exact, 1, false>(h, m, n, st)
+                                          : launch_steps_t<hb::F64Exact, 0, false>(h, m, n, st);
+}
 int hb_launch_tick(hb_handle *h, int n, cudaStream_t st) { return launch_tick(h, n, st); }
 int hb_check_range(hb_handle *h, long long n) { return check_range(h, n); }
 

@@ -72,6 +72,16 @@ struct DevMesh {
     const uint8_t *cmask;      // [C] bit j: slot j is a real slot
     R *slotw;                  // [4C][4] per-slot terms of the cell sums {F0, dWU, dWV, SIDE}
     double *ucoef;             // [C][UPDATE_COEF] update coefficients (update kernels with COEF only)
+    // Adjoint forward rollout (fp64; set only on a copy of the mesh whose
+    // step launches are captured for it, null otherwise): the cell update of
+    // step t also writes the new state into checkpoint (t + 1) / ckpt_every
+    // of `ckpt` ([][C][4]) when t + 1 is a multiple of ckpt_every, and, when
+    // t + 1 ends on an observation, a gauge cell's new depth into row
+    // (t + 1) / obs_every - 1, column gauge_of[cell], of `gauge_out`.
+    double *ckpt;
+    const int32_t *gauge_of;   // [C] gauge index of the cell, -1 for none
+    double *gauge_out;         // [observations][ngauge]
+    int ckpt_every, obs_every, ngauge;
     // records [nrecords]
     const int4 *rix;           // {a, b, sa, sb}: cell of the slot, its neighbour (-1 = none),
                                // slot 4*a+j, and for a pair the slot of b (-1 otherwise)
@@ -104,12 +114,13 @@ struct DevMesh {
     int ntiles, max_tile_cells, max_tile_pairs;
 };
 
-struct StepIndex { int par, kt, jt; };
+struct StepIndex { int par, kt, jt; long long step; };
 
 template <class A>
 __device__ __forceinline__ StepIndex step_index(const DevMesh<A> &m, int k, int per_day, int ndays) {
     const long long step = *m.step_ctr + k;
     StepIndex si;
+    si.step = step;
     si.par = (int)(step & 1);
     si.jt = (int)(step / per_day);
     si.kt = 1 + (int)(step % per_day);
@@ -573,6 +584,18 @@ __device__ __forceinline__ void update_core(const DevMesh<A> &m, int c, const Ve
     else stg4(m.S[np] + 4 * (size_t)c, o.h, o.u, o.v, o.z);
     m.W[c] = o.w;
     if (!(isfinite((double)o.h) && isfinite((double)o.u) && isfinite((double)o.v))) atomicOr(m.err, ERRBIT_NONFINITE);
+    if constexpr (std::is_same<A, F64Exact>::value) {
+        if (m.ckpt != nullptr) {
+            const long long t1 = si.step + 1;
+            if (t1 % m.ckpt_every == 0)
+                stg4(m.ckpt + 4 * ((size_t)(t1 / m.ckpt_every) * (size_t)m.C + (size_t)c), o.h, o.u, o.v, o.z);
+        }
+        if (m.gauge_of != nullptr) {
+            const long long t1 = si.step + 1;
+            const int g = m.gauge_of[c];
+            if (g >= 0 && t1 % m.obs_every == 0) m.gauge_out[(size_t)(t1 / m.obs_every - 1) * m.ngauge + g] = o.h;
+        }
+    }
 }
 
 template <class A, int VARIANT, bool COEF = false, bool SMEM_TERMS = false>

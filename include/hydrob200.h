@@ -232,8 +232,10 @@ const char *hb_status_string(int status);
  * fixed-point iteration counts) are those of the forward state.  The state is
  * checkpointed every checkpoint_every steps and each segment recomputed in
  * the backward pass.  Needs a single-mesh fp64 variant-H edge-layout handle,
- * not persistent, whose boundary codes are among KLAS 0, 1, 4, 10.  The rollout runs on the
- * handle's own mesh and state (its state is the rollout's end afterwards). */
+ * not persistent, whose boundary codes are among KLAS 0, 1, 4, 10; the gauges
+ * are distinct cells.  The rollout runs on the handle's own mesh and state
+ * (its state is the rollout's end afterwards).  Checkpoints and gauge depths
+ * are written by the rollout's own cell-update kernels. */
 typedef struct hb_adjoint hb_adjoint;
 int hb_adjoint_create(hb_handle *h, const int32_t *gauges, int32_t ngauges, int32_t obs_every, int32_t nsteps,
                       int32_t checkpoint_every, hb_adjoint **out);

@@ -227,3 +227,12 @@ def test_rejects_codes_without_a_reverse(deck_dir):
     deck = hb.Deck(deck_dir["stress_a"])
     with pytest.raises(hb.HydroError):
         Adjoint(deck, [0, 1], 5, 10)
+
+
+def test_rejects_a_cell_observed_twice(setup):
+    """Each gauge is its own cell: the rollout's cell kernels write one gauge
+    depth per cell, and the reverse sweep seeds one loss term per cell."""
+    g = list(setup["gauges"][:3]) + [setup["gauges"][0]]
+    with pytest.raises(hb.HydroError) as e:
+        Adjoint(setup["deck"], g, OBS_EVERY, NSTEPS)
+    assert e.value.status == 1
