@@ -29,7 +29,8 @@ constexpr LaunchConfig LAUNCH_CONFIGS[] = {
     {LAYOUT_EDGE, 256, 4, 8}, {LAYOUT_EDGE, 128, 7, 6}, {LAYOUT_EDGE, 256, 2, 6}, {LAYOUT_EDGE, 64, 12, 8},
     {LAYOUT_TILE, 256, 3, 0}, {LAYOUT_TILE, 256, 2, 0}, {LAYOUT_TILE, 128, 6, 0}, {LAYOUT_TILE, 128, 4, 0},
     {LAYOUT_TILE, 512, 1, 0}, {LAYOUT_TILE, 256, 4, 0},
-    {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 9}, {LAYOUT_EDGE, 128, 7, 9}, {LAYOUT_TILE, 128, 8, 0}};
+    {LAYOUT_EDGE, 128, 6, 6}, {LAYOUT_EDGE, 128, 6, 9}, {LAYOUT_EDGE, 128, 7, 9}, {LAYOUT_TILE, 128, 8, 0},
+    {LAYOUT_TILE, 256, 5, 0}};
 constexpr int N_LAUNCH_CONFIGS = sizeof(LAUNCH_CONFIGS) / sizeof(LAUNCH_CONFIGS[0]);
 constexpr int DEFAULT_EDGE_CONFIG = 0;
 constexpr int DEFAULT_TILE_CONFIG = 8;

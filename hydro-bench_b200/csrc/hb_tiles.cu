@@ -24,6 +24,7 @@ int with_tile_kernel(int config, F &&f) {
     case 12: return f(tile_kernel<A, VARIANT, 512, 1>, 512);
     case 13: return f(tile_kernel<A, VARIANT, 256, 4>, 256);
     case 17: return f(tile_kernel<A, VARIANT, 128, 8>, 128);
+    case 18: return f(tile_kernel<A, VARIANT, 256, 5>, 256);
     default: return hb::set_error(HB_E_INVALID, "launch shape %d is not a tile-layout shape", config + 1);
     }
 }
